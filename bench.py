@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Benchmark of the Imogen fluid step on B200.
+
+Workload (one GPU): the 3-D Kelvin-Helmholtz problem, plain HLLC FP64 drop-in, MC limiter:
+256^3 periodic unit cube, gamma = 5/3, P = 2.5, rho = 2 / v_x = +0.5 in the |y-1/2| < 1/4 band
+and rho = 1 / v_x = -0.5 elsewhere, seeded U(+-1e-2) velocity perturbations, CFL 0.4.
+One step = one main-loop iteration of the reference (imogen.m:115-139): CFL reduction, forward
+3-sweep fluid step, backward 3-sweep fluid step; the state advances by 2*dt.
+Metric: Mcell-updates/s = cells x iterations / seconds / 1e6 (whole job over all ranks).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: each rank runs an independent replica of the workload (the problem does not shard
+across GPUs in this build), scaling "weak"; the time is the maximum over ranks.
+--impl reference times the reference's CPU path, which for this hot path is the oracle's C
+restatement of the reference kernels (the reference itself has no CPU implementation), on all
+host cores, on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SHAPE = (256, 256, 256)
+GAMMA = 5.0 / 3.0
+CFL = 0.4
+METHOD = 2  # HLLC
+METRIC = "Mcell-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--shape", default=None, help="override grid, e.g. 128,128,128 (not the benchmark config)")
+    return ap.parse_args()
+
+
+def dist_init(n_gpus):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ["index", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + ",".join(self.FIELDS), "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            p = [x.strip() for x in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+                power.append(float(p[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_reference_sample(shape, iterations=1):
+    """Time the oracle (C restatement of the reference kernels, OpenMP on all host threads) on
+    `iterations` iterations of the workload; returns (Mcell-updates/s, seconds, threads)."""
+    from oracle import pyoracle as po
+    from gpuimogen_b200 import problems
+    po.lib()
+    q = problems.kelvin_helmholtz(shape, gamma=GAMMA, seed=12345)
+    h = [1.0 / s for s in shape]
+    sp = po.step_params(0.0, h, GAMMA, rho_min=1e-5, method=METHOD, slope="mc")
+    bc = ["circular"] * 6
+    t0 = time.perf_counter()
+    for it in range(iterations):
+        tau = po.cfl_timestep(q, shape, GAMMA, h, METHOD)
+        sp.dt = CFL * tau
+        po.fluid_step_3d(q, shape, sp, bc, 1, it)
+        po.fluid_step_3d(q, shape, sp, bc, -1, it)
+    sec = time.perf_counter() - t0
+    cells = shape[0] * shape[1] * shape[2]
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return cells * iterations / sec / 1e6, sec, threads
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    shape = tuple(int(s) for s in args.shape.split(",")) if args.shape else SHAPE
+    # bounded sample: one iteration of the full 256^3 workload per timed step
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_reference_sample((64, 64, 64), 1)
+    vals, secs = [], []
+    for _ in range(args.steps):
+        v, s, thr = cpu_reference_sample(shape, 1)
+        vals.append(v)
+        secs.append(s)
+    total = sum(secs)
+    value = shape[0] * shape[1] * shape[2] * args.steps / total / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mcell-updates/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": "kelvin_helmholtz_3d_hllc_fp64", "grid": list(shape), "gamma": GAMMA, "cfl": CFL,
+                   "limiter": "MC", "method": "HLLC", "time_scheme": "SSPRK2", "boundaries": "periodic"},
+        "cpu_baseline": {"value": value, "unit": "Mcell-updates/s", "cores": thr, "kind": "port",
+                         "sample": "%d iteration(s) of the %dx%dx%d workload per step, oracle C restatement of the "
+                                   "reference kernels (the reference has no CPU implementation of this path)"
+                                   % (1, *shape)},
+        "e2e": {"value": value, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init(args.gpus)
+    if args.impl == "reference":
+        rc = run_reference(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return rc
+
+    import torch
+    import torch.distributed as dist
+    import gpuimogen_b200 as ib
+    from gpuimogen_b200 import problems
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ib.load("product")
+    shape = tuple(int(s) for s in args.shape.split(",")) if args.shape else SHAPE
+    cells = shape[0] * shape[1] * shape[2]
+    q0 = problems.kelvin_helmholtz(shape, gamma=GAMMA, seed=12345 + rank)
+    slab = q0.shape[1]
+    fl = ib.Fluid(shape, bc="circular", q=torch.from_numpy(q0).to(dev), gamma=GAMMA)
+    geo = ib.Geometry(shape)
+    num = ib.numerics(slope="mc")
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    tm = ib.TimeManager(cfl=CFL)
+    for _ in range(args.warmup):
+        ib.run_iteration([fl], geo, tm, METHOD, num)
+    torch.cuda.synchronize()
+
+    # ---------------- device-resident timed region ----------------
+    sampler = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ
+                           else int(os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local]))
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    l0 = ib.imogen.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ib.run_iteration([fl], geo, tm, METHOD, num)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = ib.imogen.launch_count() - l0
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    barrier()
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * cells * args.steps / (ms_max / 1e3) / 1e6
+
+    # ---------------- per-kernel roofline (same stream, CUDA events) ----------------
+    peak, peak_kind = measured_peaks()
+    kern = {}
+    reps = max(3, min(10, args.steps))
+    for d, name in ((1, "x_row"), (2, "y_march"), (3, "z_march")):
+        dt = tm.dTime
+        ib.cudaFluidStep(fl, geo, [dt, 1, GAMMA, 1e-5, METHOD, d], num)  # warm
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        for _ in range(reps):
+            ib.cudaFluidStep(fl, geo, [dt, 1, GAMMA, 1e-5, METHOD, d], num)
+        b.record(stream)
+        torch.cuda.synchronize()
+        kern[name] = a.elapsed_time(b) / reps
+    # CFL reduction
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    tau_dev = torch.zeros(1, dtype=torch.float64, device=dev)
+    a.record(stream)
+    for _ in range(reps):
+        ib.cflTimestepFused(fl, GAMMA, geo, METHOD, tau_device=tau_dev)
+    b.record(stream)
+    torch.cuda.synchronize()
+    kern["cfl"] = a.elapsed_time(b) / reps
+    # share per iteration: 2 x-row launches, 2 y, 2 z, 1 cfl
+    share = {"x_row": 2 * kern["x_row"], "y_march": 2 * kern["y_march"], "z_march": 2 * kern["z_march"],
+             "cfl": kern["cfl"]}
+    dom = max(share, key=share.get)
+    alg_bytes = (80 if dom != "cfl" else 40) * cells
+    achieved = alg_bytes / (kern[dom] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": dom, "peak_source": peak_kind,
+                "per_kernel_ms": kern, "step_alg_bytes_per_cell": 480 + 40,
+                "step_frac": (520 * cells) / (ms_max / args.steps / 1e3) / 1e9 / peak}
+
+    # ---------------- end to end through the public API with host buffers ----------------
+    pinned_in = torch.from_numpy(q0).pin_memory()
+    pinned_out = torch.empty_like(pinned_in).pin_memory()
+    e2e_steps = max(2, min(args.steps, 10))
+    tm2 = ib.TimeManager(cfl=CFL)
+    torch.cuda.synchronize()
+    barrier()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(e2e_steps):
+        fl.q.copy_(pinned_in, non_blocking=True)
+        ib.run_iteration([fl], geo, tm2, METHOD, num)   # includes the CFL timestep read to the host
+        pinned_out.copy_(fl.q, non_blocking=True)
+    b.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = a.elapsed_time(b)
+    t2 = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+    e2e_val = world * cells * e2e_steps / (float(t2.item()) / 1e3) / 1e6
+    nbytes = 5 * slab * 8
+
+    # ---------------- CPU baseline (rank 0, N = 1 only) ----------------
+    cpu = None
+    if rank == 0 and world == 1 and os.environ.get("IMOGEN_BENCH_SKIP_CPU") != "1":
+        v, s, thr = cpu_reference_sample(shape, 1)
+        cpu = {"value": v, "unit": "Mcell-updates/s", "cores": thr, "kind": "port",
+               "sample": "1 iteration of the %dx%dx%d workload (%.1f s), oracle C restatement, OpenMP" % (*shape, s)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mcell-updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "kelvin_helmholtz_3d_hllc_fp64", "grid": list(shape), "gamma": GAMMA,
+                       "cfl": CFL, "limiter": "MC", "method": "HLLC", "time_scheme": "SSPRK2",
+                       "boundaries": "periodic", "parallelism": "replicas" if world > 1 else "single",
+                       "l2_policy": "state %.0f MB > 126 MB L2, no flush needed" % (nbytes / 1e6)},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_val, "unit": "Mcell-updates/s", "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes + 8, "steps": e2e_steps},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

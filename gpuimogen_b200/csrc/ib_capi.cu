@@ -1,0 +1,426 @@
+// ib_capi.cu -- extern "C" entry points (include/imogen_b200.h) and host orchestration.
+//
+// Host logic restated from the reference's mex glue and orchestration:
+//   ib_cudaFluidStep       <- cudaFluidStep.cu:161-227 + performFluidUpdate_1D :233-663
+//   ib_fluidstep           <- flux_ML_iface.cu:37-160 + performFluidUpdate_3D flux.cu:27-165
+//   ib_cflTimestep(Fused)  <- cflTimestep.cu:64-252, cudaSoundspeed.cu:54-150
+//   ib_freezeAndPtot       <- freezeAndPtot.cu:32-147
+//   ib_cudaStatics         <- cudaStatics.cu:85-104, 199-350
+//   ib_setFluidBoundary    <- cudaStatics.cu:112-197
+//   ib_cudaSource2FluidDrag<- cudaSource2FluidDrag.cu:125-246
+#include <cstdio>
+#include <cstring>
+#include <atomic>
+#include <mutex>
+
+#include "ib_internal.cuh"
+#include "ib_sweep_launch.cuh"
+
+namespace ib {
+
+static thread_local int g_last_cuda_error = 0;
+
+int check_cuda(cudaError_t e)
+{
+    if (e != cudaSuccess) {
+        g_last_cuda_error = (int)e;
+        return (e == cudaErrorMemoryAllocation) ? IB_ERROR_NOMEM : IB_ERROR_CUDA;
+    }
+    return IB_SUCCESSFUL;
+}
+
+static std::atomic<long long> g_launches{0};
+
+int check_launch()
+{
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return check_cuda(cudaGetLastError());
+}
+
+int num_sms()
+{
+    static int cache[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (cache[dev] == 0) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+        cache[dev] = v;
+    }
+    return cache[dev];
+}
+
+static std::mutex g_scratch_mu;
+
+Scratch &scratch()
+{
+    static Scratch per_dev[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    return per_dev[dev];
+}
+
+double *Scratch::cfl_partial(int nblocks)
+{
+    std::lock_guard<std::mutex> g(g_scratch_mu);
+    if (nblocks > partial_n_) {
+        if (partial_) cudaFree(partial_);
+        partial_ = nullptr;
+        partial_n_ = 0;
+        if (cudaMalloc(&partial_, sizeof(double) * nblocks) != cudaSuccess) return nullptr;
+        partial_n_ = nblocks;
+    }
+    return partial_;
+}
+
+unsigned int *Scratch::cfl_counter()
+{
+    std::lock_guard<std::mutex> g(g_scratch_mu);
+    if (!counter_) {
+        if (cudaMalloc(&counter_, sizeof(unsigned int)) != cudaSuccess) { counter_ = nullptr; return nullptr; }
+        if (cudaMemset(counter_, 0, sizeof(unsigned int)) != cudaSuccess) return nullptr;
+    }
+    return counter_;
+}
+
+double *Scratch::cfl_tau()
+{
+    std::lock_guard<std::mutex> g(g_scratch_mu);
+    if (!tau_) {
+        if (cudaMalloc(&tau_, sizeof(double)) != cudaSuccess) { tau_ = nullptr; return nullptr; }
+    }
+    return tau_;
+}
+
+double *Scratch::bytes(size_t nbytes)
+{
+    std::lock_guard<std::mutex> g(g_scratch_mu);
+    if (nbytes > gen_n_) {
+        if (gen_) cudaFree(gen_);
+        gen_ = nullptr;
+        gen_n_ = 0;
+        if (cudaMalloc(&gen_, nbytes) != cudaSuccess) return nullptr;
+        gen_n_ = nbytes;
+    }
+    return gen_;
+}
+
+int launch_sweep(int method, int slope, int precision, int dir, double *q, int64_t slab, const int grid[3],
+                 double lambda, double gamma, double rho_min, double c_iso, cudaStream_t st)
+{
+    if (method == IB_METHOD_HLLC) {
+        if (precision == IB_PREC_FP32_FLUX)
+            return launch_hllc32(slope, dir, q, slab, grid, lambda, gamma, rho_min, c_iso, st);
+        return launch_hllc64(slope, dir, q, slab, grid, lambda, gamma, rho_min, c_iso, st);
+    }
+    if (method == IB_METHOD_HLL) return launch_hll64(slope, dir, q, slab, grid, lambda, gamma, rho_min, c_iso, st);
+    return IB_ERROR_INVALID_ARGS;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Validation helpers
+// ---------------------------------------------------------------------------------------------
+static int validate_grid(const ib_grid &g)
+{
+    if (g.nx < 1 || g.ny < 1 || g.nz < 1) return IB_ERROR_INVALID_ARGS;
+    int64_t n = (int64_t)g.nx * g.ny * g.nz;
+    if (g.slab_pitch < n) return IB_ERROR_INVALID_ARGS;
+    if (n > ((int64_t)1 << 31)) return IB_ERROR_INVALID_ARGS;  // 32-bit cell indices in the reductions
+    return IB_SUCCESSFUL;
+}
+
+static int validate_fluid(const ib_fluid *f)
+{
+    if (!f || !f->q) return IB_ERROR_NULL_POINTER;
+    int rc = validate_grid(f->grid);
+    if (rc) return rc;
+    for (int i = 0; i < 6; i++)
+        if (f->bc[i] < IB_BC_CIRCULAR || f->bc[i] > IB_BC_FREEBALANCE) return IB_ERROR_INVALID_ARGS;
+    if (f->halo < 1 || f->halo > 8) return IB_ERROR_INVALID_ARGS;
+    return IB_SUCCESSFUL;
+}
+
+struct Numerics {
+    int slope = IB_SLOPE_OSPRE, flim = IB_FLUX_OSPRE, prec = IB_PREC_FP64;
+};
+
+static int get_numerics(const ib_numerics *num, Numerics &n)
+{
+    if (num) {
+        n.slope = num->slope_limiter;
+        n.flim = num->flux_limiter;
+        n.prec = num->precision;
+    }
+    if (n.slope < IB_SLOPE_OSPRE || n.slope > IB_SLOPE_ZERO) return IB_ERROR_INVALID_ARGS;
+    if (n.flim < IB_FLUX_OSPRE || n.flim > IB_FLUX_ZERO) return IB_ERROR_INVALID_ARGS;
+    if (n.prec != IB_PREC_FP64 && n.prec != IB_PREC_FP32_FLUX) return IB_ERROR_INVALID_ARGS;
+    return IB_SUCCESSFUL;
+}
+
+// One directional update (performFluidUpdate_1D); gamma already 2 for isothermal fluids.
+static int fluid_update_1d(ib_fluid *f, const ib_geometry *geo, int method, int dir, double dt, double gamma,
+                           double rho_min, double c_iso, const Numerics &nm, cudaStream_t st)
+{
+    const int grid[3] = {f->grid.nx, f->grid.ny, f->grid.nz};
+    if (grid[dir - 1] < 3) return IB_SUCCESSFUL;  // cudaFluidStep.cu:313
+    const double lambda = dt / geo->h[dir - 1];
+    if (method == IB_METHOD_XINJIN)
+        return launch_xj_sweep(nm.flim, dir, f->q, f->grid.slab_pitch, grid, lambda, gamma, rho_min, st);
+    return launch_sweep(method, nm.slope, nm.prec, dir, f->q, f->grid.slab_pitch, grid, lambda, gamma, rho_min, c_iso,
+                        st);
+}
+
+static bool has_statics(const ib_fluid *f)
+{
+    for (int k = 0; k < 5; k++)
+        if (f->statics[k].data && f->statics[k].count > 0) return true;
+    return false;
+}
+
+// setFluidBoundary (cudaStatics.cu:112-197): statics of the density array, then per side the
+// statics of every array followed by that side's condition.
+static int fluid_boundary(ib_fluid *f, int dir, cudaStream_t st)
+{
+    const int grid[3] = {f->grid.nx, f->grid.ny, f->grid.nz};
+    const int64_t S = f->grid.slab_pitch;
+    int rc;
+    if (!has_statics(f)) return launch_fluid_boundary(f->q, S, grid, f->bc, f->halo, dir, st);
+    if ((rc = launch_statics(f->q, &f->statics[0], st))) return rc;
+    for (int side = 0; side < 2; side++) {
+        for (int k = 0; k < 5; k++)
+            if ((rc = launch_statics(f->q + k * S, &f->statics[k], st))) return rc;
+        int32_t bc1[6];
+        memcpy(bc1, f->bc, sizeof(bc1));
+        bc1[2 * (dir - 1) + (1 - side)] = IB_BC_CIRCULAR;
+        if ((rc = launch_fluid_boundary(f->q, S, grid, bc1, f->halo, dir, st))) return rc;
+    }
+    return IB_SUCCESSFUL;
+}
+
+}  // namespace ib
+
+using namespace ib;
+
+// =============================================================================================
+// C ABI
+// =============================================================================================
+extern "C" {
+
+int64_t ib_slab_pitch(int32_t nx, int32_t ny, int32_t nz)
+{
+    int64_t n = (int64_t)nx * ny * nz;
+    return ((n + 31) / 32) * 32;
+}
+
+const char *ib_status_string(int status)
+{
+    switch (status) {
+    case IB_SUCCESSFUL: return "SUCCESSFUL";
+    case IB_ERROR_INVALID_ARGS: return "ERROR_INVALID_ARGS";
+    case IB_ERROR_CRASH: return "ERROR_CRASH";
+    case IB_ERROR_NULL_POINTER: return "ERROR_NULL_POINTER";
+    case IB_ERROR_NOIMPLEMENT: return "ERROR_NOIMPLEMENT";
+    case IB_ERROR_NOMEM: return "ERROR_NOMEM";
+    case IB_ERROR_CUDA: return "ERROR_CUDA";
+    default: return "UNKNOWN";
+    }
+}
+
+int ib_last_cuda_error(void) { return g_last_cuda_error; }
+
+long long ib_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int ib_cudaFluidStep(ib_fluid *fluid, const ib_geometry *geo, const double *params, int nparams,
+                     const ib_numerics *num, void *stream)
+{
+    int rc;
+    if (!geo || !params) return IB_ERROR_NULL_POINTER;
+    if ((rc = validate_fluid(fluid))) return rc;
+    if (nparams != 6 && nparams != 7) return IB_ERROR_INVALID_ARGS;
+    Numerics nm;
+    if ((rc = get_numerics(num, nm))) return rc;
+    if (geo->shape != 0) return IB_ERROR_NOIMPLEMENT;  // cylindrical sweeps are not built
+    const double dt = params[0];
+    const int purehydro = (int)params[1];
+    double gamma = params[2];
+    const double rho_min = params[3];
+    const int method = (int)params[4];
+    const int dir = (int)params[5];
+    double c_iso = -1;
+    if (nparams == 7) {
+        c_iso = params[6];
+        gamma = 2;
+    }
+    if (purehydro != 1) return IB_ERROR_NOIMPLEMENT;  // the MHD sweeps are dead in the reference
+    if (method < IB_METHOD_HLL || method > IB_METHOD_XINJIN || dir < 1 || dir > 3) return IB_ERROR_INVALID_ARGS;
+    return fluid_update_1d(fluid, geo, method, dir, dt, gamma, rho_min, c_iso, nm, (cudaStream_t)stream);
+}
+
+int ib_fluidstep(ib_fluid *fluids, const ib_fluid_thermo *thermo, int nfluids, const ib_geometry *geo,
+                 const double *params, int nparams, const ib_numerics *num, void *stream)
+{
+    static const int fluxcall[3][6] = {{1, 2, 1, 2, 3, 3}, {3, 1, 2, 3, 1, 2}, {2, 3, 3, 1, 2, 1}};
+    int rc;
+    if (!fluids || !thermo || !geo || !params) return IB_ERROR_NULL_POINTER;
+    if (nparams != 5 || nfluids < 1) return IB_ERROR_INVALID_ARGS;
+    Numerics nm;
+    if ((rc = get_numerics(num, nm))) return rc;
+    if (geo->shape != 0) return IB_ERROR_NOIMPLEMENT;
+    const double dt = params[0];
+    const int purehydro = (int)params[1];
+    const int sweep_dir = (int)params[2];
+    const int step_number = (int)params[3];
+    const int method = (int)params[4];
+    if (purehydro != 1) return IB_ERROR_NOIMPLEMENT;
+    if (method < IB_METHOD_HLL || method > IB_METHOD_XINJIN) return IB_ERROR_INVALID_ARGS;
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int fi = 0; fi < nfluids; fi++) {
+        ib_fluid *f = &fluids[fi];
+        if ((rc = validate_fluid(f))) return rc;
+        double gamma = thermo[fi].gamma, c_iso = thermo[fi].c_isothermal;
+        if (c_iso != -1) gamma = 2;  // flux_ML_iface.cu:140-143
+        const double rho_min = thermo[fi].rho_min;
+        const int ext[3] = {f->grid.nx, f->grid.ny, f->grid.nz};
+        if (ext[1] == 1 && ext[2] == 1) {  // flux.cu:35-68
+            if ((rc = fluid_update_1d(f, geo, method, 1, dt, gamma, rho_min, c_iso, nm, st))) return rc;
+            if ((rc = fluid_boundary(f, 1, st))) return rc;
+            continue;
+        }
+        const int sweep = (step_number + 3 * (sweep_dir > 0)) % 6;
+        for (int n = 0; n < 3; n++) {
+            const int d = fluxcall[n][(sweep + 6) % 6];
+            if (ext[d - 1] > 3) {
+                if ((rc = fluid_update_1d(f, geo, method, d, dt, gamma, rho_min, c_iso, nm, st))) return rc;
+                if ((rc = fluid_boundary(f, d, st))) return rc;
+            }
+        }
+    }
+    return IB_SUCCESSFUL;
+}
+
+int ib_cudaSoundspeed(const ib_fluid *fluid, double gamma, double *cs_out, void *stream)
+{
+    int rc;
+    if (!fluid || !cs_out) return IB_ERROR_NULL_POINTER;
+    if ((rc = validate_grid(fluid->grid))) return rc;
+    if (!fluid->q) return IB_ERROR_NULL_POINTER;
+    const int64_t n = (int64_t)fluid->grid.nx * fluid->grid.ny * fluid->grid.nz;
+    return launch_soundspeed(fluid->q, fluid->grid.slab_pitch, n, gamma, cs_out, (cudaStream_t)stream);
+}
+
+static int cfl_common(const ib_fluid *fluid, const double *cs, double gamma, const ib_geometry *geo, int method,
+                      double *tau_host, double *tau_device, void *stream)
+{
+    int rc;
+    if (!fluid || !geo || !fluid->q) return IB_ERROR_NULL_POINTER;
+    if ((rc = validate_grid(fluid->grid))) return rc;
+    if (method < IB_METHOD_HLL || method > IB_METHOD_XINJIN) return IB_ERROR_INVALID_ARGS;
+    if (geo->shape != 0) return IB_ERROR_NOIMPLEMENT;
+    if (!tau_host && !tau_device) return IB_ERROR_NULL_POINTER;
+    cudaStream_t st = (cudaStream_t)stream;
+    double *tau = tau_device ? tau_device : scratch().cfl_tau();
+    if (!tau) return IB_ERROR_NOMEM;
+    const int grid[3] = {fluid->grid.nx, fluid->grid.ny, fluid->grid.nz};
+    if ((rc = launch_cfl(fluid->q, cs, fluid->grid.slab_pitch, grid, geo, method, gamma, tau, st))) return rc;
+    if (tau_host) {
+        if ((rc = check_cuda(cudaMemcpyAsync(tau_host, tau, sizeof(double), cudaMemcpyDeviceToHost, st)))) return rc;
+        if ((rc = check_cuda(cudaStreamSynchronize(st)))) return rc;
+    }
+    return IB_SUCCESSFUL;
+}
+
+int ib_cflTimestep(const ib_fluid *fluid, const double *cs, const ib_geometry *geo, int method, double *tau_host,
+                   void *stream)
+{
+    if (!cs || !tau_host) return IB_ERROR_NULL_POINTER;
+    return cfl_common(fluid, cs, 0.0, geo, method, tau_host, nullptr, stream);
+}
+
+int ib_cflTimestepFused(const ib_fluid *fluid, double gamma, const ib_geometry *geo, int method, double *tau_host,
+                        double *tau_device, void *stream)
+{
+    return cfl_common(fluid, nullptr, gamma, geo, method, tau_host, tau_device, stream);
+}
+
+int ib_freezeAndPtot(ib_fluid *fluid, double gamma, int purehydro, double cs_min, double *ptot, double *freeze,
+                     void *stream)
+{
+    int rc;
+    if (!fluid || !fluid->q || !ptot || !freeze) return IB_ERROR_NULL_POINTER;
+    if ((rc = validate_grid(fluid->grid))) return rc;
+    if (purehydro != 1) return IB_ERROR_NOIMPLEMENT;
+    const int grid[3] = {fluid->grid.nx, fluid->grid.ny, fluid->grid.nz};
+    return launch_freeze_ptot(fluid->q, fluid->grid.slab_pitch, grid, gamma, cs_min, ptot, freeze,
+                              (cudaStream_t)stream);
+}
+
+int ib_cudaStatics(double *phi, const ib_grid *grid, const int32_t bc[6], int halo, int vector_component,
+                   const ib_statics *statics, int direction, void *stream)
+{
+    int rc;
+    if (!phi || !grid || !bc) return IB_ERROR_NULL_POINTER;
+    if ((rc = validate_grid(*grid))) return rc;
+    if (direction < 1 || direction > 3 || halo < 1 || halo > 8) return IB_ERROR_INVALID_ARGS;
+    if (vector_component < 0 || vector_component > 3) return IB_ERROR_INVALID_ARGS;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int g3[3] = {grid->nx, grid->ny, grid->nz};
+    for (int side = 0; side < 2; side++) {
+        if ((rc = launch_statics(phi, statics, st))) return rc;
+        const int mode = bc[2 * (direction - 1) + side];
+        if (mode == IB_BC_OUTFLOW) {
+            int32_t bc1[6] = {IB_BC_CIRCULAR, IB_BC_CIRCULAR, IB_BC_CIRCULAR,
+                              IB_BC_CIRCULAR, IB_BC_CIRCULAR, IB_BC_CIRCULAR};
+            bc1[2 * (direction - 1) + side] = IB_BC_OUTFLOW;
+            rc = launch_fluid_boundary(phi, grid->slab_pitch, g3, bc1, halo, direction, st);
+        } else {
+            rc = launch_array_boundary(phi, g3, mode, direction, side, vector_component, halo, st);
+        }
+        if (rc) return rc;
+    }
+    return IB_SUCCESSFUL;
+}
+
+int ib_setFluidBoundary(ib_fluid *fluid, int direction, void *stream)
+{
+    int rc;
+    if ((rc = validate_fluid(fluid))) return rc;
+    if (direction < 1 || direction > 3) return IB_ERROR_INVALID_ARGS;
+    return fluid_boundary(fluid, direction, (cudaStream_t)stream);
+}
+
+int ib_cudaSource2FluidDrag(ib_fluid *gas, ib_fluid *dust, const ib_thermo *tg, const ib_thermo *td,
+                            const ib_geometry *geo, const double *params, int nparams, void *stream)
+{
+    int rc;
+    if (!gas || !dust || !tg || !td || !params || !gas->q || !dust->q) return IB_ERROR_NULL_POINTER;
+    if (nparams != 2) return IB_ERROR_INVALID_ARGS;  // cudaSource2FluidDrag.cu:157-163
+    if ((rc = validate_grid(gas->grid))) return rc;
+    if (gas->grid.nx != dust->grid.nx || gas->grid.ny != dust->grid.ny || gas->grid.nz != dust->grid.nz ||
+        gas->grid.slab_pitch != dust->grid.slab_pitch)
+        return IB_ERROR_INVALID_ARGS;
+    (void)geo;
+    const double dt = params[0];
+    const int method = (int)params[1];
+    if (method < IB_DRAG_EMP || method > IB_DRAG_LOGTRAP3) return IB_ERROR_INVALID_ARGS;
+    // drag constants (cudaSource2FluidDrag.cu:196-218)
+    double dp[11];
+    const double gam = tg->gamma;
+    const double ddust = sqrt(td->sigma0 / 3.141592653589793);
+    dp[0] = tg->mu0;
+    dp[1] = -tg->mu_t_index;
+    dp[2] = tg->sigma_t_index;
+    dp[3] = tg->mass * (gam - 1.0) / (298.15 * tg->k_bolt);
+    dp[4] = sqrt(2.0) * tg->mass / (tg->sigma0 * ddust);
+    dp[5] = ddust / tg->mu0;
+    dp[6] = td->sigma0 / (1.0 * td->mass);
+    dp[7] = dt;
+    dp[8] = (gam - 1.0);
+    dp[9] = .25 * td->sigma0 / td->mass;
+    dp[10] = 16 * (gam - 1.0) / 3.0;
+    const int64_t n = (int64_t)gas->grid.nx * gas->grid.ny * gas->grid.nz;
+    return launch_drag(gas->q, dust->q, gas->grid.slab_pitch, n, dp, dt, method, (cudaStream_t)stream);
+}
+
+}  // extern "C"

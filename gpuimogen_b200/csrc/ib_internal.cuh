@@ -1,0 +1,55 @@
+// ib_internal.cuh -- host-side plumbing shared by the library's translation units.
+#pragma once
+
+#include <algorithm>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "ib_common.cuh"
+
+namespace ib {
+
+// Records the last CUDA error and maps it to the library's status codes.
+int check_cuda(cudaError_t e);
+int check_launch();
+int num_sms();
+
+// Reusable per-device scratch: grown on demand, never shrunk, freed at process exit.  The
+// reference allocates and frees a 6-slab temporary per call (cudaFluidStep.cu:508-513); the
+// fused sweeps here need none, only the reductions and the Xin-Jin pencils use this.
+class Scratch {
+public:
+    double *cfl_partial(int nblocks);
+    unsigned int *cfl_counter();
+    double *cfl_tau();
+    double *bytes(size_t nbytes);  // general scratch (reused between calls on the device)
+
+private:
+    double *partial_ = nullptr;
+    int partial_n_ = 0;
+    unsigned int *counter_ = nullptr;
+    double *tau_ = nullptr;
+    double *gen_ = nullptr;
+    size_t gen_n_ = 0;
+};
+Scratch &scratch();
+
+// Launchers (return IB_* status)
+int launch_sweep(int method, int slope, int precision, int dir, double *q, int64_t slab, const int grid[3],
+                 double lambda, double gamma, double rho_min, double c_iso, cudaStream_t st);
+int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
+                    double rho_min, cudaStream_t st);
+int launch_cfl(const double *q, const double *cs, int64_t slab, const int grid[3], const ib_geometry *geo,
+               int method, double gamma, double *tau_dev, cudaStream_t st);
+int launch_soundspeed(const double *q, int64_t slab, int64_t n, double gamma, double *cs, cudaStream_t st);
+int launch_freeze_ptot(double *q, int64_t slab, const int grid[3], double gamma, double cs_min, double *ptot,
+                       double *freeze, cudaStream_t st);
+int launch_fluid_boundary(double *q, int64_t slab, const int grid[3], const int32_t bc[6], int halo, int dir,
+                          cudaStream_t st);
+int launch_array_boundary(double *phi, const int grid[3], int mode, int dir, int side, int vec_component, int halo,
+                          cudaStream_t st);
+int launch_statics(double *phi, const ib_statics *st_list, cudaStream_t st);
+int launch_drag(double *gas, double *dust, int64_t slab, int64_t n, const double dp[11], double dt, int method,
+                cudaStream_t st);
+
+}  // namespace ib

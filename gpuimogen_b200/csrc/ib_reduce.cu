@@ -1,0 +1,218 @@
+// ib_reduce.cu -- soundspeed, CFL timestep reduction and freezeAndPtot.
+//
+// The reference computes the CFL limit in three steps: a soundspeed pass that writes c_s
+// (gpuclass/cudaSoundspeed.cu:178-193), a reduction kernel that reads the fluid and c_s and
+// leaves at most 128 block minima in pinned host memory (cflTimestep.cu:276-377), then a host
+// loop, MPI_Allreduce and the HLL/HLLC halving (:204-237).  Here the fused variant computes c_s
+// inline, reduces with warp shuffles, and the last block to finish folds the block minima and
+// applies the halving on the device, so the timestep can stay on the GPU.
+#include "ib_internal.cuh"
+
+namespace ib {
+
+// c_s^2 = gamma(gamma-1)(E - p^2/2rho)/rho, clamped at 0 (cudaSoundspeed.cu:184-191)
+__device__ __forceinline__ double soundspeed_cell(double rho, double E, double px, double py, double pz, double gg1)
+{
+    double rhoinv = 1 / rho;
+    double csq = gg1 * (E - .5 * (px * px + py * py + pz * pz) * rhoinv) * rhoinv;
+    if (csq < 0.0) csq = 0.0;
+    return sqrt(csq);
+}
+
+__global__ void soundspeed_kernel(const double *__restrict__ q, int64_t slab, int64_t n, double gg1,
+                                  double *__restrict__ cs)
+{
+    for (int64_t x = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; x < n; x += (int64_t)blockDim.x * gridDim.x) {
+        cs[x] = soundspeed_cell(q[x], q[x + slab], q[x + 2 * slab], q[x + 3 * slab], q[x + 4 * slab], gg1);
+    }
+}
+
+// Signal-crossing time of one cell (cflTimestep.cu:254-340).  sim = spatial dimension.
+template <int SIM, bool XJ>
+__device__ __forceinline__ double cfl_cell(double rho, double px, double py, double pz, double cs, double hmin,
+                                           double hx, double hy, double hz)
+{
+    double u;
+    if constexpr (!XJ) {
+        double p;
+        if constexpr (SIM == 1) {
+            p = fabs(px);
+        } else {
+            double pp = px * px;
+            pp = pp + py * py;
+            if constexpr (SIM > 2) pp = pp + pz * pz;
+            p = sqrt(pp);
+        }
+        u = p / rho + cs;
+        u = hmin / u;
+    } else {
+        double v;
+        u = hx / (fabs(px) / rho + cs);
+        v = hy / (fabs(py) / rho + cs);
+        u = (u < v) ? u : v;
+        if constexpr (SIM > 2) {
+            v = hz / (fabs(pz) / rho + cs);
+            u = (u < v) ? u : v;
+        }
+    }
+    return u;
+}
+
+// NaN-ignoring minimum, as the reference's ternaries: a NaN candidate never replaces the running value
+__device__ __forceinline__ double min_keep(double cur, double cand) { return (cand < cur) ? cand : cur; }
+
+template <int SIM, bool XJ, bool FUSED>
+__global__ void __launch_bounds__(256) cfl_kernel(const double *__restrict__ q, const double *__restrict__ cs_in,
+                                                  int64_t slab, int64_t n, double gg1, double hmin, double hx,
+                                                  double hy, double hz, int halve, double *__restrict__ partial,
+                                                  unsigned int *__restrict__ counter, double *__restrict__ tau_out)
+{
+    double tmin = 1e37;
+    for (int64_t x = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; x < n; x += (int64_t)blockDim.x * gridDim.x) {
+        double rho = q[x], px = q[x + 2 * slab], py = 0, pz = 0;
+        if (SIM > 1 || XJ) py = q[x + 3 * slab];
+        if (SIM > 2 || XJ) pz = q[x + 4 * slab];
+        double cs;
+        if constexpr (FUSED) {
+            cs = soundspeed_cell(rho, q[x + slab], px, q[x + 3 * slab], q[x + 4 * slab], gg1);
+        } else {
+            cs = cs_in[x];
+        }
+        tmin = min_keep(tmin, cfl_cell<SIM, XJ>(rho, px, py, pz, cs, hmin, hx, hy, hz));
+    }
+    // warp then block reduction
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tmin = min_keep(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
+    __shared__ double wmin[8];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) wmin[wid] = tmin;
+    __syncthreads();
+    if (wid == 0) {
+        tmin = (lane < (int)(blockDim.x >> 5)) ? wmin[lane] : 1e37;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) tmin = min_keep(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
+        if (lane == 0) {
+            partial[blockIdx.x] = tmin;
+            __threadfence();
+            unsigned int done = atomicAdd(counter, 1u);
+            last = (done == gridDim.x - 1);
+        }
+    }
+    __syncthreads();
+    if (last) {
+        // final fold of the block minima by the last block (reads see all blocks' writes after
+        // their fences and the counter)
+        __threadfence();
+        double m = 1e37;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) m = min_keep(m, ((volatile double *)partial)[b]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = min_keep(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0) wmin[wid] = m;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double r = 1e38;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) r = (wmin[w] < r) ? wmin[w] : r;
+            if (halve) r = r / 2;  // HLL/HLLC (cflTimestep.cu:232-237)
+            *tau_out = r;
+            *counter = 0u;  // ready for the next call on this stream
+        }
+    }
+}
+
+int launch_cfl(const double *q, const double *cs, int64_t slab, const int grid[3], const ib_geometry *geo,
+               int method, double gamma, double *tau_dev, cudaStream_t st)
+{
+    int sim = 1;
+    if (geo->global_rez[1] > 1) sim = 2;
+    if (geo->global_rez[2] > 1) sim = 3;
+    const bool xj = (method == IB_METHOD_XINJIN) && (sim > 1);  // 1-D XJ uses the HLL kernel
+    double hmin = geo->h[0];
+    if (sim > 1 && geo->h[1] < hmin) hmin = geo->h[1];
+    if (sim > 2 && geo->h[2] < hmin) hmin = geo->h[2];
+    int64_t n = (int64_t)grid[0] * grid[1] * grid[2];
+    int nb = (int)std::min<int64_t>((n + 255) / 256, (int64_t)4 * num_sms());
+    if (nb < 1) nb = 1;
+    Scratch &sc = scratch();
+    double *partial = sc.cfl_partial(nb);
+    unsigned int *counter = sc.cfl_counter();
+    if (!partial || !counter) return IB_ERROR_NOMEM;
+    int halve = (method == IB_METHOD_HLL || method == IB_METHOD_HLLC) ? 1 : 0;
+    double gg1 = gamma * (gamma - 1);
+    bool fused = (cs == nullptr);
+#define IB_CFL_LAUNCH(S, X, F)                                                                            \
+    cfl_kernel<S, X, F><<<nb, 256, 0, st>>>(q, cs, slab, n, gg1, hmin, geo->h[0], geo->h[1], geo->h[2], halve, \
+                                            partial, counter, tau_dev)
+    if (fused) {
+        if (xj) { if (sim == 2) IB_CFL_LAUNCH(2, true, true); else IB_CFL_LAUNCH(3, true, true); }
+        else if (sim == 1) IB_CFL_LAUNCH(1, false, true);
+        else if (sim == 2) IB_CFL_LAUNCH(2, false, true);
+        else IB_CFL_LAUNCH(3, false, true);
+    } else {
+        if (xj) { if (sim == 2) IB_CFL_LAUNCH(2, true, false); else IB_CFL_LAUNCH(3, true, false); }
+        else if (sim == 1) IB_CFL_LAUNCH(1, false, false);
+        else if (sim == 2) IB_CFL_LAUNCH(2, false, false);
+        else IB_CFL_LAUNCH(3, false, false);
+    }
+#undef IB_CFL_LAUNCH
+    return check_launch();
+}
+
+int launch_soundspeed(const double *q, int64_t slab, int64_t n, double gamma, double *cs, cudaStream_t st)
+{
+    int nb = (int)std::min<int64_t>((n + 255) / 256, (int64_t)8 * num_sms());
+    if (nb < 1) nb = 1;
+    soundspeed_kernel<<<nb, 256, 0, st>>>(q, slab, n, gamma * (gamma - 1), cs);
+    return check_launch();
+}
+
+// ------------------------------------------------------------------------------------------
+// freezeAndPtot, hydro (cukern_FreezeSpeed_hydro, freezeAndPtot.cu:229-290): one warp-multiple
+// block per x row.
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) freeze_ptot_kernel(double *__restrict__ q, int64_t slab, int nx, double gam,
+                                                          double gm1, double cs0sq, double *__restrict__ ptot,
+                                                          double *__restrict__ freeze)
+{
+    const int64_t row = blockIdx.x;
+    double *rho = q + row * nx, *E = rho + slab, *px = rho + 2 * slab, *py = rho + 3 * slab, *pz = rho + 4 * slab;
+    double *pt = ptot + row * nx;
+    double CsMax = 0.0;
+    for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+        double rhoinv = 1.0 / rho[x];
+        double psqhf = .5 * (px[x] * px[x] + py[x] * py[x] + pz[x] * pz[x]);
+        double P = gm1 * (E[x] - psqhf * rhoinv);
+        if (gam * P * rhoinv < cs0sq) {
+            P = cs0sq / (gam * rhoinv);
+            E[x] = psqhf * rhoinv + P / gm1;
+        }
+        pt[x] = P;
+        double Cs = sqrt(gam * P * rhoinv) + fabs(px[x] * rhoinv);
+        if (Cs > CsMax) CsMax = Cs;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        double v = __shfl_xor_sync(0xffffffffu, CsMax, o);
+        if (v > CsMax) CsMax = v;
+    }
+    __shared__ double wm[4];
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = CsMax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = wm[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) if (wm[w] > m) m = wm[w];
+        freeze[row] = m;
+    }
+}
+
+int launch_freeze_ptot(double *q, int64_t slab, const int grid[3], double gamma, double cs_min, double *ptot,
+                       double *freeze, cudaStream_t st)
+{
+    int64_t rows = (int64_t)grid[1] * grid[2];
+    if (rows <= 0) return IB_SUCCESSFUL;
+    freeze_ptot_kernel<<<(unsigned)rows, 128, 0, st>>>(q, slab, grid[0], gamma, gamma - 1.0, cs_min * cs_min, ptot,
+                                                      freeze);
+    return check_launch();
+}
+
+}  // namespace ib

@@ -1,0 +1,467 @@
+// ib_sweep.cuh -- fused SSPRK2 directional sweep kernels (HLLC, HLL) without transposes.
+//
+// The reference runs each sweep as two kernels (stage A into a 6-slab temporary, stage B
+// back into the fluid) along memory x, after transposing the arrays so that the swept axis is
+// fastest (gpuclass/flux.cu:46-49, cudaArrayRotateB.cu).  Each stage's value at cell i depends
+// only on cells i-2..i+2 of the row, periodically wrapped (cudaFluidStep.cu:1157-1162), so here
+// both stages run in one kernel straight on the XYZ arrays:
+//
+//  * row kernel (x sweeps, rows up to 1024 cells): one CTA holds one whole periodic row, one
+//    thread per cell (or two), neighbours exchanged through two shared-memory planes;
+//    coalesced loads and stores, no halo recomputation.
+//  * march kernel (y and z sweeps; x sweeps of longer rows): one thread marches along a chunk
+//    of one pencil keeping a sliding window of the stencil in registers, lanes of a warp on
+//    neighbouring pencils so every load and store is a full 256-byte line.  All chunks of a
+//    pencil live in the same CTA: each chunk defers writing its first four outputs until
+//    every chunk has finished reading (they are its left neighbour's right halo) and writes
+//    its others only after a barrier that follows every chunk's reads of its left halo.
+#pragma once
+
+#include "ib_common.cuh"
+
+namespace ib {
+
+// ------------------------------------------------------------------------------------------
+// Stage helpers shared by both kernels
+// ------------------------------------------------------------------------------------------
+template <typename FT>
+__device__ __forceinline__ V5<FT> v5_sub(const V5<FT> &a, const V5<FT> &b)
+{
+    V5<FT> r;
+#pragma unroll
+    for (int k = 0; k < 5; k++) r.a[k] = a.a[k] - b.a[k];
+    return r;
+}
+
+// HLL primitives: [rho, v_n, P, v_t1, v_t2] with P taken from the floored pressure
+// (cudaFluidStep.cu:1864-1888)
+template <typename FT>
+__device__ __forceinline__ V5<FT> hll_prims(FT rho, FT pn, FT P, FT pt1, FT pt2)
+{
+    V5<FT> w;
+    w.a[0] = rho;
+    w.a[1] = pn / rho;
+    w.a[2] = P;
+    w.a[3] = pt1 / rho;
+    w.a[4] = pt2 / rho;
+    return w;
+}
+
+template <int SLOPE, typename FT>
+__device__ __forceinline__ void hll_faces(const V5<FT> &w, const V5<FT> &dl, const V5<FT> &dr,
+                                          V5<FT> &L, V5<FT> &R)
+{
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        FT s = slope_limit<SLOPE, FT>(dl.a[k], dr.a[k]);
+        R.a[k] = w.a[k] + s;
+        L.a[k] = w.a[k] - s;
+    }
+}
+
+// HLL flux (cudaFluidStep.cu:2057-2198).  le = right face of the left cell, re = left face of
+// the right cell, both [rho, v_n, P, v_t1, v_t2].  Output [rho, E, p_n, p_t1, p_t2].
+template <typename FT>
+__device__ __forceinline__ V5<FT> hll_flux(const FluidConsts<FT> &c, const V5<FT> &le, const V5<FT> &re)
+{
+    const FT Ale = le.a[0], Ble = le.a[1], Cle = le.a[2], Dle = le.a[3], Ele = le.a[4];
+    const FT Are = re.a[0], Bre = re.a[1], Cre = re.a[2], Dre = re.a[3], Ere = re.a[4];
+    FT Utilde = (Bre - Ble), Sleft = (Dre - Dle), Sright = (Ere - Ele);
+    FT sl, sr;
+    const bool iso = !(c.isotemp == (FT)-1);
+    if (!iso) {
+        einfeldt<FT>(c, Ale, Ble, Cle, Are, Bre, Cre, Utilde * Utilde + Sleft * Sleft + Sright * Sright, sl, sr);
+    } else {
+        // the isothermal bound receives c_iso^2 where a speed is expected (cudaFluidStep.cu:2131)
+        einfeldt_iso<FT>(Ale, Ble, Are, Bre, c.isotempsq, sl, sr);
+    }
+    Sleft = sl;
+    Sright = sr;
+    FT Atilde = 1 / (Sright - Sleft);
+    FT Fa = Ale * Ble;
+    FT Fb = Are * Bre;
+    V5<FT> f;
+    int mode = 1;
+    if (Sleft >= 0) mode = 0;
+    if (Sright <= 0) mode = 2;
+    if (mode == 0) {
+        f.a[0] = Fa;
+        if (!iso) {
+            f.a[1] = Ble * (c.govergm1 * Cle + (FT).5 * Ale * (Ble * Ble + Dle * Dle + Ele * Ele));
+            f.a[2] = Fa * Ble + Cle;
+        } else {
+            f.a[1] = Ble * (Cle + (FT).5 * Ale * (Ble * Ble + Dle * Dle + Ele * Ele));
+            f.a[2] = Fa * Ble + c.isotempsq * Ale;
+        }
+        f.a[3] = Fa * Dle;
+        f.a[4] = Fa * Ele;
+    } else if (mode == 1) {
+        f.a[0] = (Sright * (Ble - Sleft) * Ale - Sleft * (Bre - Sright) * Are) * Atilde;
+        if (!iso) {
+            f.a[2] = (Sright * (Ble - Sleft) * Fa - Sleft * (Bre - Sright) * Fb + Sright * Cle - Sleft * Cre) * Atilde;
+        } else {
+            f.a[2] = (Sright * (Ble - Sleft) * Fa - Sleft * (Bre - Sright) * Fb +
+                      c.isotempsq * (Sright * Ale - Sleft * Are)) * Atilde;
+        }
+        f.a[3] = (Sright * (Ble - Sleft) * Ale * Dle - Sleft * (Bre - Sright) * Are * Dre) * Atilde;
+        f.a[4] = (Sright * (Ble - Sleft) * Ale * Ele - Sleft * (Bre - Sright) * Are * Ere) * Atilde;
+        if (!iso) {
+            Fa = (FT).5 * Ale * (Ble * Ble + Dle * Dle + Ele * Ele);
+            Fb = (FT).5 * Are * (Bre * Bre + Dre * Dre + Ere * Ere);
+            FT e = (Sright * (Ble - Sleft) * Fa - Sleft * (Bre - Sright) * Fb);
+            f.a[1] = (e + (c.govergm1 * (Sright * Cle * Ble - Sleft * Cre * Bre) + Sleft * Sright * (Cre - Cle) / c.gm1)) * Atilde;
+        } else {
+            // isothermal energy flux lacks the 1/(S_R-S_L) factor (cudaFluidStep.cu:2178-2182)
+            Fa = (FT).5 * Ale * (Ble * Ble + Dle * Dle + Ele * Ele) + Cle;
+            Fb = (FT).5 * Are * (Bre * Bre + Dre * Dre + Ere * Ere) + Cre;
+            f.a[1] = (Sright * (Ble - Sleft) * Fa - Sleft * (Bre - Sright) * Fb);
+        }
+    } else {
+        f.a[0] = Fb;
+        if (!iso) {
+            f.a[1] = Bre * (c.govergm1 * Cre + (FT).5 * Are * (Bre * Bre + Dre * Dre + Ere * Ere));
+            f.a[2] = Fb * Bre + Cre;
+        } else {
+            f.a[1] = Bre * (Cre + (FT).5 * Are * (Bre * Bre + Dre * Dre + Ere * Ere));
+            f.a[2] = Fb * Bre + c.isotemp * Are;  // c_iso, not c_iso^2 (cudaFluidStep.cu:2191)
+        }
+        f.a[3] = Fb * Dre;
+        f.a[4] = Fb * Ere;
+    }
+    return f;
+}
+
+// HLL pressure solver with floors (cukern_PressureSolverHydro, cudaFluidStep.cu:2813-2864) on a
+// conserved state in local order u = [rho, E, p_n, p_t1, p_t2]; mom[m] = local index of memory
+// slab 2+m (the reference sums px, py, pz in slab order).  Returns P, modifies u.
+template <int DIR>
+__device__ __forceinline__ double hll_pressure(double u[5], double minmass, double mintemp, double gm1)
+{
+    // local index of memory slabs 2,3,4 under HllSlots<DIR>
+    constexpr int m2 = (HllSlots<DIR>::n == 2) ? 2 : ((HllSlots<DIR>::t1 == 2) ? 3 : 4);
+    constexpr int m3 = (HllSlots<DIR>::n == 3) ? 2 : ((HllSlots<DIR>::t1 == 3) ? 3 : 4);
+    constexpr int m4 = (HllSlots<DIR>::n == 4) ? 2 : ((HllSlots<DIR>::t1 == 4) ? 3 : 4);
+    double rho = u[0], E, z, momsq, P;
+    if (rho < minmass) {
+        P = minmass / rho;
+        rho = u[0] = minmass;
+        E = u[1] = P * u[1];
+        z = u[m2] = P * u[m2];
+        momsq = z * z;
+        z = u[m3] = P * u[m3];
+        momsq += z * z;
+        z = u[m4] = P * u[m4];
+        momsq += z * z;
+    } else {
+        E = u[1];
+        z = u[m2];
+        momsq = z * z;
+        z = u[m3];
+        momsq += z * z;
+        z = u[m4];
+        momsq += z * z;
+    }
+    P = E - .5 * momsq / rho;
+    if (P < rho * mintemp) {
+        P = mintemp * rho;
+        u[1] = (.5 * momsq / rho) + P;
+    }
+    return P * gm1;
+}
+
+// Local component k of a sweep along DIR -> memory slab
+template <int METHOD, int DIR>
+__device__ __forceinline__ constexpr int slot_of(int k)
+{
+    if (k < 2) return k;
+    if constexpr (METHOD == IB_METHOD_HLLC) {
+        return k == 2 ? HllcSlots<DIR>::n : (k == 3 ? HllcSlots<DIR>::t1 : HllcSlots<DIR>::t2);
+    } else {
+        return k == 2 ? HllSlots<DIR>::n : (k == 3 ? HllSlots<DIR>::t1 : HllSlots<DIR>::t2);
+    }
+}
+
+// Per-cell stage "prims" for either method.  For HLL the floors are applied to u first.
+template <int METHOD, int DIR, typename FT>
+__device__ __forceinline__ V5<FT> stage_prims(double u[5], const FluidConsts<FT> &c)
+{
+    if constexpr (METHOD == IB_METHOD_HLLC) {
+        return hllc_prims<FT>((FT)u[0], (FT)u[1], (FT)u[2], (FT)u[3], (FT)u[4]);
+    } else {
+        double P = hll_pressure<DIR>(u, c.minmass, c.mintemp, (double)c.gm1);
+        return hll_prims<FT>((FT)u[0], (FT)u[2], (FT)P, (FT)u[3], (FT)u[4]);
+    }
+}
+
+template <int METHOD, int SLOPE, typename FT>
+__device__ __forceinline__ void stage_faces(const FluidConsts<FT> &c, const V5<FT> &w, const V5<FT> &dl,
+                                            const V5<FT> &dr, V5<FT> &L, V5<FT> &R)
+{
+    if constexpr (METHOD == IB_METHOD_HLLC) hllc_faces<SLOPE, FT>(c, w, dl, dr, L, R);
+    else hll_faces<SLOPE, FT>(w, dl, dr, L, R);
+}
+
+template <int METHOD, typename FT>
+__device__ __forceinline__ V5<FT> stage_flux(const FluidConsts<FT> &c, const V5<FT> &l, const V5<FT> &r)
+{
+    if constexpr (METHOD == IB_METHOD_HLLC) return hllc_flux<FT>(c, l, r);
+    else return hll_flux<FT>(c, l, r);
+}
+
+struct SweepArgs {
+    double *q;
+    int64_t slab;
+    int nx, ny, nz;
+    double lambda;
+};
+
+// ------------------------------------------------------------------------------------------
+// Row kernel: one CTA per x row (nx <= CPT*blockDim.x), periodic in shared memory.
+// Dynamic shared memory: 2 planes x 5 components x nx elements of FT.
+// ------------------------------------------------------------------------------------------
+template <int METHOD, int SLOPE, typename FT, int CPT>
+__global__ void __launch_bounds__(512) sweep_row_kernel(SweepArgs a, FluidConsts<FT> c)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FT *SA = reinterpret_cast<FT *>(smem_raw);
+    FT *SB = SA + 5 * a.nx;
+    const int n = a.nx;
+    const int64_t row = blockIdx.x;
+    double *q = a.q + row * n;
+    const int64_t S = a.slab;
+    const double lambda = a.lambda;
+
+    double u0[CPT][5], u1[CPT][5];
+    V5<FT> keep[CPT];  // right faces, later fluxes
+    bool act[CPT];
+#pragma unroll
+    for (int m = 0; m < CPT; m++) {
+        int i = threadIdx.x + m * blockDim.x;
+        act[m] = i < n;
+#pragma unroll
+        for (int k = 0; k < 5; k++) u0[m][k] = act[m] ? q[(int64_t)slot_of<METHOD, 1>(k) * S + i] : 1.0;
+    }
+
+#pragma unroll
+    for (int stage = 0; stage < 2; stage++) {
+        double (*u)[5] = (stage == 0) ? u0 : u1;
+        // (a) primitives -> SA
+#pragma unroll
+        for (int m = 0; m < CPT; m++) {
+            int i = threadIdx.x + m * blockDim.x;
+            if (act[m]) {
+                V5<FT> w = stage_prims<METHOD, 1, FT>(u[m], c);
+#pragma unroll
+                for (int k = 0; k < 5; k++) SA[k * n + i] = w.a[k];
+            }
+        }
+        __syncthreads();
+        // (b) limited faces; left faces -> SB, right faces kept
+#pragma unroll
+        for (int m = 0; m < CPT; m++) {
+            int i = threadIdx.x + m * blockDim.x;
+            if (act[m]) {
+                int il = (i == 0) ? n - 1 : i - 1, ir = (i == n - 1) ? 0 : i + 1;
+                V5<FT> w, dl, dr, L;
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    w.a[k] = SA[k * n + i];
+                    dl.a[k] = w.a[k] - SA[k * n + il];
+                    dr.a[k] = SA[k * n + ir] - w.a[k];
+                }
+                stage_faces<METHOD, SLOPE, FT>(c, w, dl, dr, L, keep[m]);
+#pragma unroll
+                for (int k = 0; k < 5; k++) SB[k * n + i] = L.a[k];
+            }
+        }
+        __syncthreads();
+        // (c) flux through face i+1/2 -> SA
+#pragma unroll
+        for (int m = 0; m < CPT; m++) {
+            int i = threadIdx.x + m * blockDim.x;
+            if (act[m]) {
+                int ir = (i == n - 1) ? 0 : i + 1;
+                V5<FT> Lr;
+#pragma unroll
+                for (int k = 0; k < 5; k++) Lr.a[k] = SB[k * n + ir];
+                keep[m] = stage_flux<METHOD, FT>(c, keep[m], Lr);
+#pragma unroll
+                for (int k = 0; k < 5; k++) SA[k * n + i] = keep[m].a[k];
+            }
+        }
+        __syncthreads();
+        // (d) conservative update
+#pragma unroll
+        for (int m = 0; m < CPT; m++) {
+            int i = threadIdx.x + m * blockDim.x;
+            if (act[m]) {
+                int il = (i == 0) ? n - 1 : i - 1;
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    double df = (double)keep[m].a[k] - (double)SA[k * n + il];
+                    if (stage == 0) u1[m][k] = u0[m][k] - lambda * df;
+                    else u1[m][k] = .5 * (u1[m][k] + u0[m][k] - lambda * df);
+                }
+            }
+        }
+        if (stage == 0) __syncthreads();
+    }
+#pragma unroll
+    for (int m = 0; m < CPT; m++) {
+        int i = threadIdx.x + m * blockDim.x;
+        if (act[m]) {
+#pragma unroll
+            for (int k = 0; k < 5; k++) q[(int64_t)slot_of<METHOD, 1>(k) * S + i] = u1[m][k];
+        }
+    }
+}
+
+// The HLL corrector adds (fluid after the floors of the predictor's pressure pass) and
+// (predicted state after its own floors): u0 above already holds the floored fluid because
+// stage_prims floors u in place, and u1 holds the floored prediction.  Both match the
+// reference, whose pressure passes write the floors back to memory before each stage.
+
+// ------------------------------------------------------------------------------------------
+// March kernel: blockDim = (PW pencils, C chunks); chunk c of pencil p covers cells
+// [c*L, min((c+1)*L, n)).  Shared memory: deferred first-four outputs, 20 doubles per thread.
+// ------------------------------------------------------------------------------------------
+struct MarchArgs {
+    double *q;
+    int64_t slab;
+    int nx, ny, nz;
+    int n;            // pencil length
+    int64_t npencil;
+    int L;            // chunk length
+    double lambda;
+};
+
+__device__ __forceinline__ int mod_n(int j, int n)
+{
+    int r = j % n;
+    return r < 0 ? r + n : r;
+}
+
+template <int METHOD, int SLOPE, typename FT, int DIR>
+__global__ void __launch_bounds__(256) sweep_march_kernel(MarchArgs a, FluidConsts<FT> c)
+{
+    extern __shared__ __align__(16) double defer[];  // [20][blockDim.x*blockDim.y]
+    const int nthr = blockDim.x * blockDim.y;
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int chunk = threadIdx.y;
+    const int n = a.n;
+    const bool live_p = p < a.npencil;
+    const int j0 = chunk * a.L;
+    const int j1 = min(j0 + a.L, n);
+    const bool live = live_p && (j0 < n);
+    const int64_t S = a.slab;
+    const double lambda = a.lambda;
+
+    int64_t base, stride;
+    if (DIR == 1) { base = p * a.nx; stride = 1; }
+    else if (DIR == 2) { base = (p % a.nx) + (int64_t)a.nx * a.ny * (p / a.nx); stride = a.nx; }
+    else { base = p; stride = (int64_t)a.nx * a.ny; }
+    double *q = a.q + (live ? base : 0);
+
+    constexpr int s0 = slot_of<METHOD, DIR>(0), s1 = slot_of<METHOD, DIR>(1), s2 = slot_of<METHOD, DIR>(2),
+                  s3 = slot_of<METHOD, DIR>(3), s4 = slot_of<METHOD, DIR>(4);
+
+    // sliding windows
+    V5<FT> wA, dA, RA, FA;      // stage A: prims j-1, diff j-1, right face j-2, flux face j-5/2
+    V5<FT> wB, dB, RB, FB;      // stage B, same roles for k = j-2
+    double ua1[5], ua2[5], ua3[5], ua4[5];  // U0 at j-1 .. j-4 (floored for HLL)
+    double ub1[5], ub2[5];                  // U1 at k-1, k-2
+    double nxt[5];
+
+    const int nsteps = (j1 - j0) + 8;
+    // prefetch first cell
+    if (live) {
+        int64_t off = (int64_t)mod_n(j0 - 4, n) * stride;
+        nxt[0] = q[s0 * S + off]; nxt[1] = q[s1 * S + off]; nxt[2] = q[s2 * S + off];
+        nxt[3] = q[s3 * S + off]; nxt[4] = q[s4 * S + off];
+    }
+
+    auto step = [&](int s) {
+        const int j = j0 - 4 + s;
+        double u[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) u[k] = nxt[k];
+        if (s + 1 < nsteps) {
+            int64_t off = (int64_t)mod_n(j + 1, n) * stride;
+            nxt[0] = q[s0 * S + off]; nxt[1] = q[s1 * S + off]; nxt[2] = q[s2 * S + off];
+            nxt[3] = q[s3 * S + off]; nxt[4] = q[s4 * S + off];
+        }
+        // ---- stage A ----
+        V5<FT> w = stage_prims<METHOD, DIR, FT>(u, c);  // floors u in place for HLL
+        V5<FT> d = v5_sub(w, wA);
+        V5<FT> Lf, Rf, f;
+        bool haveU1 = false;
+        double u1[5];
+        if (s >= 2) stage_faces<METHOD, SLOPE, FT>(c, wA, dA, d, Lf, Rf);   // faces of j-1
+        if (s >= 3) f = stage_flux<METHOD, FT>(c, RA, Lf);                  // face j-3/2
+        if (s >= 4) {                                                        // U1[j-2]
+#pragma unroll
+            for (int k = 0; k < 5; k++) u1[k] = ua2[k] - lambda * ((double)f.a[k] - (double)FA.a[k]);
+            haveU1 = true;
+        }
+        // shift stage A window; ua4 keeps U0[j-4] for the final update below
+        if (s >= 2) RA = Rf;
+        if (s >= 3) FA = f;
+        dA = d;
+        wA = w;
+#pragma unroll
+        for (int k = 0; k < 5; k++) { ua4[k] = ua3[k]; ua3[k] = ua2[k]; ua2[k] = ua1[k]; ua1[k] = u[k]; }
+        if (!haveU1) return;
+        // ---- stage B on k = j-2 ----
+        const int sb = s - 4;
+        V5<FT> wb = stage_prims<METHOD, DIR, FT>(u1, c);
+        V5<FT> db = v5_sub(wb, wB);
+        V5<FT> Lb, Rb, fb;
+        if (sb >= 2) stage_faces<METHOD, SLOPE, FT>(c, wB, dB, db, Lb, Rb);
+        if (sb >= 3) fb = stage_flux<METHOD, FT>(c, RB, Lb);
+        if (sb >= 4) {
+            // final update of cell k-2 = j-4: .5*(U1 + U0 - lambda*dF)
+            const int jo = j - 4;
+            double out[5];
+#pragma unroll
+            for (int k = 0; k < 5; k++) out[k] = .5 * (ub2[k] + ua4[k] - lambda * ((double)fb.a[k] - (double)FB.a[k]));
+            if (jo - j0 < 4) {
+                const int slot = jo - j0;
+#pragma unroll
+                for (int k = 0; k < 5; k++) defer[(slot * 5 + k) * nthr + tid] = out[k];
+            } else {
+                int64_t off = (int64_t)jo * stride;
+                q[s0 * S + off] = out[0]; q[s1 * S + off] = out[1]; q[s2 * S + off] = out[2];
+                q[s3 * S + off] = out[3]; q[s4 * S + off] = out[4];
+            }
+        }
+        if (sb >= 2) RB = Rb;
+        if (sb >= 3) FB = fb;
+        dB = db;
+        wB = wb;
+#pragma unroll
+        for (int k = 0; k < 5; k++) { ub2[k] = ub1[k]; ub1[k] = u1[k]; }
+    };
+
+    // prologue: the first eight cells (j0-4 .. j0+3) are read before any chunk writes
+    if (live) {
+        for (int s = 0; s < 8 && s < nsteps; s++) step(s);
+    }
+    __syncthreads();
+    if (live) {
+        for (int s = 8; s < nsteps; s++) step(s);
+    }
+    __syncthreads();
+    if (live) {
+        for (int slot = 0; slot < 4 && j0 + slot < j1; slot++) {
+            int64_t off = (int64_t)(j0 + slot) * stride;
+            q[s0 * S + off] = defer[(slot * 5 + 0) * nthr + tid];
+            q[s1 * S + off] = defer[(slot * 5 + 1) * nthr + tid];
+            q[s2 * S + off] = defer[(slot * 5 + 2) * nthr + tid];
+            q[s3 * S + off] = defer[(slot * 5 + 3) * nthr + tid];
+            q[s4 * S + off] = defer[(slot * 5 + 4) * nthr + tid];
+        }
+    }
+}
+
+}  // namespace ib

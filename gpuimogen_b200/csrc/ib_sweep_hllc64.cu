@@ -1,0 +1,10 @@
+// ib_sweep_hllc64.cu -- instantiates the fused sweep kernels for method IB_METHOD_HLLC with double flux arithmetic.
+#include "ib_sweep_launch.cuh"
+
+namespace ib {
+int launch_hllc64(int slope, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
+              double rho_min, double c_iso, cudaStream_t st)
+{
+    return launch_sweep_slope<IB_METHOD_HLLC, double>(slope, dir, q, slab, grid, lambda, gamma, rho_min, c_iso, st);
+}
+}  // namespace ib

@@ -1,0 +1,81 @@
+// ib_sweep_launch.cuh -- host launch logic for the fused sweep kernels of one (method, flux type).
+#pragma once
+
+#include "ib_internal.cuh"
+#include "ib_sweep.cuh"
+
+namespace ib {
+
+template <int METHOD, int SLOPE, typename FT>
+int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c,
+                   cudaStream_t st)
+{
+    const int nx = grid[0], ny = grid[1], nz = grid[2];
+    const int n = grid[dir - 1];
+    const int64_t N = (int64_t)nx * ny * nz;
+    if (n <= 0 || N <= 0) return IB_SUCCESSFUL;
+
+    if (dir == 1 && nx <= 1024) {
+        // one CTA per row, one or two cells per thread
+        SweepArgs a{q, slab, nx, ny, nz, lambda};
+        const int64_t rows = (int64_t)ny * nz;
+        const size_t shm = (size_t)10 * nx * sizeof(FT);
+        if (nx <= 512) {
+            int nt = ((nx + 31) / 32) * 32;
+            sweep_row_kernel<METHOD, SLOPE, FT, 1><<<(unsigned)rows, nt, shm, st>>>(a, c);
+        } else {
+            int nt = (((nx + 1) / 2 + 31) / 32) * 32;
+            sweep_row_kernel<METHOD, SLOPE, FT, 2><<<(unsigned)rows, nt, shm, st>>>(a, c);
+        }
+        return check_launch();
+    }
+
+    // march kernel: PW pencils x C chunks per CTA, C*PW <= 256
+    const int64_t npencil = N / n;
+    int PW = 32;
+    if (dir == 1) PW = 32;  // lanes on different rows: correct, uncoalesced fallback for long rows
+    // target ~4 resident waves of threads; chunk length at least 16 cells
+    const int64_t target_threads = (int64_t)num_sms() * 1024;
+    int C = 1;
+    while (C < 64 && (npencil * C) < target_threads && n / (2 * C) >= 16) C *= 2;
+    while (PW * C > 256 && PW > 4) PW /= 2;
+    while (PW * C > 256) C /= 2;
+    int L = (n + C - 1) / C;
+    C = (n + L - 1) / L;
+    MarchArgs a{q, slab, nx, ny, nz, n, npencil, L, lambda};
+    dim3 block(PW, C);
+    dim3 gridd((unsigned)((npencil + PW - 1) / PW));
+    size_t shm = (size_t)20 * sizeof(double) * PW * C;
+    switch (dir) {
+    case 1: sweep_march_kernel<METHOD, SLOPE, FT, 1><<<gridd, block, shm, st>>>(a, c); break;
+    case 2: sweep_march_kernel<METHOD, SLOPE, FT, 2><<<gridd, block, shm, st>>>(a, c); break;
+    default: sweep_march_kernel<METHOD, SLOPE, FT, 3><<<gridd, block, shm, st>>>(a, c); break;
+    }
+    return check_launch();
+}
+
+template <int METHOD, typename FT>
+int launch_sweep_slope(int slope, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
+                       double rho_min, double c_iso, cudaStream_t st)
+{
+    FluidConsts<FT> c = make_consts<FT>(gamma, rho_min, c_iso);
+    switch (slope) {
+    case IB_SLOPE_OSPRE: return launch_sweep_t<METHOD, IB_SLOPE_OSPRE, FT>(dir, q, slab, grid, lambda, c, st);
+    case IB_SLOPE_MC: return launch_sweep_t<METHOD, IB_SLOPE_MC, FT>(dir, q, slab, grid, lambda, c, st);
+    case IB_SLOPE_VANLEER: return launch_sweep_t<METHOD, IB_SLOPE_VANLEER, FT>(dir, q, slab, grid, lambda, c, st);
+    case IB_SLOPE_MINMOD: return launch_sweep_t<METHOD, IB_SLOPE_MINMOD, FT>(dir, q, slab, grid, lambda, c, st);
+    case IB_SLOPE_SUPERBEE: return launch_sweep_t<METHOD, IB_SLOPE_SUPERBEE, FT>(dir, q, slab, grid, lambda, c, st);
+    case IB_SLOPE_VANALBADA: return launch_sweep_t<METHOD, IB_SLOPE_VANALBADA, FT>(dir, q, slab, grid, lambda, c, st);
+    case IB_SLOPE_ZERO: return launch_sweep_t<METHOD, IB_SLOPE_ZERO, FT>(dir, q, slab, grid, lambda, c, st);
+    default: return IB_ERROR_INVALID_ARGS;
+    }
+}
+
+int launch_hllc64(int slope, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
+                  double rho_min, double c_iso, cudaStream_t st);
+int launch_hllc32(int slope, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
+                  double rho_min, double c_iso, cudaStream_t st);
+int launch_hll64(int slope, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
+                 double rho_min, double c_iso, cudaStream_t st);
+
+}  // namespace ib

@@ -1,0 +1,220 @@
+/*
+ * imogen_b200.h -- C ABI of the B200-native Imogen fluid-step library (libimogen_b200.so).
+ *
+ * One entry point per mex function of the reference's fluid-step hot path
+ * (imogenproject/gpuImogen, gpuclass/), with the same argument meaning and in-place
+ * semantics, expressed with plain pointers and POD structs so that a thin mex / ctypes / cgo
+ * shim can bind them.  All array pointers are DEVICE pointers unless stated otherwise; the
+ * caller owns every buffer it passes.  Every call is ordered on the given CUDA stream
+ * (NULL = legacy default stream) and only returns to the host early where it must produce a
+ * host value (the CFL timestep).  Return value: IB_SUCCESSFUL (0) or one of the reference's
+ * error codes (gpuclass/imogenChecks.h:11-24); no entry point calls exit().
+ *
+ * Layout of a fluid: one allocation of five slabs [rho, E, px, py, pz]; each slab holds
+ * nx*ny*nz doubles, x fastest, and slabs are `slab_pitch` doubles apart (a multiple of 32,
+ * i.e. 256 B, as MGA_allocSlab pads them, gpuclass/cudaCommon.cu:339-370).  Arrays always stay
+ * in XYZ order: the library sweeps y and z in place instead of transposing
+ * (gpuclass/cudaArrayRotateB.cu is not needed).
+ */
+#ifndef IMOGEN_B200_H
+#define IMOGEN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define IB_API __attribute__((visibility("default")))
+#else
+#define IB_API
+#endif
+
+/* Status codes (gpuclass/imogenChecks.h:11-24) */
+#define IB_SUCCESSFUL 0
+#define IB_ERROR_INVALID_ARGS -100
+#define IB_ERROR_CRASH -101
+#define IB_ERROR_NULL_POINTER -102
+#define IB_ERROR_NOIMPLEMENT -105
+#define IB_ERROR_NOMEM -106
+#define IB_ERROR_CUDA -1000
+
+/* Fluid methods (gpuclass/cudaFluidStep.h:6-8) */
+#define IB_METHOD_HLL 1
+#define IB_METHOD_HLLC 2
+#define IB_METHOD_XINJIN 3
+
+/* Slope limiters for HLL/HLLC reconstruction (gpuclass/limiter_functions.h:54-119).
+ * The reference selects one at compile time (SLOPEFUNC, cudaFluidStep.cu:129-135; default
+ * Ospre); here it is a runtime choice. */
+#define IB_SLOPE_OSPRE 0
+#define IB_SLOPE_MC 1
+#define IB_SLOPE_VANLEER 2
+#define IB_SLOPE_MINMOD 3
+#define IB_SLOPE_SUPERBEE 4
+#define IB_SLOPE_VANALBADA 5
+#define IB_SLOPE_ZERO 6
+
+/* Flux limiters for the Xin-Jin TVD correction (limiter_functions.h:11-45; LIMITERFUNC,
+ * cudaFluidStep.cu:122-127, default Ospre). */
+#define IB_FLUX_OSPRE 0
+#define IB_FLUX_VANLEER 1
+#define IB_FLUX_MINMOD 2
+#define IB_FLUX_SUPERBEE 3
+#define IB_FLUX_ZERO 4
+
+/* Flux precision: FP64 everywhere, or HLLC/limiter arithmetic in FP32 with FP64 conserved
+ * accumulation (the reference's FLOATFLUX compile option, cudaFluidStep.cu:118-122). */
+#define IB_PREC_FP64 0
+#define IB_PREC_FP32_FLUX 1
+
+/* Boundary modes, BCModeTypes (gpuclass/cudaCommon.h:49); order [-X, +X, -Y, +Y, -Z, +Z]. */
+#define IB_BC_CIRCULAR 0
+#define IB_BC_MIRROR 1
+#define IB_BC_WALL 2
+#define IB_BC_STATIONARY 3
+#define IB_BC_CONST 4
+#define IB_BC_LINEAR 5
+#define IB_BC_OUTFLOW 6
+#define IB_BC_FREEBALANCE 7
+
+/* Drag integrators (cudaSource2FluidDrag.cu:226-245) */
+#define IB_DRAG_EMP 0
+#define IB_DRAG_RK4 1
+#define IB_DRAG_ETDRK1 2
+#define IB_DRAG_ETDRK2 3
+#define IB_DRAG_LOGTRAP2 4
+#define IB_DRAG_LOGTRAP3 5
+
+typedef struct ib_grid {
+    int32_t nx, ny, nz;
+    int32_t reserved;
+    int64_t slab_pitch; /* doubles between slabs, multiple of 32, >= nx*ny*nz */
+} ib_grid;
+
+/* Statics ("fade") list of one array: device array [3][pitch] of
+ * [linear index; value; coefficient] (cudaStatics.cu:1240-1266). */
+typedef struct ib_statics {
+    const double *data;
+    int64_t count;
+    int64_t pitch;
+} ib_statics;
+
+/* One fluid: the FluidManager canister (mass/ener/mom, cudaCommonML.cu:400-432) with its
+ * boundary data (BCSettings, cudaCommon.h:51-58) and halo depth (4, run/starterRun.m:60-67). */
+typedef struct ib_fluid {
+    double *q;
+    ib_grid grid;
+    int32_t bc[6];
+    int32_t halo;
+    int32_t reserved;
+    ib_statics statics[5];
+} ib_fluid;
+
+/* Per-fluid thermodynamics used by the fluid step (fluid.thermoDetails, fluid.MINMASS;
+ * flux_ML_iface.cu:117-143). c_isothermal = -1 for an adiabatic fluid. */
+typedef struct ib_fluid_thermo {
+    double gamma;
+    double rho_min;
+    double c_isothermal;
+} ib_fluid_thermo;
+
+/* Geometry (GeometryParams, cudaCommon.h; accessMatlabGeometryClass, cudaCommonML.cu:453-481).
+ * Only shape 0 = SQUARE is implemented. global_rez gives the dimensionality for the CFL
+ * (globalDomainRez, cflTimestep.cu:85-87). */
+typedef struct ib_geometry {
+    double h[3];
+    double r_inner;
+    int32_t shape;
+    int32_t global_rez[3];
+} ib_geometry;
+
+/* Numerical switches that the reference fixes at compile time; NULL = reference defaults
+ * (Ospre slope limiter, Ospre flux limiter, FP64). */
+typedef struct ib_numerics {
+    int32_t slope_limiter;
+    int32_t flux_limiter;
+    int32_t precision;
+    int32_t reserved;
+} ib_numerics;
+
+/* Microphysics of one fluid for the drag source (ThermoDetails, cudaCommon.h;
+ * accessMatlabThermoDetails, cudaCommonML.cu:434-451). */
+typedef struct ib_thermo {
+    double gamma, mass, mu0, mu_t_index, sigma0, sigma_t_index, k_bolt, c_isothermal;
+} ib_thermo;
+
+/* Smallest legal slab pitch (doubles) for an nx*ny*nz array: numel rounded up to 32. */
+IB_API int64_t ib_slab_pitch(int32_t nx, int32_t ny, int32_t nz);
+
+/* Human-readable name of a status code. */
+IB_API const char *ib_status_string(int status);
+
+/* Last CUDA error seen by the library (cudaError_t value), 0 if none. */
+IB_API int ib_last_cuda_error(void);
+
+/* Number of kernels this process has launched through the library (all devices). */
+IB_API long long ib_launch_count(void);
+
+/* Replaces the cudaFluidStep mex (gpuclass/cudaFluidStep.cu:161-227): one SSPRK2 directional
+ * sweep of one fluid, in place, without boundary fill.
+ * params = [dt, purehydro, gamma, rho_min, method (1 HLL | 2 HLLC | 3 XJ), direction (1..3)
+ *           (, c_isothermal)], nparams 6 or 7; with 7 the fluid is isothermal and gamma := 2. */
+IB_API int ib_cudaFluidStep(ib_fluid *fluid, const ib_geometry *geo, const double *params, int nparams,
+                     const ib_numerics *num, void *stream);
+
+/* Replaces the fluidstep mex (gpuclass/flux_ML_iface.cu:37-160 -> performFluidUpdate_3D,
+ * flux.cu:27-165): the three Strang-ordered sweeps plus boundary fill after each, for every
+ * fluid in turn.  params = [dt, purehydro, sweep direction (+1 | -1), iteration, method]. */
+IB_API int ib_fluidstep(ib_fluid *fluids, const ib_fluid_thermo *thermo, int nfluids,
+                 const ib_geometry *geo, const double *params, int nparams,
+                 const ib_numerics *num, void *stream);
+
+/* Replaces the cudaSoundspeed mex for hydro (gpuclass/cudaSoundspeed.cu:54-105,
+ * calculateSoundspeed :107-150): cs_out[N] = sqrt(max(0, gamma(gamma-1) e_int / rho)). */
+IB_API int ib_cudaSoundspeed(const ib_fluid *fluid, double gamma, double *cs_out, void *stream);
+
+/* Replaces the cflTimestep mex (gpuclass/cflTimestep.cu:64-103 -> computeLocalCFLTimestep
+ * :107-252): *tau_host = min over cells of the signal-crossing time, halved for HLL/HLLC.
+ * cs is the soundspeed array from ib_cudaSoundspeed.  Synchronises the stream. */
+IB_API int ib_cflTimestep(const ib_fluid *fluid, const double *cs, const ib_geometry *geo, int method,
+                   double *tau_host, void *stream);
+
+/* Same value as ib_cudaSoundspeed + ib_cflTimestep in one pass over the fluid (no soundspeed
+ * array).  If tau_device is not NULL the result is also left there and the call does not
+ * synchronise (tau_host may then be NULL). */
+IB_API int ib_cflTimestepFused(const ib_fluid *fluid, double gamma, const ib_geometry *geo, int method,
+                        double *tau_host, double *tau_device, void *stream);
+
+/* Replaces the freezeAndPtot mex for hydro (gpuclass/freezeAndPtot.cu:32-147, kernel
+ * :229-290): ptot[N] = gas pressure (raising E where c_s < cs_min), freeze[ny*nz] = max over
+ * each x row of |px|/rho + c_s. */
+IB_API int ib_freezeAndPtot(ib_fluid *fluid, double gamma, int purehydro, double cs_min, double *ptot,
+                     double *freeze, void *stream);
+
+/* Replaces the cudaStatics mex = setBoundaryConditions (gpuclass/cudaStatics.cu:85-104 ->
+ * setArrayBoundaryConditions :199-286) for one array stored in XYZ order: applies its statics
+ * and its boundary modes on both faces of `direction`.  vector_component: 0 scalar, 1..3 the
+ * momentum component the array holds (mirror parity).  For outflow the array must be the
+ * density slab of a fluid (the reference's numSlabs == 0 check, :255-259); the whole fluid
+ * whose density slab starts at phi is then updated (slab_pitch from grid). */
+IB_API int ib_cudaStatics(double *phi, const ib_grid *grid, const int32_t bc[6], int halo,
+                   int vector_component, const ib_statics *statics, int direction, void *stream);
+
+/* Boundary fill of a whole fluid as the fluid step performs it after a sweep along
+ * `direction` (setFluidBoundary, gpuclass/cudaStatics.cu:112-197). */
+IB_API int ib_setFluidBoundary(ib_fluid *fluid, int direction, void *stream);
+
+/* Replaces the cudaSource2FluidDrag mex (gpuclass/cudaSource2FluidDrag.cu:125-181 ->
+ * sourcefunction_2FluidDrag :189-246): gas-dust drag over dt, in place.
+ * params = [dt, method (IB_DRAG_*)]. */
+IB_API int ib_cudaSource2FluidDrag(ib_fluid *gas, ib_fluid *dust, const ib_thermo *thermo_gas,
+                            const ib_thermo *thermo_dust, const ib_geometry *geo,
+                            const double *params, int nparams, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IMOGEN_B200_H */

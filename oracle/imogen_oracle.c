@@ -1,0 +1,1165 @@
+/*
+ * imogen_oracle.c -- CPU oracle (test infrastructure) for the Imogen fluid-step hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY: called by tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline as the checker; never by the product library.
+ *
+ * Every function restates the arithmetic of one reference kernel (imogenproject/gpuImogen,
+ * paths relative to that project) in the reference's own evaluation order, so that with
+ * -ffp-contract=off the results are the same IEEE operations the reference performs (the
+ * reference kernels are SIMT FP64; their per-thread expressions are reproduced here per cell).
+ * The transposes the reference performs between sweeps (cudaArrayRotateB.cu) only move data,
+ * so the oracle sweeps each pencil in place with the matching stride instead.
+ */
+#include "imogen_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define OR_OK 0
+#define OR_ERR_INVALID 1
+#define OR_ERR_NOIMPL 2
+
+/* ------------------------------------------------------------------------------------------
+ * Limiters (gpuclass/limiter_functions.h:11-119).  Slope limiters return HALF the limited
+ * difference (projection from cell centre to face).
+ * ---------------------------------------------------------------------------------------- */
+static double slope_ospre(double A, double B)          /* limiter_functions.h:87-95 */
+{
+    double R = A * B;
+    if (R > 0) {
+        double S = A + B;
+        return .75 * R * S / (S * S - R);
+    }
+    return 0.0;
+}
+
+static double slope_mc(double A, double B)             /* limiter_functions.h:105-115 */
+{
+    if (A * B <= 0) return 0;
+    double R = B / A;
+    double S = .25 + .25 * R;
+    S = (S < R) ? S : R;
+    S = (S < 1) ? S : 1.0;
+    return S * A;
+}
+
+static double slope_vanleer(double A, double B)        /* limiter_functions.h:54-61 */
+{
+    double r = A * B;
+    if (r > 0.0) return r / (A + B);
+    return 0;
+}
+
+static double slope_minmod(double A, double B)         /* limiter_functions.h:71-77 */
+{
+    /* the FP64 build declares this limiter with a float return type: the half slope is
+     * rounded to single precision on return */
+    if (A * B < 0) return 0.0;
+    if (fabs(A) > fabs(B)) return (double)(float)(.5 * B);
+    return (double)(float)(.5 * A);
+}
+
+static double flux_minmod(double A, double B)          /* limiter_functions.h:21-26 */
+{
+    if (A * B < 0) return 0.0;
+    if (fabs(A) > fabs(B)) return B;
+    return A;
+}
+
+static double slope_superbee(double A, double B)       /* limiter_functions.h:80-86 */
+{
+    if (A * B < 0) return 0.0;
+    if (B < A) return flux_minmod(A, 2 * B);
+    return .5 * flux_minmod(2 * A, B);
+}
+
+static double slope_vanalbada(double A, double B)      /* limiter_functions.h:97-102 */
+{
+    double R = A * B;
+    if (R < 0) return 0;
+    return .5 * R * (A + B) / (A * A + B * B);
+}
+
+static double slope_apply(int which, double A, double B)
+{
+    switch (which) {
+    case OR_SLOPE_OSPRE: return slope_ospre(A, B);
+    case OR_SLOPE_MC: return slope_mc(A, B);
+    case OR_SLOPE_VANLEER: return slope_vanleer(A, B);
+    case OR_SLOPE_MINMOD: return slope_minmod(A, B);
+    case OR_SLOPE_SUPERBEE: return slope_superbee(A, B);
+    case OR_SLOPE_VANALBADA: return slope_vanalbada(A, B);
+    default: return 0.0;
+    }
+}
+
+static double flux_ospre(double A, double B)           /* limiter_functions.h:36-42 */
+{
+    double r = A * B;
+    if (r <= 0.0) return 0.0;
+    return 1.5 * r * (A + B) / (A * A + r + B * B);
+}
+
+static double flux_vanleer(double A, double B)         /* limiter_functions.h:11-19 */
+{
+    double r = 2.0 * A * B;
+    if (r > 0.0) return r / (A + B);
+    return 0;
+}
+
+static double flux_superbee(double A, double B)        /* limiter_functions.h:28-34 */
+{
+    if (A * B < 0) return 0.0;
+    if (B < A) return flux_minmod(A, 2 * B);
+    return flux_minmod(2 * A, B);
+}
+
+static double flux_apply(int which, double A, double B)
+{
+    switch (which) {
+    case OR_FLUX_OSPRE: return flux_ospre(A, B);
+    case OR_FLUX_VANLEER: return flux_vanleer(A, B);
+    case OR_FLUX_MINMOD: return flux_minmod(A, B);
+    case OR_FLUX_SUPERBEE: return flux_superbee(A, B);
+    default: return 0.0;
+    }
+}
+
+/* ------------------------------------------------------------------------------------------
+ * Constants uploaded per sweep (cudaFluidStep.cu:289-311)
+ * ---------------------------------------------------------------------------------------- */
+typedef struct {
+    double gamma, gm1, minmass, mintemp, govergm1, isotemp, isotempsq;
+} fconst;
+
+static fconst make_consts(const or_step *p)
+{
+    fconst c;
+    c.gamma = p->gamma;
+    c.gm1 = p->gamma - 1.0;
+    c.minmass = p->rho_min;
+    c.mintemp = 1e-5 / (p->gamma - 1);       /* cudaFluidStep.cu:298 */
+    c.govergm1 = p->gamma / (p->gamma - 1.0);
+    c.isotemp = p->c_iso;
+    c.isotempsq = p->c_iso * p->c_iso;
+    return c;
+}
+
+typedef struct { double vl, vr; } bounds2;
+
+/* computeEinfeldtBounds (cudaFluidStep.cu:1728-1755) */
+static bounds2 einfeldt(const fconst *c, double rhoL, double vL, double PL, double rhoR,
+                        double vR, double PR, double dvsq)
+{
+    double csql = c->gamma * PL / rhoL;
+    double csqr = c->gamma * PR / rhoR;
+    double Fa = sqrt(rhoR / rhoL);
+    double Fb = 1.0 / (1.0 + Fa);
+    double Croe = ((csql + Fa * csqr) + .5 * c->gm1 * dvsq * Fa * Fb) * Fb;
+    bounds2 sb;
+    double Vroe = (vL + Fa * vR) * Fb;
+    Croe = Vroe - sqrt(Croe);
+    sb.vl = vL - sqrt(csql);
+    sb.vr = vR + sqrt(csqr);
+    sb.vl = (Croe < sb.vl) ? Croe : sb.vl;
+    Croe = 2 * Vroe - Croe;
+    sb.vr = (Croe > sb.vr) ? Croe : sb.vr;
+    return sb;
+}
+
+/* computeEinfeldtBounds_isothermal (cudaFluidStep.cu:1780-1799) */
+static bounds2 einfeldt_iso(double rhoL, double vL, double rhoR, double vR, double cs)
+{
+    double Fa = sqrt(rhoR / rhoL);
+    double Fb = 1.0 / (1.0 + Fa);
+    bounds2 sb;
+    double Vroe = (vL + Fa * vR) * Fb;
+    cs = Vroe - cs;
+    sb.vl = vL - cs;
+    sb.vr = vR + cs;
+    sb.vl = (cs < sb.vl) ? cs : sb.vl;
+    cs = 2 * Vroe - cs;
+    sb.vr = (cs > sb.vr) ? cs : sb.vr;
+    return sb;
+}
+
+/* Row buffers: a pencil is gathered into local order [rho, E, p_normal, p_t1, p_t2]. */
+typedef struct {
+    int n;
+    double *u[5];    /* conserved, local order */
+    double *w[5];    /* scratch */
+    double *edge[10];
+    double *flux[5];
+    double *tmp[5];
+} rowbuf;
+
+static void rowbuf_alloc(rowbuf *r, int n)
+{
+    int k;
+    double *blk = (double *)malloc(sizeof(double) * (size_t)n * 30);
+    r->n = n;
+    for (k = 0; k < 5; k++) r->u[k] = blk + (size_t)n * k;
+    for (k = 0; k < 5; k++) r->w[k] = blk + (size_t)n * (5 + k);
+    for (k = 0; k < 10; k++) r->edge[k] = blk + (size_t)n * (10 + k);
+    for (k = 0; k < 5; k++) r->flux[k] = blk + (size_t)n * (20 + k);
+    for (k = 0; k < 5; k++) r->tmp[k] = blk + (size_t)n * (25 + k);
+}
+
+static void rowbuf_free(rowbuf *r) { free(r->u[0]); }
+
+static inline int wrap(int i, int n) { return (i < 0) ? i + n : ((i >= n) ? i - n : i); }
+
+/* ------------------------------------------------------------------------------------------
+ * HLLC, 2nd order MUSCL (cukern_HLLC_2ndorder, cudaFluidStep.cu:1124-1463), one stage.
+ * in[5]: conserved state of the row (local order).  flux[k][i] = flux through face i+1/2.
+ * ---------------------------------------------------------------------------------------- */
+static void hllc_row_flux(rowbuf *r, double *const in[5], const fconst *c, int slope)
+{
+    int n = r->n, i, k;
+    /* primitive variables: rho, e_int, vx, vy, vz (cudaFluidStep.cu:1200-1237) */
+    for (i = 0; i < n; i++) {
+        double A = in[0][i], B = in[1][i], C = in[2][i], D = in[3][i], E = in[4][i];
+        double F = 1.0 / A;
+        B -= .5 * (C * C + D * D + E * E) * F;
+        C *= F;
+        D *= F;
+        E *= F;
+        r->w[0][i] = A; r->w[1][i] = B; r->w[2][i] = C; r->w[3][i] = D; r->w[4][i] = E;
+    }
+    /* backward difference, limited half slope, face states (cudaFluidStep.cu:1287-1310) */
+    for (k = 0; k < 5; k++) {
+        double *v = r->w[k];
+        for (i = 0; i < n; i++) {
+            double dl = v[i] - v[wrap(i - 1, n)];
+            double dr = v[wrap(i + 1, n)] - v[i];
+            double s = slope_apply(slope, dl, dr);
+            if (k == 1) {
+                r->edge[2][i] = c->gm1 * (v[i] - s);  /* pressure, left face  (BOS2) */
+                r->edge[3][i] = c->gm1 * (v[i] + s);  /* pressure, right face (BOS3) */
+            } else {
+                r->edge[2 * k][i] = v[i] - s;
+                r->edge[2 * k + 1][i] = v[i] + s;
+            }
+        }
+    }
+    /* Riemann problem at face i+1/2 between cell i (right face) and i+1 (left face) */
+    for (i = 0; i < n; i++) {
+        int ir = wrap(i + 1, n);
+        double rhoL = r->edge[1][i], PL = r->edge[3][i], vxL = r->edge[5][i];
+        double vyL = r->edge[7][i], vzL = r->edge[9][i];
+        double rhoR = r->edge[0][ir], PR = r->edge[2][ir], vxR = r->edge[4][ir];
+        double vyR = r->edge[6][ir], vzR = r->edge[8][ir];
+        double A, B, C, D, E, F, G, H;
+        int mode;
+        double fr, fe, fpx, fpy, fpz;
+
+        C = vxL - vxR;
+        D = vyL - vyR;
+        E = vzL - vzR;
+        C = C * C + D * D + E * E;
+        bounds2 sb = einfeldt(c, rhoL, vxL, PL, rhoR, vxR, PR, C);
+        C = sb.vl;
+        D = sb.vr;
+        A = vxL;
+        B = vxR;
+        A = rhoL * (C - A);
+        B = rhoR * (D - B);
+        E = (B * vxR - PR - A * vxL + PL) / (B - A);  /* Batten et al. eq. 34 */
+
+        if (E > 0) mode = (C > 0) ? 0 : 2;
+        else mode = (D > 0) ? 3 : 1;
+
+        switch (mode) {
+        case 0:
+            A = rhoL; B = vxL; C = vyL; D = vzL;
+            E = .5 * (B * B + C * C + D * D) * A;
+            F = PL;
+            A *= B;
+            C *= A;
+            D *= A;
+            G = A * B + F;
+            B *= (E + c->govergm1 * F);
+            fr = A; fe = B; fpx = G; fpy = C; fpz = D;
+            break;
+        case 2:
+            A = rhoL; B = vxL;
+            D = A * (C - B) / (C - E);
+            F = vyL; H = vzL;
+            G = .5 * (B * B + F * F + H * H);
+            A = D * E;
+            F *= A;
+            H *= A;
+            C *= (E - B);
+            B = PL + D * (C + E * B);
+            G = D * E * (c->govergm1 * PL / rhoL + G + C);
+            fr = A; fe = G; fpx = B; fpy = F; fpz = H;
+            break;
+        case 3:
+            A = rhoR; B = vxR;
+            C = A * (D - B) / (D - E);
+            F = vyR; H = vzR;
+            G = .5 * (B * B + F * F + H * H);
+            A = C * E;
+            F *= A;
+            H *= A;
+            D *= (E - B);
+            B = PR + C * (D + E * B);
+            G = C * E * (c->govergm1 * PR / rhoR + G + D);
+            fr = A; fe = G; fpx = B; fpy = F; fpz = H;
+            break;
+        default: /* case 1 */
+            A = rhoR; B = vxR; C = vyR; D = vzR;
+            E = .5 * (B * B + C * C + D * D) * A;
+            F = PR;
+            A *= B;
+            C *= A;
+            D *= A;
+            G = A * B + F;
+            B *= (E + c->govergm1 * F);
+            fr = A; fe = B; fpx = G; fpy = C; fpz = D;
+            break;
+        }
+        r->flux[0][i] = fr; r->flux[1][i] = fe; r->flux[2][i] = fpx;
+        r->flux[3][i] = fpy; r->flux[4][i] = fpz;
+    }
+}
+
+/* SSPRK2 with HLLC (cudaFluidStep.cu:1510-1559 stage A, 1560-1600 stage B) */
+static void hllc_row_sweep(rowbuf *r, const fconst *c, int slope, double lambda)
+{
+    int n = r->n, i, k;
+    hllc_row_flux(r, r->u, c, slope);
+    for (k = 0; k < 5; k++)
+        for (i = 0; i < n; i++)
+            r->tmp[k][i] = r->u[k][i] - lambda * (r->flux[k][i] - r->flux[k][wrap(i - 1, n)]);
+    hllc_row_flux(r, r->tmp, c, slope);
+    for (k = 0; k < 5; k++)
+        for (i = 0; i < n; i++)
+            r->u[k][i] = .5 * (r->tmp[k][i] + r->u[k][i] -
+                               lambda * (r->flux[k][i] - r->flux[k][wrap(i - 1, n)]));
+}
+
+/* ------------------------------------------------------------------------------------------
+ * HLL (cukern_HLL_step, cudaFluidStep.cu:1801-2422) and its pressure solver
+ * (cukern_PressureSolverHydro, cudaFluidStep.cu:2813-2864).
+ * ---------------------------------------------------------------------------------------- */
+/* Floors rho and e_int of state s in place (local row order is fine: the solver is
+ * symmetric in the momenta) and returns the gas pressure into P.  The reference sums the
+ * squared momenta in memory-slab order px, py, pz; mom_order gives which local index holds
+ * slab 2, 3, 4. */
+static void hll_pressure_row(double *const s[5], double *P, int n, const fconst *c,
+                             const int mom_order[3])
+{
+    int i;
+    for (i = 0; i < n; i++) {
+        double rho = s[0][i], E, z, momsq, p;
+        if (rho < c->minmass) {
+            p = c->minmass / rho;
+            rho = s[0][i] = c->minmass;
+            E = s[1][i] = p * s[1][i];
+            z = s[mom_order[0]][i] = p * s[mom_order[0]][i];
+            momsq = z * z;
+            z = s[mom_order[1]][i] = p * s[mom_order[1]][i];
+            momsq += z * z;
+            z = s[mom_order[2]][i] = p * s[mom_order[2]][i];
+            momsq += z * z;
+        } else {
+            E = s[1][i];
+            z = s[mom_order[0]][i];
+            momsq = z * z;
+            z = s[mom_order[1]][i];
+            momsq += z * z;
+            z = s[mom_order[2]][i];
+            momsq += z * z;
+        }
+        p = E - .5 * momsq / rho;
+        if (p < rho * c->mintemp) {
+            p = c->mintemp * rho;
+            s[1][i] = (.5 * momsq / rho) + p;
+            P[i] = p * c->gm1;
+        } else {
+            P[i] = p * c->gm1;
+        }
+    }
+}
+
+static void hll_row_flux(rowbuf *r, double *const in[5], const double *P, const fconst *c,
+                         int slope)
+{
+    int n = r->n, i, k;
+    /* primitives rho, v_n, P, v_t1, v_t2 -> w[0..4] (cudaFluidStep.cu:1864-1888) */
+    for (i = 0; i < n; i++) {
+        double Ale = in[0][i];
+        r->w[0][i] = Ale;
+        r->w[1][i] = in[2][i] / Ale;
+        r->w[2][i] = P[i];
+        r->w[3][i] = in[3][i] / Ale;
+        r->w[4][i] = in[4][i] / Ale;
+    }
+    /* slopes, left/right faces (cudaFluidStep.cu:1935-1959) */
+    for (k = 0; k < 5; k++) {
+        double *v = r->w[k];
+        for (i = 0; i < n; i++) {
+            double bd = v[i] - v[wrap(i - 1, n)];
+            double bdr = v[wrap(i + 1, n)] - v[i];
+            double Fa = slope_apply(slope, bd, bdr);
+            r->edge[2 * k + 1][i] = v[i] + Fa;  /* right face */
+            r->edge[2 * k][i] = v[i] - Fa;      /* left face  */
+        }
+    }
+    for (i = 0; i < n; i++) {
+        int ir = wrap(i + 1, n);
+        /* Xle = right face of cell i, Xre = left face of cell i+1 (cudaFluidStep.cu:2049-2055) */
+        double Ale = r->edge[1][i], Ble = r->edge[3][i], Cle = r->edge[5][i];
+        double Dle = r->edge[7][i], Ele = r->edge[9][i];
+        double Are = r->edge[0][ir], Bre = r->edge[2][ir], Cre = r->edge[4][ir];
+        double Dre = r->edge[6][ir], Ere = r->edge[8][ir];
+        double Utilde = (Bre - Ble), Sleft = (Dre - Dle), Sright = (Ere - Ele);
+        double Atilde, Fa, Fb;
+        double f0, f1, f2, f3, f4;
+        bounds2 sb;
+        int mode;
+        if (c->isotemp == -1) {
+            sb = einfeldt(c, Ale, Ble, Cle, Are, Bre, Cre,
+                          Utilde * Utilde + Sleft * Sleft + Sright * Sright);
+        } else {
+            /* the isothermal bound is handed c_iso^2 where a speed is expected
+             * (cudaFluidStep.cu:2131) */
+            sb = einfeldt_iso(Ale, Ble, Are, Bre, c->isotempsq);
+        }
+        Sleft = sb.vl;
+        Sright = sb.vr;
+        Atilde = 1 / (Sright - Sleft);
+        Fa = Ale * Ble;
+        Fb = Are * Bre;
+        mode = 1;
+        if (Sleft >= 0) mode = 0;
+        if (Sright <= 0) mode = 2;
+        switch (mode) {
+        case 0:
+            f0 = Fa;
+            if (c->isotemp == -1) {
+                f1 = Ble * (c->govergm1 * Cle + .5 * Ale * (Ble * Ble + Dle * Dle + Ele * Ele));
+                f2 = Fa * Ble + Cle;
+            } else {
+                f1 = Ble * (Cle + .5 * Ale * (Ble * Ble + Dle * Dle + Ele * Ele));
+                f2 = Fa * Ble + c->isotempsq * Ale;
+            }
+            f3 = Fa * Dle;
+            f4 = Fa * Ele;
+            break;
+        case 1:
+            f0 = (Sright * (Ble - Sleft) * Ale - Sleft * (Bre - Sright) * Are) * Atilde;
+            if (c->isotemp == -1) {
+                f2 = (Sright * (Ble - Sleft) * Fa - Sleft * (Bre - Sright) * Fb + Sright * Cle -
+                      Sleft * Cre) * Atilde;
+            } else {
+                f2 = (Sright * (Ble - Sleft) * Fa - Sleft * (Bre - Sright) * Fb +
+                      c->isotempsq * (Sright * Ale - Sleft * Are)) * Atilde;
+            }
+            f3 = (Sright * (Ble - Sleft) * Ale * Dle - Sleft * (Bre - Sright) * Are * Dre) * Atilde;
+            f4 = (Sright * (Ble - Sleft) * Ale * Ele - Sleft * (Bre - Sright) * Are * Ere) * Atilde;
+            if (c->isotemp == -1) {
+                Fa = .5 * Ale * (Ble * Ble + Dle * Dle + Ele * Ele);
+                Fb = .5 * Are * (Bre * Bre + Dre * Dre + Ere * Ere);
+                f1 = (Sright * (Ble - Sleft) * Fa - Sleft * (Bre - Sright) * Fb);
+                f1 = (f1 + (c->govergm1 * (Sright * Cle * Ble - Sleft * Cre * Bre) +
+                            Sleft * Sright * (Cre - Cle) / c->gm1)) * Atilde;
+            } else {
+                /* isothermal energy flux is left without the 1/(S_R-S_L) factor
+                 * (cudaFluidStep.cu:2178-2182) */
+                Fa = .5 * Ale * (Ble * Ble + Dle * Dle + Ele * Ele) + Cle;
+                Fb = .5 * Are * (Bre * Bre + Dre * Dre + Ere * Ere) + Cre;
+                f1 = (Sright * (Ble - Sleft) * Fa - Sleft * (Bre - Sright) * Fb);
+            }
+            break;
+        default:
+            f0 = Fb;
+            if (c->isotemp == -1) {
+                f1 = Bre * (c->govergm1 * Cre + .5 * Are * (Bre * Bre + Dre * Dre + Ere * Ere));
+                f2 = Fb * Bre + Cre;
+            } else {
+                f1 = Bre * (Cre + .5 * Are * (Bre * Bre + Dre * Dre + Ere * Ere));
+                /* c_iso, not c_iso^2 (cudaFluidStep.cu:2191) */
+                f2 = Fb * Bre + c->isotemp * Are;
+            }
+            f3 = Fb * Dre;
+            f4 = Fb * Ere;
+            break;
+        }
+        r->flux[0][i] = f0; r->flux[1][i] = f1; r->flux[2][i] = f2;
+        r->flux[3][i] = f3; r->flux[4][i] = f4;
+    }
+}
+
+static void hll_row_sweep(rowbuf *r, const fconst *c, int slope, double lambda,
+                          const int mom_order[3])
+{
+    int n = r->n, i, k;
+    double *P = r->tmp[0];  /* reuse: the pressure row is consumed before tmp is written */
+    double *Pcopy = (double *)malloc(sizeof(double) * (size_t)n);
+    double *U1[5];
+    double *blk = (double *)malloc(sizeof(double) * (size_t)n * 5);
+    for (k = 0; k < 5; k++) U1[k] = blk + (size_t)n * k;
+    (void)P;
+    /* pressure + floors on the fluid, predictor (PCswitch RK_PREDICT, SSPRK) */
+    hll_pressure_row(r->u, Pcopy, n, c, mom_order);
+    hll_row_flux(r, r->u, Pcopy, c, slope);
+    for (k = 0; k < 5; k++)
+        for (i = 0; i < n; i++)
+            U1[k][i] = r->u[k][i] - lambda * (r->flux[k][i] - r->flux[k][wrap(i - 1, n)]);
+    /* pressure + floors on the predicted state, corrector */
+    hll_pressure_row(U1, Pcopy, n, c, mom_order);
+    hll_row_flux(r, U1, Pcopy, c, slope);
+    for (k = 0; k < 5; k++)
+        for (i = 0; i < n; i++)
+            r->u[k][i] = .5 * (r->u[k][i] + U1[k][i] -
+                               lambda * (r->flux[k][i] - r->flux[k][wrap(i - 1, n)]));
+    free(blk);
+    free(Pcopy);
+}
+
+/* ------------------------------------------------------------------------------------------
+ * Xin-Jin relaxing TVD (cukern_XinJinHydro_step, cudaFluidStep.cu:2427-2654) with the
+ * per-row freezing speed of cukern_PressureFreezeSolverHydro (cudaFluidStep.cu:2867-2941).
+ * The XJ kernel works in memory slab order; `nslot` is the slab of the normal momentum.
+ * mem[k] = local index that holds memory slab k.
+ * ---------------------------------------------------------------------------------------- */
+static double xj_freeze(double *const s[5], int n, const fconst *c, const int mem[5])
+{
+    /* Uses memory slab 2 (p_x) as the normal momentum whatever the sweep direction, as the
+     * reference kernel does.  Max of |px|/rho + c_s over the row, NaNs never win. */
+    int i;
+    double cmax = 0.0;
+    for (i = 0; i < n; i++) {
+        double invrho = 1.0 / s[mem[0]][i];
+        double psq = s[mem[3]][i];
+        double px = s[mem[4]][i];
+        double P, locCf;
+        psq = psq * psq + px * px;
+        px = s[mem[2]][i];
+        psq += px * px;
+        P = (s[mem[1]][i] - .5 * psq * invrho) * c->gm1;
+        locCf = fabs(px) * invrho + sqrt(c->gamma * P * invrho);
+        cmax = (locCf > cmax) ? locCf : cmax;
+    }
+    return cmax;
+}
+
+static void xj_stage(double *const Qin[5], double *const Qbase[5], double *const Qout[5],
+                     int n, const fconst *c, double Cf, double lambda, int corrector,
+                     int nslot, int flim, rowbuf *r)
+{
+    /* Qin: state the fluxes are built from; Qbase: state that is updated (corrector) */
+    int i, k;
+    double *P = r->tmp[0], *vx = r->tmp[1];
+    double *L = r->w[0], *R = r->w[1], *dL = r->w[2], *dR = r->w[3];
+    double *prop[5];
+    for (k = 0; k < 5; k++) prop[k] = r->edge[k];
+    for (i = 0; i < n; i++) {
+        double q0 = Qin[0][i], q1 = Qin[1][i], q2 = Qin[2][i], q3 = Qin[3][i], q4 = Qin[4][i];
+        P[i] = c->gm1 * (q1 - .5 * (q4 * q4 + q3 * q3 + q2 * q2) / q0);
+        vx[i] = Qin[nslot][i] / q0;
+    }
+    for (k = 0; k < 5; k++) {
+        for (i = 0; i < n; i++) {
+            double w;
+            double *q = Qin[k];
+            if (k == 0) w = Qin[nslot][i];
+            else if (k == 1) w = vx[i] * (q[i] + P[i]);
+            else if (k == nslot) w = vx[i] * q[i] + P[i];
+            else w = vx[i] * q[i];
+            L[i] = (Cf * q[i] - w);   /* left-going  */
+            R[i] = (Cf * q[i] + w);   /* right-going */
+        }
+        if (corrector) {
+            for (i = 0; i < n; i++) {
+                dL[i] = 0.5 * (L[i] - L[wrap(i - 1, n)]);
+                dR[i] = 0.5 * (R[i] - R[wrap(i - 1, n)]);
+            }
+            /* limited corrections use the unmodified backward differences of the
+             * neighbour, so compute into scratch first */
+            for (i = 0; i < n; i++) {
+                r->edge[5][i] = L[i] - flux_apply(flim, dL[i], dL[wrap(i + 1, n)]);
+                r->edge[6][i] = R[i] + flux_apply(flim, dR[i], dR[wrap(i + 1, n)]);
+            }
+            for (i = 0; i < n; i++) { L[i] = r->edge[5][i]; R[i] = r->edge[6][i]; }
+        }
+        for (i = 0; i < n; i++) {
+            int il = wrap(i - 1, n), ir = wrap(i + 1, n);
+            double base = corrector ? Qbase[k][i] : Qin[k][i];
+            prop[k][i] = base - lambda * (R[i] - R[il] - L[ir] + L[i]);
+        }
+    }
+    for (i = 0; i < n; i++) {
+        double p0 = prop[0][i], p1 = prop[1][i], p2 = prop[2][i], p3 = prop[3][i], p4 = prop[4][i];
+        double w;
+        p0 = (p0 < c->minmass) ? c->minmass : p0;
+        w = .5 * (p2 * p2 + p3 * p3 + p4 * p4) / p0;
+        if ((p1 - w) < p0 * c->mintemp) p1 = w + p0 * c->mintemp;
+        Qout[0][i] = p0; Qout[1][i] = p1; Qout[2][i] = p2; Qout[3][i] = p3; Qout[4][i] = p4;
+    }
+}
+
+static void xj_row_sweep(rowbuf *r, const fconst *c, int flim, double lambda, int dir)
+{
+    /* r->u holds the row in memory slab order for XJ */
+    int n = r->n, k;
+    int mem[5] = {0, 1, 2, 3, 4};
+    int nslot = 1 + dir;
+    double *U1[5];
+    double *blk = (double *)malloc(sizeof(double) * (size_t)n * 5);
+    double Cf;
+    for (k = 0; k < 5; k++) U1[k] = blk + (size_t)n * k;
+    Cf = xj_freeze(r->u, n, c, mem);
+    xj_stage(r->u, r->u, U1, n, c, Cf, 0.25 * lambda, 0, nslot, flim, r);
+    Cf = xj_freeze(U1, n, c, mem);
+    xj_stage(U1, r->u, r->u, n, c, Cf, 0.5 * lambda, 1, nslot, flim, r);
+    free(blk);
+}
+
+/* ------------------------------------------------------------------------------------------
+ * Sweep driver: gather each pencil along dir, run the row scheme, scatter back.
+ * ---------------------------------------------------------------------------------------- */
+static void pencil_geometry(const or_grid *g, int dir, int *n, long *stride, long *npencil)
+{
+    long N = (long)g->nx * g->ny * g->nz;
+    if (dir == 1) { *n = g->nx; *stride = 1; }
+    else if (dir == 2) { *n = g->ny; *stride = g->nx; }
+    else { *n = g->nz; *stride = (long)g->nx * g->ny; }
+    *npencil = N / *n;
+}
+
+static long pencil_base(const or_grid *g, int dir, long p)
+{
+    if (dir == 1) return p * g->nx;
+    if (dir == 2) {
+        long x = p % g->nx, z = p / g->nx;
+        return x + (long)g->nx * g->ny * z;
+    }
+    return p;  /* dir 3: pencils indexed by x + nx*y */
+}
+
+int or_fluid_sweep(double *q, const or_grid *g, const or_step *p, int dir)
+{
+    int n;
+    long stride, npencil;
+    fconst c;
+    double lambda;
+    /* slab order that becomes local [rho, E, p_n, p_t1, p_t2] (cudaFluidStep.cu:1200-1219 for
+     * HLLC, 1864-1882 for HLL); XJ keeps memory order */
+    static const int hllc_map[3][5] = {{0, 1, 2, 3, 4}, {0, 1, 3, 2, 4}, {0, 1, 4, 3, 2}};
+    static const int hll_map[3][5] = {{0, 1, 2, 3, 4}, {0, 1, 3, 2, 4}, {0, 1, 4, 2, 3}};
+    const int *map;
+    int mom_order[3];
+    if (dir < 1 || dir > 3) return OR_ERR_INVALID;
+    if (p->method < 1 || p->method > 3) return OR_ERR_INVALID;
+    pencil_geometry(g, dir, &n, &stride, &npencil);
+    if (n < 3) return OR_OK;  /* cudaFluidStep.cu:313 */
+    c = make_consts(p);
+    lambda = p->dt / p->h[dir - 1];
+    map = (p->method == 2) ? hllc_map[dir - 1] : ((p->method == 1) ? hll_map[dir - 1] : hllc_map[0]);
+    if (p->method == 3) map = hllc_map[0];
+    {
+        /* local index holding memory slabs 2, 3, 4 (pressure solver sums px, py, pz) */
+        int k, m;
+        for (m = 0; m < 3; m++)
+            for (k = 0; k < 5; k++)
+                if (map[k] == 2 + m) mom_order[m] = k;
+    }
+
+#pragma omp parallel
+    {
+        rowbuf r;
+        long pp;
+        rowbuf_alloc(&r, n);
+#pragma omp for schedule(static)
+        for (pp = 0; pp < npencil; pp++) {
+            long b = pencil_base(g, dir, pp);
+            int i, k;
+            for (k = 0; k < 5; k++) {
+                const double *s = q + (long)map[k] * g->slab + b;
+                for (i = 0; i < n; i++) r.u[k][i] = s[(long)i * stride];
+            }
+            if (p->method == 2) hllc_row_sweep(&r, &c, p->slope_limiter, lambda);
+            else if (p->method == 1) hll_row_sweep(&r, &c, p->slope_limiter, lambda, mom_order);
+            else xj_row_sweep(&r, &c, p->flux_limiter, lambda, dir);
+            for (k = 0; k < 5; k++) {
+                double *s = q + (long)map[k] * g->slab + b;
+                for (i = 0; i < n; i++) s[(long)i * stride] = r.u[k][i];
+            }
+        }
+        rowbuf_free(&r);
+    }
+    return OR_OK;
+}
+
+/* ------------------------------------------------------------------------------------------
+ * Boundary conditions along a pencil with the X-kernel semantics of cudaStatics.cu (used
+ * inside the fluid step, where the swept direction is the fastest memory direction).
+ * v[k] points at the first cell of the pencil in slab k; s = stride along the pencil.
+ * ---------------------------------------------------------------------------------------- */
+#define PV(k, i) v[k][(long)(i) * s]
+
+static void bc_pencil_sas(double *v, long s, int n, int mode, int side, int anti, int depth)
+{
+    /* cukern_{x}{minus,plus}{Symmetrize,Antisymmetrize}, extrapolate{FlatConst,Linear}
+     * (cudaStatics.cu:1305-1400).  MIRROR_OFFSET = 1. */
+    int t;
+    double f[4];
+    if (mode == OR_BC_MIRROR) {
+        for (t = 0; t < depth; t++) {
+            if (side == 0) {
+                double a = v[(long)(depth + 1 + t) * s];
+                v[(long)(depth - 1 - t) * s] = anti ? -a : a;
+            } else {
+                double a = v[(long)(n - depth - 2 - t) * s];
+                v[(long)(n - depth + t) * s] = anti ? -a : a;
+            }
+        }
+    } else if (mode == OR_BC_CONST) {
+        if (side == 0) {
+            double a = v[(long)depth * s];
+            for (t = 0; t < depth; t++) v[(long)t * s] = a;
+        } else {
+            double a = v[(long)(n - depth - 1) * s];
+            for (t = 0; t < depth; t++) v[(long)(n - depth + t) * s] = a;
+        }
+    } else if (mode == OR_BC_LINEAR) {
+        if (side == 0) {
+            /* phi[t] = phi[depth] + (depth - t)*(phi[depth] - phi[depth+1]) */
+            for (t = 0; t < 4; t++) f[t] = v[(long)(t + depth) * s];
+            for (t = 0; t < depth; t++) v[(long)t * s] = v[(long)depth * s] + (double)(depth - t) * (f[0] - f[1]);
+        } else {
+            /* base = n-depth-1; phi[base+t+2] = f1 + (t+1)(f1-f0).  The reference also writes
+             * one cell past the end of the pencil (t = depth-1); that write is dropped. */
+            long b = n - depth - 1;
+            for (t = 0; t < 4; t++) f[t] = v[(b + t) * s];
+            for (t = 0; t < depth; t++) {
+                long dst = b + t + 2;
+                if (dst < n) v[dst * s] = f[1] + (double)(t + 1) * (f[1] - f[0]);
+            }
+        }
+    }
+}
+
+/* cukern_SetOutflowX (cudaStatics.cu:462-545) along one pencil of all five slabs.
+ * nd = physical normal direction (1..3).  restFrmSpeed: 1.05 on the - side, -1.198-.0047 i
+ * on the + side (cudaStatics.cu:379-384).
+ * The reference's - side kernel indexes from depth cells before the pencil start (it writes
+ * the depth cells preceding the row and reads cell 0); this restatement applies the
+ * evident intent, reading cell `depth` and writing cells 0..depth-1 like the + side. */
+static void bc_pencil_outflow(double *v[5], long s, int n, int side, int nd, int depth)
+{
+    int t, k;
+    long src = (side == 1) ? (n - 1 - depth) : depth;
+    double a = v[1 + nd][src * s];
+    int direct = side ? 1 : -1;
+    if (a * direct > 0) {
+        for (k = 0; k < 5; k++) {
+            double val = v[k][src * s];
+            for (t = 0; t < depth; t++) {
+                long dst = side ? (src + 1 + t) : t;
+                v[k][dst * s] = val;
+            }
+        }
+    } else {
+        double rho = v[0][src * s];
+        double E0 = v[1][src * s];
+        double p1x = v[2][src * s], p1y = v[3][src * s], p1z = v[4][src * s];
+        for (t = 0; t < depth; t++) {
+            long dst = side ? (src + 1 + t) : t;
+            int ridx = side ? (depth + t) : t;
+            double rf = side ? (-1.198 - .0047 * t) : 1.05;
+            double E = E0, p1, p2;
+            (void)ridx;
+            v[0][dst * s] = rho;
+            p1 = p1x; p2 = rho * 0.0;
+            v[2][dst * s] = p2;
+            E += .5 * (p2 - p1) * (p2 + p1) / rho;
+            p1 = p1y; p2 = (nd == 1) ? rho * rf : rho * (p1y / rho);
+            v[3][dst * s] = p2;
+            E += .5 * (p2 - p1) * (p2 + p1) / rho;
+            p1 = p1z; p2 = rho * 0.0;
+            v[4][dst * s] = p2;
+            E += .5 * (p2 - p1) * (p2 + p1) / rho;
+            v[1][dst * s] = E;
+        }
+    }
+}
+
+int or_fluid_boundary(double *q, const or_grid *g, const int32_t bc[6], int dir, int depth)
+{
+    int n, side;
+    long stride, npencil;
+    if (dir < 1 || dir > 3) return OR_ERR_INVALID;
+    pencil_geometry(g, dir, &n, &stride, &npencil);
+    for (side = 0; side < 2; side++) {
+        int mode = bc[2 * (dir - 1) + side];
+        long pp;
+        if (mode == OR_BC_CIRCULAR || mode == OR_BC_STATIONARY) continue;
+        if (mode == OR_BC_WALL || mode == OR_BC_FREEBALANCE) return OR_ERR_NOIMPL;
+        for (pp = 0; pp < npencil; pp++) {
+            long b = pencil_base(g, dir, pp);
+            double *v[5];
+            int k;
+            for (k = 0; k < 5; k++) v[k] = q + (long)k * g->slab + b;
+            if (mode == OR_BC_OUTFLOW) {
+                bc_pencil_outflow(v, stride, n, side, dir, depth);
+            } else {
+                for (k = 0; k < 5; k++) {
+                    int anti = (k >= 2) && (k - 1 == dir);  /* vectorComponent == direction */
+                    bc_pencil_sas(v[k], stride, n, mode, side, anti, depth);
+                }
+            }
+        }
+    }
+    return OR_OK;
+}
+
+/* ------------------------------------------------------------------------------------------
+ * performFluidUpdate_3D (flux.cu:27-165)
+ * ---------------------------------------------------------------------------------------- */
+int or_fluid_step_3d(double *q, const or_grid *g, const or_step *p, const int32_t bc[6],
+                     int sweep_dir, int step_number)
+{
+    static const int fluxcall[3][6] = {{1, 2, 1, 2, 3, 3}, {3, 1, 2, 3, 1, 2}, {2, 3, 3, 1, 2, 1}};
+    int sweep = (step_number + 3 * (sweep_dir > 0)) % 6;
+    int nstep, rc;
+    int ext[3];
+    ext[0] = g->nx; ext[1] = g->ny; ext[2] = g->nz;
+    if (g->ny == 1 && g->nz == 1) {
+        rc = or_fluid_sweep(q, g, p, 1);
+        if (rc) return rc;
+        return or_fluid_boundary(q, g, bc, 1, 4);
+    }
+    for (nstep = 0; nstep < 3; nstep++) {
+        int d = fluxcall[nstep][sweep];
+        if (ext[d - 1] > 3) {
+            rc = or_fluid_sweep(q, g, p, d);
+            if (rc) return rc;
+            rc = or_fluid_boundary(q, g, bc, d, 4);
+            if (rc) return rc;
+        }
+    }
+    return OR_OK;
+}
+
+/* ------------------------------------------------------------------------------------------
+ * Soundspeed and CFL
+ * ---------------------------------------------------------------------------------------- */
+void or_soundspeed(const double *q, const or_grid *g, double gamma, double *cs)
+{
+    long N = (long)g->nx * g->ny * g->nz, x;
+    double gg1 = gamma * (gamma - 1);
+    const double *rho = q, *E = q + g->slab, *px = q + 2 * g->slab, *py = q + 3 * g->slab,
+                 *pz = q + 4 * g->slab;
+#pragma omp parallel for schedule(static)
+    for (x = 0; x < N; x++) {
+        double rhoinv = 1 / rho[x];
+        double csq = gg1 * (E[x] - .5 * (px[x] * px[x] + py[x] * py[x] + pz[x] * pz[x]) * rhoinv) * rhoinv;
+        if (csq < 0.0) csq = 0.0;
+        cs[x] = sqrt(csq);
+    }
+}
+
+double or_cfl_timestep(const double *q, const double *cs, const or_grid *g, const double h[3],
+                       const int32_t global_rez[3], int method)
+{
+    long N = (long)g->nx * g->ny * g->nz, x;
+    int spacedim = 0, sim;
+    int algo_xj;
+    double tmin = 1e38;
+    const double *rho = q, *px = q + 2 * g->slab, *py = q + 3 * g->slab, *pz = q + 4 * g->slab;
+    double hmin;
+    if (global_rez[1] > 1) spacedim = 1;
+    if (global_rez[2] > 1) spacedim = 2;
+    sim = spacedim + 1;
+    /* ctype table (cflTimestep.cu:175-193): 1-D Xin-Jin uses the HLL/HLLC kernel */
+    algo_xj = (method == 3) && (sim > 1);
+    hmin = h[0];
+    if (sim > 1 && h[1] < hmin) hmin = h[1];
+    if (sim > 2 && h[2] < hmin) hmin = h[2];
+#pragma omp parallel for reduction(min : tmin) schedule(static)
+    for (x = 0; x < N; x++) {
+        double u, v;
+        if (!algo_xj) {
+            double p;
+            if (sim == 1) {
+                p = fabs(px[x]);
+            } else {
+                double pp = px[x], qq;
+                pp = pp * pp;
+                qq = py[x];
+                pp = pp + qq * qq;
+                if (sim > 2) {
+                    qq = pz[x];
+                    pp = pp + qq * qq;
+                }
+                p = sqrt(pp);
+            }
+            u = p / rho[x] + cs[x];
+            u = hmin / u;
+        } else {
+            double r = rho[x];
+            u = h[0] / (fabs(px[x]) / r + cs[x]);
+            v = h[1] / (fabs(py[x]) / r + cs[x]);
+            u = (u < v) ? u : v;
+            if (sim > 2) {
+                v = h[2] / (fabs(pz[x]) / r + cs[x]);
+                u = (u < v) ? u : v;
+            }
+        }
+        if (u < tmin) tmin = u;   /* NaN never wins, as in the reference's ternary min */
+    }
+    if (tmin > 1e37) tmin = 1e37;  /* per-thread initial value in the kernel */
+    if (method == 1 || method == 2) tmin = tmin / 2;
+    return tmin;
+}
+
+/* ------------------------------------------------------------------------------------------
+ * freezeAndPtot (hydro)
+ * ---------------------------------------------------------------------------------------- */
+void or_freeze_and_ptot(double *q, const or_grid *g, double gamma, double cs_min,
+                        double *ptot, double *freeze)
+{
+    long rows = (long)g->ny * g->nz, r;
+    double gm1 = gamma - 1.0, cs0sq = cs_min * cs_min;
+#pragma omp parallel for schedule(static)
+    for (r = 0; r < rows; r++) {
+        long x0 = r * g->nx, x;
+        double CsMax = 0.0;
+        double *rho = q, *E = q + g->slab, *px = q + 2 * g->slab, *py = q + 3 * g->slab,
+               *pz = q + 4 * g->slab;
+        for (x = x0; x < x0 + g->nx; x++) {
+            double rhoinv = 1.0 / rho[x];
+            double psqhf = .5 * (px[x] * px[x] + py[x] * py[x] + pz[x] * pz[x]);
+            double P = gm1 * (E[x] - psqhf * rhoinv);
+            double Cs;
+            if (gamma * P * rhoinv < cs0sq) {
+                P = cs0sq / (gamma * rhoinv);
+                E[x] = psqhf * rhoinv + P / gm1;
+            }
+            ptot[x] = P;
+            Cs = sqrt(gamma * P * rhoinv) + fabs(px[x] * rhoinv);
+            if (Cs > CsMax) CsMax = Cs;
+        }
+        freeze[r] = CsMax;
+    }
+}
+
+/* ------------------------------------------------------------------------------------------
+ * Per-array boundary conditions in XYZ storage (cudaStatics mex semantics)
+ * ---------------------------------------------------------------------------------------- */
+int or_array_boundary(double *phi, const or_grid *g, int bc_mode, int dir, int side,
+                      int vec_component, int depth)
+{
+    int n;
+    long stride, npencil, pp;
+    int anti = (vec_component == dir);
+    if (dir < 1 || dir > 3 || side < 0 || side > 1) return OR_ERR_INVALID;
+    if (bc_mode == OR_BC_CIRCULAR || bc_mode == OR_BC_STATIONARY) return OR_OK;
+    if (bc_mode == OR_BC_WALL || bc_mode == OR_BC_FREEBALANCE) return OR_ERR_NOIMPL;
+    if (bc_mode == OR_BC_OUTFLOW) return OR_OK;  /* handled by the fluid-level entry */
+    if (bc_mode == OR_BC_LINEAR && dir != 1) return OR_ERR_NOIMPL;  /* cudaStatics.cu:1187-1220 */
+    pencil_geometry(g, dir, &n, &stride, &npencil);
+    for (pp = 0; pp < npencil; pp++) {
+        double *v = phi + pencil_base(g, dir, pp);
+        long s = stride;
+        int q;
+        if (dir == 1 || bc_mode == OR_BC_LINEAR) {
+            bc_pencil_sas(v, s, n, bc_mode, side, anti, depth);
+            continue;
+        }
+        if (bc_mode == OR_BC_MIRROR) {
+            for (q = 0; q < depth; q++) {
+                double a;
+                if (side == 0) {
+                    /* y: 2*depth-1+MIRROR_OFFSET-q; z: 2*depth+MIRROR_OFFSET-q
+                     * (cudaStatics.cu:1413-1421 vs 1471-1481) */
+                    int src = (dir == 2) ? (2 * depth - q) : (2 * depth + 1 - q);
+                    a = v[(long)src * s];
+                    v[(long)q * s] = anti ? -a : a;
+                } else {
+                    a = v[(long)(n - 1 - 2 * depth + q) * s];
+                    v[(long)(n - 1 - q) * s] = anti ? -a : a;
+                }
+            }
+        } else if (bc_mode == OR_BC_CONST) {
+            if (side == 0) {
+                double f = v[(long)depth * s];
+                for (q = 0; q < depth; q++) v[(long)q * s] = f;
+            } else {
+                /* y/z + side copies cell n-depth (cudaStatics.cu:1443-1448, 1524-1531) */
+                double f = v[(long)(n - depth) * s];
+                for (q = 0; q < depth; q++) v[(long)(n - 1 - q) * s] = f;
+            }
+        }
+    }
+    return OR_OK;
+}
+
+void or_statics_fade(double *phi, const double *statics, int64_t n, int64_t pitch)
+{
+    int64_t i;
+    for (i = 0; i < n; i++) {
+        long xaddr = (long)statics[i];
+        double f0 = statics[i + pitch];
+        double c = statics[i + 2 * pitch];
+        if (c != 1.0) {
+            double wval = f0 * c + (1.0 - c) * phi[xaddr];
+            if (isnan(wval)) wval = f0 * c;
+            phi[xaddr] = wval;
+        } else {
+            phi[xaddr] = f0;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------------------------
+ * Two-fluid drag (cudaSource2FluidDrag.cu)
+ * thermo: [gamma, mass, mu0, muTindex, sigma0, sigmaTindex, kBolt, Cisothermal]
+ * ---------------------------------------------------------------------------------------- */
+void or_drag_params(const double tg[8], const double td[8], double dt, double out[11])
+{
+    /* cudaSource2FluidDrag.cu:196-218 */
+    double gam = tg[0];
+    double nu0 = tg[2], nupow = tg[3], lampow = tg[5];
+    double ddust = sqrt(td[4] / 3.141592653589793);
+    double mgas = tg[1], mdust = td[1];
+    out[0] = nu0;
+    out[1] = -nupow;
+    out[2] = lampow;
+    out[3] = mgas * (gam - 1.0) / (298.15 * tg[6]);
+    out[4] = sqrt(2.0) * mgas / (tg[4] * ddust);
+    out[5] = ddust / nu0;
+    out[6] = td[4] / (1.0 * mdust);
+    out[7] = dt;
+    out[8] = (gam - 1.0);
+    out[9] = .25 * td[4] / mdust;
+    out[10] = 16 * (gam - 1.0) / 3.0;
+}
+
+/* allregimeCdrag (cudaSource2FluidDrag.cu:819-833) */
+static double allregime_cdrag(double Re, double Kn)
+{
+    double cunningham = 1 + Kn * (1.142 + 1 * 0.558 * exp(-0.999 / Kn));
+    double C_drag = (3 / Re + .45 * pow(Re, -.319) + .0509 * Re / (8710 + Re)) / cunningham;
+    return C_drag;
+}
+
+/* cukern_GasDustDrag_GeneralLinearCore with srcBlock = 0 (cudaSource2FluidDrag.cu:836-890):
+ * returns k for |dv| = magdv and specific internal energy u; sets *skip when |dv| < 1e-9 */
+static double drag_k(const double dp[11], double rhoA, double rhoB, double magdv, double u, int *skip)
+{
+    double Tn, Re, Kn, Cd_hat;
+    if (magdv < 1e-9) { *skip = 1; return 0; }
+    *skip = 0;
+    Tn = dp[3] * u;
+    Re = dp[5] * rhoA * magdv * pow(Tn, dp[1]);
+    Kn = dp[4] * pow(Tn, dp[2]) / rhoA;
+    Cd_hat = allregime_cdrag(Re, Kn);
+    return Cd_hat * magdv * (rhoA + rhoB) * dp[6];
+}
+
+/* cukern_prepareForERK_h0 (cudaSource2FluidDrag.cu:1883-1908) + cukern_LogTrapSolve
+ * (cudaSource2FluidDrag.cu:1531-1686) for one cell; gas/dust point at the cell in slab 0. */
+static void logtrap_cell(double *gas, double *dust, long S, const double dp[11], double t, int order)
+{
+    double dv, dvsq, press, t0, t1, t2;
+    double mu, k, dv_i, dv_t, duint, rhoginv, pdustsq, vstick, q;
+    int skip;
+    /* prepare: [|dv|, u] */
+    dv = (gas[2 * S]) / gas[0] - dust[2 * S] / dust[0];
+    dvsq = dv * dv;
+    dv = (gas[3 * S]) / gas[0] - dust[3 * S] / dust[0];
+    dvsq += dv * dv;
+    dv = (gas[4 * S]) / gas[0] - dust[4 * S] / dust[0];
+    dvsq += dv * dv;
+    press = (gas[S] - .5 * (gas[2 * S] * gas[2 * S] + gas[3 * S] * gas[3 * S] + gas[4 * S] * gas[4 * S]) / gas[0]);
+    t0 = sqrt(dvsq);         /* tmp slab 0 */
+    t1 = press / gas[0];     /* tmp slab 1 */
+    t2 = 0;                  /* tmp slab 2 */
+
+    mu = dust[0] / (gas[0] + dust[0]);
+    k = drag_k(dp, gas[0], dust[0], t0, t1, &skip);
+    t2 = skip ? 0 : k;       /* resetAccumulator */
+    k = t2;
+    dv_i = t0;
+    dv_t = dv_i * exp(-t * k);
+    dvsq = dv_t * dv_t;
+    duint = -.5 * dv_i * dv_i * mu * expm1(-2 * k * t);
+    t0 = sqrt(dvsq);
+    t1 += duint;
+    k = drag_k(dp, gas[0], dust[0], t0, t1, &skip);
+    if (!skip) t2 += k;      /* accumulate */
+    if (order == 3) {
+        t1 -= duint;
+        k = .25 * (t2);
+        dv_t = dv_i * exp(-t * k);
+        dvsq = dv_t * dv_t;
+        duint = -0.5 * dv_i * dv_i * mu * expm1(-2 * k * t);
+        t0 = sqrt(dvsq);
+        t1 += duint;
+        k = drag_k(dp, gas[0], dust[0], t0, t1, &skip);
+        t0 = skip ? 0 : k;   /* written into slab 0 with reset */
+        k = (0.16666666666666666667 * t2 + 0.66666666666666666667 * t0);
+    } else {
+        k = .5 * t2;
+    }
+    mu = mu * gas[0];
+    rhoginv = 1.0 / gas[0];
+
+    pdustsq = -dust[2 * S] * dust[2 * S];
+    vstick = (gas[2 * S] + dust[2 * S]) / (gas[0] + dust[0]);
+    dv_i = (gas[2 * S]) * rhoginv - dust[2 * S] / dust[0];
+    dv_t = dv_i * exp(-t * k);
+    gas[2 * S] = gas[0] * vstick + dv_t * mu;
+    dust[2 * S] = q = dust[0] * vstick - dv_t * mu;
+    pdustsq += q * q;
+
+    pdustsq -= dust[3 * S] * dust[3 * S];
+    vstick = (gas[3 * S] + dust[3 * S]) / (gas[0] + dust[0]);
+    dv_i = (gas[3 * S]) * rhoginv - dust[3 * S] / dust[0];
+    dv_t = dv_i * exp(-t * k);
+    gas[3 * S] = gas[0] * vstick + dv_t * mu;
+    dust[3 * S] = q = dust[0] * vstick - dv_t * mu;
+    pdustsq += q * q;
+
+    pdustsq -= dust[4 * S] * dust[4 * S];
+    vstick = (gas[4 * S] + dust[4 * S]) / (gas[0] + dust[0]);
+    dv_i = (gas[4 * S]) * rhoginv - dust[4 * S] / dust[0];
+    dv_t = dv_i * exp(-t * k);
+    gas[4 * S] = gas[0] * vstick + dv_t * mu;
+    dust[4 * S] = q = dust[0] * vstick - dv_t * mu;
+    pdustsq += q * q;
+
+    gas[S] -= .5 * pdustsq / dust[0];
+}
+
+void or_drag_logtrap_cells(double *gas, double *dust, int64_t n, int64_t slab,
+                           const double dp[11], double dt, int order)
+{
+    int64_t i;
+#pragma omp parallel for schedule(static)
+    for (i = 0; i < n; i++) logtrap_cell(gas + i, dust + i, slab, dp, dt, order);
+}
+
+int or_drag_2fluid(double *gas, double *dust, const or_grid *g, const double tg[8],
+                   const double td[8], double dt, int method)
+{
+    double dp[11];
+    long N = (long)g->nx * g->ny * g->nz;
+    or_drag_params(tg, td, dt, dp);
+    if (method == 4 || method == 5) {
+        or_drag_logtrap_cells(gas, dust, N, g->slab, dp, dt, method == 4 ? 2 : 3);
+        return OR_OK;
+    }
+    return OR_ERR_NOIMPL;
+}

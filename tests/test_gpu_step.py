@@ -1,0 +1,220 @@
+"""GPU parity of the full fluid step (Strang sweep order + boundary fill), the CFL reduction,
+freezeAndPtot, the per-array boundary conditions and the drag source against the CPU oracle."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+import riemann_exact as rx
+from gpuimogen_b200 import problems
+from helpers import bits_equal, first_diff, host, max_rel, rel_l1, to_fluid
+
+pytestmark = pytest.mark.gpu
+
+BCSETS = [
+    ["circular"] * 6,
+    ["const", "const", "mirror", "mirror", "outflow", "outflow"],
+    ["outflow", "outflow", "const", "circular", "mirror", "const"],
+    ["mirror", "linear", "circular", "circular", "const", "mirror"],
+]
+
+
+@pytest.mark.parametrize("shape", [(24, 20, 18), (32, 26, 1), (70, 1, 1), (12, 4, 30)])
+@pytest.mark.parametrize("bcs", range(len(BCSETS)))
+@pytest.mark.parametrize("method", [2, 1, 3])
+def test_fluidstep_strict_bitexact(cuda, ib, po, shape, bcs, method):
+    bc = BCSETS[bcs]
+    for d in range(3):  # mirror/outflow need >= 2*halo+1 cells; degenerate axes stay circular
+        if shape[d] < 12:
+            bc = list(bc)
+            bc[2 * d] = bc[2 * d + 1] = "circular"
+    n = shape[0] * shape[1] * shape[2]
+    q = problems.random_smooth(shape, gamma=5 / 3.0, seed=31 + bcs, amp=0.3)
+    h = [1.0 / s for s in shape]
+    sp = po.step_params(0.0, h, 5 / 3.0, rho_min=1e-5, method=method, slope="mc")
+    ref = q.copy()
+    ib.use_variant("strict")
+    try:
+        fl = to_fluid(q, shape, bc=bc, gamma=5 / 3.0)
+        geo = ib.Geometry(shape, h)
+        for it in range(3):
+            tau = po.cfl_timestep(ref, shape, 5 / 3.0, h, method)
+            dt = 0.4 * tau
+            sp.dt = dt
+            tau_g = ib.cflTimestepFused(fl, 5 / 3.0, geo, method)
+            assert tau_g == tau, (it, tau_g, tau)
+            for sd in (1, -1):
+                po.fluid_step_3d(ref, shape, sp, bc, sd, it)
+                ib.fluidstep([fl], geo, [dt, 1, sd, it, method], ib.numerics(slope="mc"))
+            out = host(fl)
+            assert bits_equal(out, ref, n), (it, first_diff(out, ref, n))
+    finally:
+        ib.use_variant("product")
+
+
+def test_cfl_soundspeed_freeze_strict(cuda, ib, po):
+    for shape in [(33, 17, 9), (64, 1, 1), (40, 30, 1)]:
+        n = shape[0] * shape[1] * shape[2]
+        q = problems.random_jumpy(shape, seed=3)
+        h = (0.02, 0.03, 0.05)
+        ib.use_variant("strict")
+        try:
+            fl = to_fluid(q, shape)
+            geo = ib.Geometry(shape, h)
+            cs = ib.cudaSoundspeed(fl, 1.4)
+            cs_ref = po.soundspeed(q, shape, 1.4)
+            assert np.array_equal(cs.cpu().numpy(), cs_ref)
+            for method in (1, 2, 3):
+                t_ref = po.cfl_timestep(q, shape, 1.4, h, method, cs_ref)
+                assert ib.cflTimestep(fl, cs, geo, method) == t_ref
+                assert ib.cflTimestepFused(fl, 1.4, geo, method) == t_ref
+            ref = q.copy()
+            ptot_ref, fr_ref = po.freeze_and_ptot(ref, shape, 1.4, 0.9)
+            ptot, fr = ib.freezeAndPtot(fl, 1.4, 1, 0.9)
+            assert np.array_equal(ptot.cpu().numpy(), ptot_ref)
+            assert np.array_equal(fr.cpu().numpy(), fr_ref)
+            assert bits_equal(host(fl), ref, n)   # E floored in place where c_s < cs_min
+        finally:
+            ib.use_variant("product")
+
+
+def test_cfl_device_result_and_nan_ignored(cuda, ib, po):
+    shape = (50, 20, 10)
+    n = 50 * 20 * 10
+    q = problems.random_smooth(shape, seed=4)
+    q[0, 17] = np.nan          # a NaN cell never wins the min, as in the reference's ternaries
+    fl = to_fluid(q, shape)
+    geo = ib.Geometry(shape)
+    tau_dev = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ib.cflTimestepFused(fl, 1.4, geo, 2, tau_device=tau_dev)
+    ref = po.cfl_timestep(q, shape, 1.4, geo.h, 2)
+    assert math.isfinite(ref)
+    assert abs(float(tau_dev.item()) - ref) <= 1e-15 * ref
+    # repeated calls reuse the reduction scratch correctly
+    for _ in range(3):
+        assert abs(ib.cflTimestepFused(fl, 1.4, geo, 2) - ref) <= 1e-15 * ref
+
+
+@pytest.mark.parametrize("mode", ["mirror", "const", "linear"])
+@pytest.mark.parametrize("direction", [1, 2, 3])
+def test_cudaStatics_per_array_strict(cuda, ib, po, mode, direction):
+    shape = (14, 12, 11)
+    n = 14 * 12 * 11
+    q = problems.random_smooth(shape, seed=8)
+    bc = ["circular"] * 6
+    bc[2 * (direction - 1)] = bc[2 * (direction - 1) + 1] = mode
+    fl = to_fluid(q, shape, bc=bc)
+    ref = q.copy()
+    for slab in range(5):
+        vec = slab - 1 if slab >= 2 else 0
+        phi = ref[slab, :n].copy()
+        rc0 = po.array_boundary(phi, shape, mode, direction, 0, vec)
+        rc1 = po.array_boundary(phi, shape, mode, direction, 1, vec)
+        if rc0 or rc1:
+            with pytest.raises(ib.ImogenError):
+                ib.cudaStatics(fl, slab, direction)
+            return
+        ref[slab, :n] = phi
+        ib.cudaStatics(fl, slab, direction)
+    assert bits_equal(host(fl), ref, n), first_diff(host(fl), ref, n)
+
+
+def test_statics_fade(cuda, ib, po):
+    shape = (16, 8, 4)
+    n = 16 * 8 * 4
+    q = problems.random_smooth(shape, seed=2)
+    rng = np.random.default_rng(0)
+    idx = rng.choice(n, size=40, replace=False).astype(np.float64)
+    st = np.stack([idx, rng.uniform(0.5, 2, 40), np.where(np.arange(40) % 3 == 0, 1.0, 0.3)])
+    ref = q.copy()
+    phi = ref[0, :n].copy()
+    for _ in range(3):  # fluid step applies the density statics three times per sweep direction
+        po.statics_fade(phi, st)
+    ref[0, :n] = phi
+    fl = to_fluid(q, shape, bc=["circular"] * 6,
+                  statics=[torch.from_numpy(st).cuda()] + [None] * 4)
+    ib.setFluidBoundary(fl, 1)
+    out = host(fl)
+    assert np.array_equal(out[0, :n], ref[0, :n])
+
+
+@pytest.mark.parametrize("method", [4, 5])
+def test_drag_logtrap_matches_oracle(cuda, ib, po, method):
+    shape = (64, 32, 1)
+    n = 64 * 32
+    rng = np.random.default_rng(1)
+    rho_g = 1.0 + 0.1 * rng.uniform(-1, 1, n)
+    gas = problems.pack(shape, rho_g, 0, rho_g * rng.uniform(-1e-2, 1e-2, n), rho_g * rng.uniform(-1e-2, 1e-2, n), 0)
+    gas[1, :n] = 1.0 / (5 / 3.0 - 1) + 0.5 * (gas[2, :n] ** 2 + gas[3, :n] ** 2) / rho_g
+    rho_d = rho_g * 10 ** rng.uniform(-2, 0, n)
+    dust = problems.pack(shape, rho_d, 0, rho_d * rng.uniform(-2e-2, 2e-2, n), 0, 0)
+    dust[1, :n] = 0.5 * dust[2, :n] ** 2 / rho_d + 1e-4 * rho_d
+    tg = [5 / 3.0, 3.3e-27, 8.4e-6, 0.7, 2.4e-19, 0.2, 1.381e-23, -1]
+    td = [1.01, 3e-11, 0, 0, math.pi * 25e-12, 0, 1.381e-23, 0.1]
+    g_ref, d_ref = gas.copy(), dust.copy()
+    po.drag_2fluid(g_ref, d_ref, shape, tg, td, 0.05, method)
+    fg, fd = to_fluid(gas, shape), to_fluid(dust, shape)
+    ib.cudaSource2FluidDrag(fg, fd, tg, td, ib.Geometry(shape), [0.05, method])
+    # transcendental functions (pow, exp, expm1) come from CUDA's libdevice on the GPU and glibc
+    # on the CPU: compare within a few ulp-scaled relative error
+    assert max_rel(host(fg), g_ref, n) < 1e-12
+    assert max_rel(host(fd), d_ref, n) < 1e-12
+    assert not np.array_equal(g_ref[2, :n], gas[2, :n])   # the drag did act
+
+
+def test_sod_gpu_matches_oracle_and_exact(cuda, ib, po):
+    n = 1024
+    q = problems.sod(n)
+    shape = (n, 1, 1)
+    fl = to_fluid(q, shape, bc="const", gamma=1.4)
+    geo = ib.Geometry(shape)
+    tm = ib.TimeManager(cfl=0.4, tmax=0.2)
+    while tm.running:
+        ib.run_iteration([fl], geo, tm, 2)
+    out = host(fl)
+    x = (np.arange(n) + 0.5) / n
+    ex = rx.sample(x, tm.time, 0.5, (1.0, 0.0, 1.0), (0.125, 0.0, 0.1), 1.4)
+    l1 = np.mean(np.abs(out[0, :n] - ex[0]))
+    assert abs(tm.time - 0.2) < 1e-14
+    assert l1 < 1.0e-3, l1
+    # oracle replay with the same dt sequence semantics
+    ref = problems.sod(n)
+    sp = po.step_params(0.0, geo.h, 1.4, method=2)
+    t, it, kc = 0.0, 0, 0.0
+    while t < 0.2 * (1 - 1e-14):
+        dt = 0.4 * po.cfl_timestep(ref, shape, 1.4, geo.h, 2)
+        if t + 2 * dt > 0.2:
+            dt = .5 * (0.2 - t)
+        sp.dt = dt
+        po.fluid_step_3d(ref, shape, sp, ["const"] * 6, 1, it)
+        po.fluid_step_3d(ref, shape, sp, ["const"] * 6, -1, it)
+        y = 2 * dt - kc
+        tn = t + y
+        kc = (tn - t) - y
+        t = tn
+        it += 1
+    assert it == tm.iteration
+    assert np.all(rel_l1(out, ref, n) <= 1e-12), rel_l1(out, ref, n)
+
+
+def test_kelvin_helmholtz_product_vs_oracle(cuda, ib, po):
+    """3-D HLLC with the MC limiter, periodic: relative L1 per field after 10 iterations."""
+    shape = (48, 48, 48)
+    n = 48 ** 3
+    q = problems.kelvin_helmholtz(shape, seed=7)
+    fl = to_fluid(q, shape, gamma=5 / 3.0)
+    geo = ib.Geometry(shape)
+    ref = q.copy()
+    sp = po.step_params(0.0, geo.h, 5 / 3.0, method=2, slope="mc")
+    num = ib.numerics(slope="mc")
+    tm = ib.TimeManager(cfl=0.4)
+    for it in range(10):
+        dt_ref = 0.4 * po.cfl_timestep(ref, shape, 5 / 3.0, geo.h, 2)
+        sp.dt = dt_ref
+        po.fluid_step_3d(ref, shape, sp, ["circular"] * 6, 1, it)
+        po.fluid_step_3d(ref, shape, sp, ["circular"] * 6, -1, it)
+        dt = ib.run_iteration([fl], geo, tm, 2, num)
+        assert abs(dt - dt_ref) <= 1e-13 * dt_ref
+    err = rel_l1(host(fl), ref, n)
+    assert np.all(err <= 1e-12), err
