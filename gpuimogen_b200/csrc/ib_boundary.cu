@@ -187,7 +187,7 @@ int launch_array_boundary(double *phi, const int grid[3], int mode, int dir, int
     if (mode == IB_BC_LINEAR && dir != 1) return IB_ERROR_NOIMPLEMENT;  // cudaStatics.cu:1187-1220
     if (!(mode == IB_BC_MIRROR || mode == IB_BC_CONST || mode == IB_BC_LINEAR)) return IB_ERROR_INVALID_ARGS;
     const int n = grid[dir - 1];
-    if (n < 2 * halo + 1) return IB_ERROR_INVALID_ARGS;
+    if (n < 2 * halo + 2) return IB_ERROR_INVALID_ARGS;  // the z mirror reads cell 2*halo+1
     const int64_t N = (int64_t)grid[0] * grid[1] * grid[2];
     const int64_t np = N / n;
     PencilIdx pi{grid[0], grid[1], grid[2], dir};
@@ -197,11 +197,13 @@ int launch_array_boundary(double *phi, const int grid[3], int mode, int dir, int
 }
 
 // cukern_applySpecial_fade (cudaStatics.cu:1240-1266)
-__global__ void statics_kernel(double *phi, const double *statics, int64_t count, int64_t pitch)
+__global__ void statics_kernel(double *phi, const double *statics, int64_t count, int64_t pitch, int64_t numel)
 {
     const int64_t i = threadIdx.x + (int64_t)blockIdx.x * blockDim.x;
     if (i >= count) return;
-    const int64_t xaddr = (int64_t)statics[i];
+    const double xd = statics[i];
+    if (!(xd >= 0.0 && xd < (double)numel)) return;  // indices outside the array are ignored
+    const int64_t xaddr = (int64_t)xd;
     const double f0 = statics[i + pitch];
     const double c = statics[i + 2 * pitch];
     if (c != 1.0) {
@@ -213,11 +215,11 @@ __global__ void statics_kernel(double *phi, const double *statics, int64_t count
     }
 }
 
-int launch_statics(double *phi, const ib_statics *sl, cudaStream_t st)
+int launch_statics(double *phi, const ib_statics *sl, int64_t numel, cudaStream_t st)
 {
     if (sl == nullptr || sl->data == nullptr || sl->count <= 0) return IB_SUCCESSFUL;
     if (sl->pitch < sl->count) return IB_ERROR_INVALID_ARGS;
-    statics_kernel<<<(unsigned)((sl->count + 127) / 128), 128, 0, st>>>(phi, sl->data, sl->count, sl->pitch);
+    statics_kernel<<<(unsigned)((sl->count + 127) / 128), 128, 0, st>>>(phi, sl->data, sl->count, sl->pitch, numel);
     return check_launch();
 }
 

@@ -187,10 +187,11 @@ static int fluid_boundary(ib_fluid *f, int dir, cudaStream_t st)
     const int64_t S = f->grid.slab_pitch;
     int rc;
     if (!has_statics(f)) return launch_fluid_boundary(f->q, S, grid, f->bc, f->halo, dir, st);
-    if ((rc = launch_statics(f->q, &f->statics[0], st))) return rc;
+    const int64_t numel = (int64_t)grid[0] * grid[1] * grid[2];
+    if ((rc = launch_statics(f->q, &f->statics[0], numel, st))) return rc;
     for (int side = 0; side < 2; side++) {
         for (int k = 0; k < 5; k++)
-            if ((rc = launch_statics(f->q + k * S, &f->statics[k], st))) return rc;
+            if ((rc = launch_statics(f->q + k * S, &f->statics[k], numel, st))) return rc;
         int32_t bc1[6];
         memcpy(bc1, f->bc, sizeof(bc1));
         bc1[2 * (dir - 1) + (1 - side)] = IB_BC_CIRCULAR;
@@ -367,7 +368,7 @@ int ib_cudaStatics(double *phi, const ib_grid *grid, const int32_t bc[6], int ha
     cudaStream_t st = (cudaStream_t)stream;
     const int g3[3] = {grid->nx, grid->ny, grid->nz};
     for (int side = 0; side < 2; side++) {
-        if ((rc = launch_statics(phi, statics, st))) return rc;
+        if ((rc = launch_statics(phi, statics, (int64_t)grid->nx * grid->ny * grid->nz, st))) return rc;
         const int mode = bc[2 * (direction - 1) + side];
         if (mode == IB_BC_OUTFLOW) {
             int32_t bc1[6] = {IB_BC_CIRCULAR, IB_BC_CIRCULAR, IB_BC_CIRCULAR,

@@ -366,15 +366,17 @@ __global__ void __launch_bounds__(256) sweep_march_kernel(MarchArgs a, FluidCons
     constexpr int s0 = slot_of<METHOD, DIR>(0), s1 = slot_of<METHOD, DIR>(1), s2 = slot_of<METHOD, DIR>(2),
                   s3 = slot_of<METHOD, DIR>(3), s4 = slot_of<METHOD, DIR>(4);
 
-    // sliding windows
-    V5<FT> wA, dA, RA, FA;      // stage A: prims j-1, diff j-1, right face j-2, flux face j-5/2
-    V5<FT> wB, dB, RB, FB;      // stage B, same roles for k = j-2
-    double ua1[5], ua2[5], ua3[5], ua4[5];  // U0 at j-1 .. j-4 (floored for HLL)
-    double ub1[5], ub2[5];                  // U1 at k-1, k-2
+    // Sliding windows.  At step s the cell j = j0-4+s arrives:
+    //   stage A: prims of j-1 (wA), its backward difference (dA), right face of j-2 (RA),
+    //            flux through face j-5/2 (FA), U0 history j-1..j-4 (ua1..ua4)
+    //   stage B works on k = j-2 with the same roles (wB, dB, RB, FB), U1 history k-1, k-2
+    V5<FT> wA, dA, RA, FA;
+    V5<FT> wB, dB, RB, FB;
+    double ua1[5], ua2[5], ua3[5], ua4[5];
+    double ub1[5], ub2[5];
     double nxt[5];
 
     const int nsteps = (j1 - j0) + 8;
-    // prefetch first cell
     if (live) {
         int64_t off = (int64_t)mod_n(j0 - 4, n) * stride;
         nxt[0] = q[s0 * S + off]; nxt[1] = q[s1 * S + off]; nxt[2] = q[s2 * S + off];
@@ -386,7 +388,7 @@ __global__ void __launch_bounds__(256) sweep_march_kernel(MarchArgs a, FluidCons
         double u[5];
 #pragma unroll
         for (int k = 0; k < 5; k++) u[k] = nxt[k];
-        if (s + 1 < nsteps) {
+        if (s + 1 < nsteps) {  // prefetch the next cell
             int64_t off = (int64_t)mod_n(j + 1, n) * stride;
             nxt[0] = q[s0 * S + off]; nxt[1] = q[s1 * S + off]; nxt[2] = q[s2 * S + off];
             nxt[3] = q[s3 * S + off]; nxt[4] = q[s4 * S + off];
@@ -395,52 +397,51 @@ __global__ void __launch_bounds__(256) sweep_march_kernel(MarchArgs a, FluidCons
         V5<FT> w = stage_prims<METHOD, DIR, FT>(u, c);  // floors u in place for HLL
         V5<FT> d = v5_sub(w, wA);
         V5<FT> Lf, Rf, f;
-        bool haveU1 = false;
         double u1[5];
-        if (s >= 2) stage_faces<METHOD, SLOPE, FT>(c, wA, dA, d, Lf, Rf);   // faces of j-1
-        if (s >= 3) f = stage_flux<METHOD, FT>(c, RA, Lf);                  // face j-3/2
-        if (s >= 4) {                                                        // U1[j-2]
+        if (s >= 2) stage_faces<METHOD, SLOPE, FT>(c, wA, dA, d, Lf, Rf);  // faces of j-1
+        if (s >= 3) f = stage_flux<METHOD, FT>(c, RA, Lf);                 // face j-3/2
+        if (s >= 4) {                                                       // U1[j-2]
 #pragma unroll
             for (int k = 0; k < 5; k++) u1[k] = ua2[k] - lambda * ((double)f.a[k] - (double)FA.a[k]);
-            haveU1 = true;
         }
-        // shift stage A window; ua4 keeps U0[j-4] for the final update below
         if (s >= 2) RA = Rf;
         if (s >= 3) FA = f;
         dA = d;
         wA = w;
+        // ---- stage B on k = j-2 ----
+        if (s >= 4) {
+            const int sb = s - 4;
+            V5<FT> wb = stage_prims<METHOD, DIR, FT>(u1, c);  // floors u1 in place for HLL
+            V5<FT> db = v5_sub(wb, wB);
+            V5<FT> Lb, Rb, fb;
+            if (sb >= 2) stage_faces<METHOD, SLOPE, FT>(c, wB, dB, db, Lb, Rb);
+            if (sb >= 3) fb = stage_flux<METHOD, FT>(c, RB, Lb);
+            if (sb >= 4) {
+                // final update of cell k-2 = j-4: .5*(U1 + U0 - lambda*dF)
+                const int jo = j - 4;
+                double out[5];
+#pragma unroll
+                for (int k = 0; k < 5; k++)
+                    out[k] = .5 * (ub2[k] + ua4[k] - lambda * ((double)fb.a[k] - (double)FB.a[k]));
+                if (jo - j0 < 4) {
+                    const int slot = jo - j0;
+#pragma unroll
+                    for (int k = 0; k < 5; k++) defer[(slot * 5 + k) * nthr + tid] = out[k];
+                } else {
+                    int64_t off = (int64_t)jo * stride;
+                    q[s0 * S + off] = out[0]; q[s1 * S + off] = out[1]; q[s2 * S + off] = out[2];
+                    q[s3 * S + off] = out[3]; q[s4 * S + off] = out[4];
+                }
+            }
+            if (sb >= 2) RB = Rb;
+            if (sb >= 3) FB = fb;
+            dB = db;
+            wB = wb;
+#pragma unroll
+            for (int k = 0; k < 5; k++) { ub2[k] = ub1[k]; ub1[k] = u1[k]; }
+        }
 #pragma unroll
         for (int k = 0; k < 5; k++) { ua4[k] = ua3[k]; ua3[k] = ua2[k]; ua2[k] = ua1[k]; ua1[k] = u[k]; }
-        if (!haveU1) return;
-        // ---- stage B on k = j-2 ----
-        const int sb = s - 4;
-        V5<FT> wb = stage_prims<METHOD, DIR, FT>(u1, c);
-        V5<FT> db = v5_sub(wb, wB);
-        V5<FT> Lb, Rb, fb;
-        if (sb >= 2) stage_faces<METHOD, SLOPE, FT>(c, wB, dB, db, Lb, Rb);
-        if (sb >= 3) fb = stage_flux<METHOD, FT>(c, RB, Lb);
-        if (sb >= 4) {
-            // final update of cell k-2 = j-4: .5*(U1 + U0 - lambda*dF)
-            const int jo = j - 4;
-            double out[5];
-#pragma unroll
-            for (int k = 0; k < 5; k++) out[k] = .5 * (ub2[k] + ua4[k] - lambda * ((double)fb.a[k] - (double)FB.a[k]));
-            if (jo - j0 < 4) {
-                const int slot = jo - j0;
-#pragma unroll
-                for (int k = 0; k < 5; k++) defer[(slot * 5 + k) * nthr + tid] = out[k];
-            } else {
-                int64_t off = (int64_t)jo * stride;
-                q[s0 * S + off] = out[0]; q[s1 * S + off] = out[1]; q[s2 * S + off] = out[2];
-                q[s3 * S + off] = out[3]; q[s4 * S + off] = out[4];
-            }
-        }
-        if (sb >= 2) RB = Rb;
-        if (sb >= 3) FB = fb;
-        dB = db;
-        wB = wb;
-#pragma unroll
-        for (int k = 0; k < 5; k++) { ub2[k] = ub1[k]; ub1[k] = u1[k]; }
     };
 
     // prologue: the first eight cells (j0-4 .. j0+3) are read before any chunk writes

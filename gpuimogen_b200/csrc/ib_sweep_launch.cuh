@@ -25,6 +25,13 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
             sweep_row_kernel<METHOD, SLOPE, FT, 1><<<(unsigned)rows, nt, shm, st>>>(a, c);
         } else {
             int nt = (((nx + 1) / 2 + 31) / 32) * 32;
+            static bool attr_set = false;  // rows above 512 cells need more than 48 KB
+            if (!attr_set) {
+                int rc = check_cuda(cudaFuncSetAttribute(sweep_row_kernel<METHOD, SLOPE, FT, 2>,
+                                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+                if (rc) return rc;
+                attr_set = true;
+            }
             sweep_row_kernel<METHOD, SLOPE, FT, 2><<<(unsigned)rows, nt, shm, st>>>(a, c);
         }
         return check_launch();

@@ -147,7 +147,8 @@ int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3
     const int64_t N = (int64_t)grid[0] * grid[1] * grid[2];
     if (n > 2048) return IB_ERROR_NOIMPLEMENT;  // per-thread proposal registers cover 8 cells x 256 threads
     const size_t shm = (size_t)16 * n * sizeof(double);
-    if (shm > 227 * 1024) return IB_ERROR_NOIMPLEMENT;
+    const size_t shm_cap = 227 * 1024 - 1024;  // opt-in limit minus the kernel's static shared memory
+    if (shm > shm_cap) return IB_ERROR_NOIMPLEMENT;
     const int64_t np = N / n;
     const double mintemp = 1e-5 / (gamma - 1);
     int nt = std::min(256, ((n + 31) / 32) * 32);
@@ -156,7 +157,9 @@ int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3
     do {                                                                                                      \
         static bool attr_set = false;                                                                         \
         if (!attr_set) {                                                                                      \
-            cudaFuncSetAttribute(xj_pencil_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024); \
+            int rc_ = check_cuda(cudaFuncSetAttribute(xj_pencil_kernel<F>,                                    \
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm_cap)); \
+            if (rc_) return rc_;                                                                              \
             attr_set = true;                                                                                  \
         }                                                                                                     \
         xj_pencil_kernel<F><<<(unsigned)np, nt, shm, st>>>(q, slab, grid[0], grid[1], grid[2], dir, lambda, gamma, \

@@ -31,12 +31,28 @@ def max_rel(a, b, n, floor=1e-300):
     return float(np.max(d / np.maximum(s, 1e-12 * np.max(np.abs(b[:, :n]), axis=1, keepdims=True))))
 
 
+def _bitdiff(a, b, n):
+    # NaNs compare equal whatever their payload (x86 and CUDA produce different NaN bits)
+    x, y = a[:, :n], b[:, :n]
+    both_nan = np.isnan(x) & np.isnan(y)
+    return (x.view(np.int64) != y.view(np.int64)) & ~both_nan
+
+
 def bits_equal(a, b, n):
-    return np.array_equal(a[:, :n].view(np.int64), b[:, :n].view(np.int64))
+    return not np.any(_bitdiff(a, b, n))
+
+
+def product_close(a, b, n, l1=1e-13, scale=1e-11):
+    """FMA-contracted product build vs the oracle: relative L1 per field <= l1 and every cell
+    within `scale` of its field's largest magnitude."""
+    err = rel_l1(a, b, n)
+    big = np.max(np.abs(b[:, :n]), axis=1, keepdims=True)
+    absd = np.max(np.abs(a[:, :n] - b[:, :n]) / np.maximum(big, 1e-300))
+    return bool(np.all(err <= l1) and absd <= scale), (err, absd)
 
 
 def first_diff(a, b, n):
-    d = np.argwhere(a[:, :n].view(np.int64) != b[:, :n].view(np.int64))
+    d = np.argwhere(_bitdiff(a, b, n))
     if len(d) == 0:
         return None
     k, i = d[0]

@@ -8,7 +8,7 @@ import torch
 
 import riemann_exact as rx
 from gpuimogen_b200 import problems
-from helpers import bits_equal, first_diff, host, max_rel, rel_l1, to_fluid
+from helpers import bits_equal, first_diff, host, product_close, rel_l1, to_fluid
 
 pytestmark = pytest.mark.gpu
 
@@ -106,18 +106,23 @@ def test_cudaStatics_per_array_strict(cuda, ib, po, mode, direction):
     bc[2 * (direction - 1)] = bc[2 * (direction - 1) + 1] = mode
     fl = to_fluid(q, shape, bc=bc)
     ref = q.copy()
-    for slab in range(5):
-        vec = slab - 1 if slab >= 2 else 0
-        phi = ref[slab, :n].copy()
-        rc0 = po.array_boundary(phi, shape, mode, direction, 0, vec)
-        rc1 = po.array_boundary(phi, shape, mode, direction, 1, vec)
-        if rc0 or rc1:
-            with pytest.raises(ib.ImogenError):
-                ib.cudaStatics(fl, slab, direction)
-            return
-        ref[slab, :n] = phi
-        ib.cudaStatics(fl, slab, direction)
-    assert bits_equal(host(fl), ref, n), first_diff(host(fl), ref, n)
+    ib.use_variant("strict")
+    try:
+        for slab in range(5):
+            vec = slab - 1 if slab >= 2 else 0
+            phi = ref[slab, :n].copy()
+            rc0 = po.array_boundary(phi, shape, mode, direction, 0, vec)
+            rc1 = po.array_boundary(phi, shape, mode, direction, 1, vec)
+            if rc0 or rc1:
+                with pytest.raises(ib.ImogenError):
+                    ib.cudaStatics(fl, slab, direction)
+                return
+            ref[slab, :n] = phi
+            ib.cudaStatics(fl, slab, direction)
+        out = host(fl)
+    finally:
+        ib.use_variant("product")
+    assert bits_equal(out, ref, n), first_diff(out, ref, n)
 
 
 def test_statics_fade(cuda, ib, po):
@@ -134,8 +139,12 @@ def test_statics_fade(cuda, ib, po):
     ref[0, :n] = phi
     fl = to_fluid(q, shape, bc=["circular"] * 6,
                   statics=[torch.from_numpy(st).cuda()] + [None] * 4)
-    ib.setFluidBoundary(fl, 1)
-    out = host(fl)
+    ib.use_variant("strict")
+    try:
+        ib.setFluidBoundary(fl, 1)
+        out = host(fl)
+    finally:
+        ib.use_variant("product")
     assert np.array_equal(out[0, :n], ref[0, :n])
 
 
@@ -144,11 +153,13 @@ def test_drag_logtrap_matches_oracle(cuda, ib, po, method):
     shape = (64, 32, 1)
     n = 64 * 32
     rng = np.random.default_rng(1)
+    cube = (1, 32, 64)
     rho_g = 1.0 + 0.1 * rng.uniform(-1, 1, n)
-    gas = problems.pack(shape, rho_g, 0, rho_g * rng.uniform(-1e-2, 1e-2, n), rho_g * rng.uniform(-1e-2, 1e-2, n), 0)
+    gas = problems.pack(shape, rho_g.reshape(cube), 0, (rho_g * rng.uniform(-1e-2, 1e-2, n)).reshape(cube),
+                        (rho_g * rng.uniform(-1e-2, 1e-2, n)).reshape(cube), 0)
     gas[1, :n] = 1.0 / (5 / 3.0 - 1) + 0.5 * (gas[2, :n] ** 2 + gas[3, :n] ** 2) / rho_g
     rho_d = rho_g * 10 ** rng.uniform(-2, 0, n)
-    dust = problems.pack(shape, rho_d, 0, rho_d * rng.uniform(-2e-2, 2e-2, n), 0, 0)
+    dust = problems.pack(shape, rho_d.reshape(cube), 0, (rho_d * rng.uniform(-2e-2, 2e-2, n)).reshape(cube), 0, 0)
     dust[1, :n] = 0.5 * dust[2, :n] ** 2 / rho_d + 1e-4 * rho_d
     tg = [5 / 3.0, 3.3e-27, 8.4e-6, 0.7, 2.4e-19, 0.2, 1.381e-23, -1]
     td = [1.01, 3e-11, 0, 0, math.pi * 25e-12, 0, 1.381e-23, 0.1]
@@ -157,9 +168,12 @@ def test_drag_logtrap_matches_oracle(cuda, ib, po, method):
     fg, fd = to_fluid(gas, shape), to_fluid(dust, shape)
     ib.cudaSource2FluidDrag(fg, fd, tg, td, ib.Geometry(shape), [0.05, method])
     # transcendental functions (pow, exp, expm1) come from CUDA's libdevice on the GPU and glibc
-    # on the CPU: compare within a few ulp-scaled relative error
-    assert max_rel(host(fg), g_ref, n) < 1e-12
-    assert max_rel(host(fd), d_ref, n) < 1e-12
+    # on the CPU, and the momenta are differences of two larger terms: per field relative L1
+    # <= 1e-13 and every cell within 1e-11 of its field's largest magnitude
+    ok, info = product_close(host(fg), g_ref, n, l1=1e-13, scale=1e-11)
+    assert ok, info
+    ok, info = product_close(host(fd), d_ref, n, l1=1e-13, scale=1e-11)
+    assert ok, info
     assert not np.array_equal(g_ref[2, :n], gas[2, :n])   # the drag did act
 
 
