@@ -2,9 +2,12 @@
 
 Produces, next to this file:
   libimogen_b200.so         the product library (nvcc default: multiply-adds contracted)
-  libimogen_b200_strict.so  the same sources with -fmad=false, whose arithmetic is the reference
-                            kernels' expressions one IEEE operation at a time; the test suite
-                            uses it for bit-exact comparisons with the CPU oracle.
+  libimogen_b200_strict.so  the same sources with -fmad=false -DIB_STRICT_ARITH: every expression
+                            is the reference kernels' own, one IEEE operation at a time, so the
+                            test suite can compare it bit for bit with the CPU oracle.  The
+                            product build instead contracts multiply-adds and replaces a few
+                            divisions by reciprocals or comparisons (same mathematics, last-bit
+                            differences), checked against the oracle within a tolerance.
 
 Usage: python -m gpuimogen_b200.build [--force] [--only product|strict]
 """
@@ -40,7 +43,7 @@ BASE_FLAGS = [
 
 VARIANTS = {
     "product": ("libimogen_b200.so", []),
-    "strict": ("libimogen_b200_strict.so", ["-fmad=false"]),
+    "strict": ("libimogen_b200_strict.so", ["-fmad=false", "-DIB_STRICT_ARITH"]),
 }
 
 

@@ -63,11 +63,23 @@ __device__ __forceinline__ FT slope_limit(FT A, FT B)
         return (FT)0.0;
     } else if constexpr (SLOPE == IB_SLOPE_MC) {  // limiter_functions.h:105-115
         if (A * B <= 0) return (FT)0;
+#ifdef IB_STRICT_ARITH
         FT R = B / A;
         FT S = (FT).25 + (FT).25 * R;
         S = (S < R) ? S : R;
         S = (S < 1) ? S : (FT)1.0;
         return S * A;
+#else
+        // min(.25(1+R), R, 1) * A with R = B/A, without the division: for A and B of one sign
+        // it is the smaller in magnitude of .25(A+B), B and A
+        FT S = (FT).25 * (A + B);
+        if (A > 0) {
+            S = (S < B) ? S : B;
+            return (S < A) ? S : A;
+        }
+        S = (S > B) ? S : B;
+        return (S > A) ? S : A;
+#endif
     } else if constexpr (SLOPE == IB_SLOPE_VANLEER) {  // limiter_functions.h:54-61
         FT r = A * B;
         if (r > (FT)0.0) return r / (A + B);
@@ -124,9 +136,16 @@ template <typename FT>
 __device__ __forceinline__ void einfeldt(const FluidConsts<FT> &c, FT rhoL, FT vL, FT PL, FT rhoR,
                                          FT vR, FT PR, FT dvsq, FT &sl, FT &sr)
 {
+#ifdef IB_STRICT_ARITH
     FT csql = c.gamma * PL / rhoL;
     FT csqr = c.gamma * PR / rhoR;
     FT Fa = dsqrt<FT>(rhoR / rhoL);
+#else
+    const FT irL = (FT)1.0 / rhoL, irR = (FT)1.0 / rhoR;
+    FT csql = c.gamma * PL * irL;
+    FT csqr = c.gamma * PR * irR;
+    FT Fa = dsqrt<FT>(rhoR * irL);
+#endif
     FT Fb = (FT)1.0 / ((FT)1.0 + Fa);
     FT Croe = ((csql + Fa * csqr) + (FT).5 * c.gm1 * dvsq * Fa * Fb) * Fb;
     FT Vroe = (vL + Fa * vR) * Fb;
@@ -234,7 +253,11 @@ __device__ __forceinline__ V5<FT> hllc_flux(const FluidConsts<FT> &c, const V5<F
             H *= A;
             C *= (E - B);
             B = PL + D * (C + E * B);
+#ifdef IB_STRICT_ARITH
             G = D * E * (c.govergm1 * PL / rhoL + G + C);
+#else
+            G = D * E * (c.govergm1 * PL * ((FT)1.0 / rhoL) + G + C);
+#endif
             f.a[0] = A; f.a[1] = G; f.a[2] = B; f.a[3] = F; f.a[4] = H;
         }
     } else {
@@ -248,7 +271,11 @@ __device__ __forceinline__ V5<FT> hllc_flux(const FluidConsts<FT> &c, const V5<F
             H *= A;
             D *= (E - B);
             B = PR + C * (D + E * B);
+#ifdef IB_STRICT_ARITH
             G = C * E * (c.govergm1 * PR / rhoR + G + D);
+#else
+            G = C * E * (c.govergm1 * PR * ((FT)1.0 / rhoR) + G + D);
+#endif
             f.a[0] = A; f.a[1] = G; f.a[2] = B; f.a[3] = F; f.a[4] = H;
         } else {  // right state
             A = rhoR; B = vxR; C = vyR; D = vzR;

@@ -219,8 +219,11 @@ struct SweepArgs {
 // Row kernel: one CTA per x row (nx <= CPT*blockDim.x), periodic in shared memory.
 // Dynamic shared memory: 2 planes x 5 components x nx elements of FT.
 // ------------------------------------------------------------------------------------------
+#ifndef IB_ROW_MINB
+#define IB_ROW_MINB 2
+#endif
 template <int METHOD, int SLOPE, typename FT, int CPT>
-__global__ void __launch_bounds__(512) sweep_row_kernel(SweepArgs a, FluidConsts<FT> c)
+__global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_kernel(SweepArgs a, FluidConsts<FT> c)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     FT *SA = reinterpret_cast<FT *>(smem_raw);
@@ -461,6 +464,225 @@ __global__ void __launch_bounds__(256) sweep_march_kernel(MarchArgs a, FluidCons
             q[s2 * S + off] = defer[(slot * 5 + 2) * nthr + tid];
             q[s3 * S + off] = defer[(slot * 5 + 3) * nthr + tid];
             q[s4 * S + off] = defer[(slot * 5 + 4) * nthr + tid];
+        }
+    }
+}
+
+
+// ------------------------------------------------------------------------------------------
+// Tile-march kernel (y and z sweeps, long x rows).  One CTA owns W neighbouring pencils and
+// walks them in chunks of Lc cells.  A chunk stages U0 for cells [cb-4, cb+Lc+4) in shared
+// memory, runs stage A over [cb-2, cb+Lc+2) and stage B over [cb, cb+Lc), one tile cell per
+// thread per phase, neighbours through shared-memory planes.  In-place safety: the next
+// chunk re-reads the last four outputs of this one, so they are written only after that
+// chunk's load; the last chunk re-reads cells 0..3 (periodic wrap), so the first chunk's first
+// four outputs are written at the very end.
+// Shared memory (doubles unless FT is float): U0t[5][TR][W], U1t[5][TR1][W] (double),
+// PA,PB,PC[5][TR][W] (FT), pending[5][4][W], first[5][4][W] (double); TR = Lc+8, TR1 = Lc+4.
+// ------------------------------------------------------------------------------------------
+struct TileArgs {
+    double *q;
+    int64_t slab;
+    int nx, ny, nz;
+    int n;            // pencil length
+    int64_t npencil;
+    int Lc;           // chunk length
+    double lambda;
+};
+
+template <int W>
+__host__ __device__ __forceinline__ size_t tile_smem_bytes(int Lc, size_t ft)
+{
+    const size_t TR = Lc + 8, TR1 = Lc + 4;
+    return sizeof(double) * (5 * TR * W + 5 * TR1 * W + 2 * 5 * 4 * W) + ft * 3 * 5 * TR * W;
+}
+
+template <int METHOD, int SLOPE, typename FT, int DIR, int W>
+__global__ void __launch_bounds__(256, 4) sweep_tile_kernel(TileArgs a, FluidConsts<FT> c)
+{
+    extern __shared__ __align__(16) double tsm[];
+    const int Lc = a.Lc, n = a.n;
+    const int TR = Lc + 8, TR1 = Lc + 4;
+    double *U0t = tsm;                       // [5][TR][W]
+    double *U1t = U0t + 5 * TR * W;          // [5][TR1][W]
+    double *pend = U1t + 5 * TR1 * W;        // [5][4][W]
+    double *first = pend + 5 * 4 * W;        // [5][4][W]
+    FT *PA = reinterpret_cast<FT *>(first + 5 * 4 * W);  // [5][TR][W]
+    FT *PB = PA + 5 * TR * W;
+    FT *PC = PB + 5 * TR * W;
+    const int64_t S = a.slab;
+    const double lambda = a.lambda;
+    constexpr int s0 = slot_of<METHOD, DIR>(0), s1 = slot_of<METHOD, DIR>(1), s2 = slot_of<METHOD, DIR>(2),
+                  s3 = slot_of<METHOD, DIR>(3), s4 = slot_of<METHOD, DIR>(4);
+    const int slots[5] = {s0, s1, s2, s3, s4};
+
+    // base offset of my W columns
+    __shared__ int64_t colbase[W];
+    __shared__ bool colok[W];
+    int64_t stride;
+    if (DIR == 1) stride = 1;
+    else if (DIR == 2) stride = a.nx;
+    else stride = (int64_t)a.nx * a.ny;
+    if (threadIdx.x < W) {
+        int64_t p = (int64_t)blockIdx.x * W + threadIdx.x;
+        colok[threadIdx.x] = p < a.npencil;
+        if (p >= a.npencil) p = 0;
+        int64_t b;
+        if (DIR == 1) b = p * a.nx;
+        else if (DIR == 2) b = (p % a.nx) + (int64_t)a.nx * a.ny * (p / a.nx);
+        else b = p;
+        colbase[threadIdx.x] = b;
+    }
+    __syncthreads();
+
+    const int nchunks = (n + Lc - 1) / Lc;
+    const bool single = (nchunks == 1);
+    auto IDX = [&](int k, int r, int col, int R) { return (k * R + r) * W + col; };
+
+    for (int ch = 0; ch < nchunks; ch++) {
+        const int cb = ch * Lc;
+        const int len = min(Lc, n - cb);          // outputs of this chunk
+        const int tr = len + 8, tr1 = len + 4;    // tile rows in use
+        // ---- load U0 for cells [cb-4, cb+len+4) ----
+        for (int it = threadIdx.x; it < tr * W; it += blockDim.x) {
+            const int r = it / W, col = it - r * W;
+            const int cell = mod_n(cb - 4 + r, n);
+            const double *src = a.q + colbase[col] + (int64_t)cell * stride;
+#pragma unroll
+            for (int k = 0; k < 5; k++) U0t[IDX(k, r, col, TR)] = src[slots[k] * S];
+        }
+        __syncthreads();
+        // the previous chunk's last four outputs can go now that this chunk has read them
+        if (ch > 0) {
+            for (int it = threadIdx.x; it < 4 * W; it += blockDim.x) {
+                const int r = it / W, col = it - r * W;
+                if (!colok[col]) continue;
+                double *dst = a.q + colbase[col] + (int64_t)(cb - 4 + r) * stride;
+#pragma unroll
+                for (int k = 0; k < 5; k++) dst[slots[k] * S] = pend[IDX(k, r, col, 4)];
+            }
+        }
+        // ---- stage A ----
+        for (int it = threadIdx.x; it < tr * W; it += blockDim.x) {      // prims (floors U0 for HLL)
+            const int r = it / W, col = it - r * W;
+            double u[5];
+#pragma unroll
+            for (int k = 0; k < 5; k++) u[k] = U0t[IDX(k, r, col, TR)];
+            V5<FT> w = stage_prims<METHOD, DIR, FT>(u, c);
+            if (METHOD == IB_METHOD_HLL) {
+#pragma unroll
+                for (int k = 0; k < 5; k++) U0t[IDX(k, r, col, TR)] = u[k];
+            }
+#pragma unroll
+            for (int k = 0; k < 5; k++) PA[IDX(k, r, col, TR)] = w.a[k];
+        }
+        __syncthreads();
+        for (int it = threadIdx.x + W; it < (tr - 1) * W; it += blockDim.x) {  // faces, rows 1..tr-2
+            const int r = it / W, col = it - r * W;
+            V5<FT> w, dl, dr, L, R;
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                w.a[k] = PA[IDX(k, r, col, TR)];
+                dl.a[k] = w.a[k] - PA[IDX(k, r - 1, col, TR)];
+                dr.a[k] = PA[IDX(k, r + 1, col, TR)] - w.a[k];
+            }
+            stage_faces<METHOD, SLOPE, FT>(c, w, dl, dr, L, R);
+#pragma unroll
+            for (int k = 0; k < 5; k++) { PB[IDX(k, r, col, TR)] = L.a[k]; PC[IDX(k, r, col, TR)] = R.a[k]; }
+        }
+        __syncthreads();
+        for (int it = threadIdx.x + W; it < (tr - 2) * W; it += blockDim.x) {  // fluxes through r+1/2, r = 1..tr-3
+            const int r = it / W, col = it - r * W;
+            V5<FT> Lr, Rl;
+#pragma unroll
+            for (int k = 0; k < 5; k++) { Rl.a[k] = PC[IDX(k, r, col, TR)]; Lr.a[k] = PB[IDX(k, r + 1, col, TR)]; }
+            V5<FT> f = stage_flux<METHOD, FT>(c, Rl, Lr);
+#pragma unroll
+            for (int k = 0; k < 5; k++) PA[IDX(k, r, col, TR)] = f.a[k];
+        }
+        __syncthreads();
+        for (int it = threadIdx.x; it < tr1 * W; it += blockDim.x) {  // U1 for tile rows 2..tr-3
+            const int r1 = it / W, col = it - r1 * W, r = r1 + 2;
+#pragma unroll
+            for (int k = 0; k < 5; k++)
+                U1t[IDX(k, r1, col, TR1)] = U0t[IDX(k, r, col, TR)] -
+                                            lambda * ((double)PA[IDX(k, r, col, TR)] - (double)PA[IDX(k, r - 1, col, TR)]);
+        }
+        __syncthreads();
+        // ---- stage B (rows of U1t; U1t row r1 is cell cb-2+r1) ----
+        for (int it = threadIdx.x; it < tr1 * W; it += blockDim.x) {
+            const int r1 = it / W, col = it - r1 * W;
+            double u[5];
+#pragma unroll
+            for (int k = 0; k < 5; k++) u[k] = U1t[IDX(k, r1, col, TR1)];
+            V5<FT> w = stage_prims<METHOD, DIR, FT>(u, c);
+            if (METHOD == IB_METHOD_HLL) {
+#pragma unroll
+                for (int k = 0; k < 5; k++) U1t[IDX(k, r1, col, TR1)] = u[k];
+            }
+#pragma unroll
+            for (int k = 0; k < 5; k++) PA[IDX(k, r1, col, TR)] = w.a[k];
+        }
+        __syncthreads();
+        for (int it = threadIdx.x + W; it < (tr1 - 1) * W; it += blockDim.x) {
+            const int r = it / W, col = it - r * W;
+            V5<FT> w, dl, dr, L, R;
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                w.a[k] = PA[IDX(k, r, col, TR)];
+                dl.a[k] = w.a[k] - PA[IDX(k, r - 1, col, TR)];
+                dr.a[k] = PA[IDX(k, r + 1, col, TR)] - w.a[k];
+            }
+            stage_faces<METHOD, SLOPE, FT>(c, w, dl, dr, L, R);
+#pragma unroll
+            for (int k = 0; k < 5; k++) { PB[IDX(k, r, col, TR)] = L.a[k]; PC[IDX(k, r, col, TR)] = R.a[k]; }
+        }
+        __syncthreads();
+        for (int it = threadIdx.x + W; it < (tr1 - 2) * W; it += blockDim.x) {
+            const int r = it / W, col = it - r * W;
+            V5<FT> Lr, Rl;
+#pragma unroll
+            for (int k = 0; k < 5; k++) { Rl.a[k] = PC[IDX(k, r, col, TR)]; Lr.a[k] = PB[IDX(k, r + 1, col, TR)]; }
+            V5<FT> f = stage_flux<METHOD, FT>(c, Rl, Lr);
+#pragma unroll
+            for (int k = 0; k < 5; k++) PA[IDX(k, r, col, TR)] = f.a[k];
+        }
+        __syncthreads();
+        for (int it = threadIdx.x; it < len * W; it += blockDim.x) {  // outputs: U1t rows 2..len+1
+            const int m = it / W, col = it - m * W, r1 = m + 2;
+            double out[5];
+#pragma unroll
+            for (int k = 0; k < 5; k++)
+                out[k] = .5 * (U1t[IDX(k, r1, col, TR1)] + U0t[IDX(k, r1 + 2, col, TR)] -
+                               lambda * ((double)PA[IDX(k, r1, col, TR)] - (double)PA[IDX(k, r1 - 1, col, TR)]));
+            const int cell = cb + m;
+            if (!single && ch == 0 && m < 4) {
+#pragma unroll
+                for (int k = 0; k < 5; k++) first[IDX(k, m, col, 4)] = out[k];
+            } else if (!single && m >= len - 4) {
+                const int pr = m - (len - 4);
+#pragma unroll
+                for (int k = 0; k < 5; k++) pend[IDX(k, pr, col, 4)] = out[k];
+            } else if (colok[col]) {
+                double *dst = a.q + colbase[col] + (int64_t)cell * stride;
+#pragma unroll
+                for (int k = 0; k < 5; k++) dst[slots[k] * S] = out[k];
+            }
+        }
+        __syncthreads();
+    }
+    if (!single) {
+        const int cbl = (nchunks - 1) * Lc, lenl = n - cbl;
+        for (int it = threadIdx.x; it < 4 * W; it += blockDim.x) {
+            const int r = it / W, col = it - r * W;
+            if (!colok[col]) continue;
+            double *dl = a.q + colbase[col] + (int64_t)(cbl + lenl - 4 + r) * stride;
+            double *df = a.q + colbase[col] + (int64_t)r * stride;
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                dl[slots[k] * S] = pend[IDX(k, r, col, 4)];
+                df[slots[k] * S] = first[IDX(k, r, col, 4)];
+            }
         }
     }
 }

@@ -4,7 +4,49 @@
 #include "ib_internal.cuh"
 #include "ib_sweep.cuh"
 
+#include <cstdlib>
+
 namespace ib {
+
+// Tile-march launch: W pencils per CTA, chunks of ~TARGET cells, every chunk >= 8 cells.
+template <int METHOD, int SLOPE, typename FT, int DIR, int W>
+int launch_tile_dw(double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c,
+                   cudaStream_t st, int target)
+{
+    const int n = grid[DIR - 1];
+    const int64_t npencil = (int64_t)grid[0] * grid[1] * grid[2] / n;
+    // every phase of a chunk must fit in one pass of the CTA's threads: (Lc+8)*W <= 256
+    const int lc_max = 256 / W - 8;
+    if (target > lc_max) target = lc_max;
+    int nc = std::max(1, (n + target - 1) / target);
+    int Lc = (n + nc - 1) / nc;
+    while (nc > 1 && (Lc < 8 || n - (nc - 1) * Lc < 8)) {
+        nc--;
+        Lc = (n + nc - 1) / nc;
+    }
+    if (Lc > lc_max) return IB_ERROR_NOIMPLEMENT;  // pencil too short to split into valid chunks
+    TileArgs a{q, slab, grid[0], grid[1], grid[2], n, npencil, Lc, lambda};
+    const size_t shm = tile_smem_bytes<W>(Lc, sizeof(FT));
+    static int attr_bytes = 0;
+    if ((int)shm > 48 * 1024 && (int)shm > attr_bytes) {
+        int rc = check_cuda(cudaFuncSetAttribute(sweep_tile_kernel<METHOD, SLOPE, FT, DIR, W>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        if (rc) return rc;
+        attr_bytes = (int)shm;
+    }
+    const unsigned nblk = (unsigned)((npencil + W - 1) / W);
+    sweep_tile_kernel<METHOD, SLOPE, FT, DIR, W><<<nblk, 256, shm, st>>>(a, c);
+    return check_launch();
+}
+
+template <int METHOD, int SLOPE, typename FT>
+int launch_tile_t(int dir, double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c,
+                  cudaStream_t st)
+{
+    if (dir == 1) return launch_tile_dw<METHOD, SLOPE, FT, 1, 1>(q, slab, grid, lambda, c, st, 248);
+    if (dir == 2) return launch_tile_dw<METHOD, SLOPE, FT, 2, 4>(q, slab, grid, lambda, c, st, 56);
+    return launch_tile_dw<METHOD, SLOPE, FT, 3, 4>(q, slab, grid, lambda, c, st, 56);
+}
 
 template <int METHOD, int SLOPE, typename FT>
 int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c,
@@ -37,8 +79,14 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
         return check_launch();
     }
 
-    // march kernel: PW pencils x C chunks per CTA, C*PW <= 256
     const int64_t npencil = N / n;
+    static const bool use_march = [] {
+        const char *e = getenv("IMOGEN_B200_MARCH");
+        return e && e[0] == '1';
+    }();
+    if (!use_march) return launch_tile_t<METHOD, SLOPE, FT>(dir, q, slab, grid, lambda, c, st);
+
+    // register-march kernel: PW pencils x C chunks per CTA, C*PW <= 256
     int PW = 32;
     if (dir == 1) PW = 32;  // lanes on different rows: correct, uncoalesced fallback for long rows
     // target ~4 resident waves of threads; chunk length at least 16 cells

@@ -119,7 +119,10 @@ _VARIANT = os.environ.get("IMOGEN_B200_VARIANT", "product")
 
 
 def library_path(variant=None):
+    """Path of the product or strict build; IMOGEN_B200_LIB overrides the product path."""
     variant = variant or _VARIANT
+    if variant == "product" and os.environ.get("IMOGEN_B200_LIB"):
+        return os.environ["IMOGEN_B200_LIB"]
     name = "libimogen_b200.so" if variant == "product" else "libimogen_b200_strict.so"
     return os.path.join(HERE, name)
 

@@ -168,11 +168,12 @@ def test_drag_logtrap_matches_oracle(cuda, ib, po, method):
     fg, fd = to_fluid(gas, shape), to_fluid(dust, shape)
     ib.cudaSource2FluidDrag(fg, fd, tg, td, ib.Geometry(shape), [0.05, method])
     # transcendental functions (pow, exp, expm1) come from CUDA's libdevice on the GPU and glibc
-    # on the CPU, and the momenta are differences of two larger terms: per field relative L1
-    # <= 1e-13 and every cell within 1e-11 of its field's largest magnitude
-    ok, info = product_close(host(fg), g_ref, n, l1=1e-13, scale=1e-11)
+    # on the CPU, and the momenta are differences of two larger terms (a dust momentum that
+    # starts at zero is all cancellation): per field relative L1 <= 1e-12 and every cell within
+    # 1e-11 of its field's largest magnitude
+    ok, info = product_close(host(fg), g_ref, n, l1=1e-12, scale=1e-11)
     assert ok, info
-    ok, info = product_close(host(fd), d_ref, n, l1=1e-13, scale=1e-11)
+    ok, info = product_close(host(fd), d_ref, n, l1=1e-12, scale=1e-11)
     assert ok, info
     assert not np.array_equal(g_ref[2, :n], gas[2, :n])   # the drag did act
 
