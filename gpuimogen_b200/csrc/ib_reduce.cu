@@ -6,6 +6,9 @@
 // loop, MPI_Allreduce and the HLL/HLLC halving (:204-237).  Here the fused variant computes c_s
 // inline, reduces with warp shuffles, and the last block to finish folds the block minima and
 // applies the halving on the device, so the timestep can stay on the GPU.
+#include <cstdio>
+#include <mutex>
+
 #include "ib_internal.cuh"
 
 namespace ib {
@@ -216,3 +219,99 @@ int launch_freeze_ptot(double *q, int64_t slab, const int grid[3], double gamma,
 }
 
 }  // namespace ib
+
+// ------------------------------------------------------------------------------------------
+// CFL timestep without any device allocation (ib_cflTimestepNoAlloc)
+//
+// The ordinary CFL entry points keep their per-block minima in scratch memory that the library
+// obtains from cudaMalloc on first use.  Some callers cannot let the library allocate: a host
+// application that has reserved the GPU's memory for its own pool (so an extra cudaMalloc may
+// fail), or a time-critical loop that must not pay for the device-wide synchronisation that
+// cudaMalloc and cudaFree can cause.  This variant runs the same reduction kernel with its
+// scratch in a fixed array compiled into the library instead.
+//
+// The array is a file-scope device variable, so every GPU that loads the library carries it
+// (a little over 64 KB) until the process exits.  All calls on a device share it and it keeps
+// whatever the last call left there: the completion counter is cleared at the start of every
+// call, and two calls that overlap on the GPU (for example on two streams) would race on it.
+// ------------------------------------------------------------------------------------------
+namespace ib {
+
+constexpr int kNoAllocMaxBlocks = 8192;        // one partial minimum per reduction block
+constexpr int kNoAllocCellsPerBlock = 256 * 64;  // 256 threads x 64 cells each
+// largest grid the fixed scratch covers: 8192 blocks x 16384 cells = 134,217,728 cells
+constexpr int64_t kNoAllocMaxCells = (int64_t)kNoAllocMaxBlocks * kNoAllocCellsPerBlock;
+
+// [0, 256): completion counter (first 4 bytes); [256, 256 + 8*8192): partial minima
+static __device__ __align__(256) unsigned char g_cfl_noalloc_scratch[256 + sizeof(double) * kNoAllocMaxBlocks];
+
+// Device address of the array per device, looked up once with that device current.  Host code
+// must not hand the symbol itself to a kernel: in host code it names a host-side stand-in.
+static unsigned char *g_noalloc_addr[64] = {nullptr};
+static std::mutex g_noalloc_mu;
+
+static int noalloc_scratch(unsigned char **out)
+{
+    int dev = 0;
+    int rc = check_cuda(cudaGetDevice(&dev));
+    if (rc) return rc;
+    if (dev < 0 || dev >= 64) return IB_ERROR_INVALID_ARGS;
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        rc = check_cuda(cudaGetSymbolAddress(&p, g_cfl_noalloc_scratch));
+        if (rc) return rc;
+        g_noalloc_addr[dev] = static_cast<unsigned char *>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return IB_SUCCESSFUL;
+}
+
+}  // namespace ib
+
+extern "C" int ib_cflTimestepNoAlloc(const ib_fluid *fluid, double gamma, const ib_geometry *geo, int method,
+                                     double *tau_device, void *stream)
+{
+    using namespace ib;
+    if (!fluid || !geo || !fluid->q || !tau_device) return IB_ERROR_NULL_POINTER;
+    const ib_grid &g = fluid->grid;
+    if (g.nx < 1 || g.ny < 1 || g.nz < 1) return IB_ERROR_INVALID_ARGS;
+    const int64_t n = (int64_t)g.nx * g.ny * g.nz;
+    if (g.slab_pitch < n) return IB_ERROR_INVALID_ARGS;
+    if (n > kNoAllocMaxCells) {
+        fprintf(stderr, "ib_cflTimestepNoAlloc: %lld cells exceed the fixed scratch limit of %lld cells\n",
+                (long long)n, (long long)kNoAllocMaxCells);
+        return IB_ERROR_INVALID_ARGS;
+    }
+    if (method < IB_METHOD_HLL || method > IB_METHOD_XINJIN) return IB_ERROR_INVALID_ARGS;
+    if (geo->shape != 0) return IB_ERROR_NOIMPLEMENT;
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned char *base = nullptr;
+    int rc = noalloc_scratch(&base);
+    if (rc) return rc;
+    unsigned int *counter = reinterpret_cast<unsigned int *>(base);
+    double *partial = reinterpret_cast<double *>(base + 256);
+    if ((rc = check_cuda(cudaMemsetAsync(counter, 0, sizeof(unsigned int), st)))) return rc;
+
+    int sim = 1;
+    if (geo->global_rez[1] > 1) sim = 2;
+    if (geo->global_rez[2] > 1) sim = 3;
+    const bool xj = (method == IB_METHOD_XINJIN) && (sim > 1);
+    double hmin = geo->h[0];
+    if (sim > 1 && geo->h[1] < hmin) hmin = geo->h[1];
+    if (sim > 2 && geo->h[2] < hmin) hmin = geo->h[2];
+    const int nb = (int)std::max<int64_t>(1, (n + kNoAllocCellsPerBlock - 1) / kNoAllocCellsPerBlock);
+    const int halve = (method == IB_METHOD_HLL || method == IB_METHOD_HLLC) ? 1 : 0;
+    const double gg1 = gamma * (gamma - 1);
+    const int64_t slab = g.slab_pitch;
+    const double *q = fluid->q;
+#define IB_NOALLOC_CFL(S, X)                                                                             \
+    cfl_kernel<S, X, true><<<nb, 256, 0, st>>>(q, nullptr, slab, n, gg1, hmin, geo->h[0], geo->h[1], geo->h[2], \
+                                               halve, partial, counter, tau_device)
+    if (xj) { if (sim == 2) IB_NOALLOC_CFL(2, true); else IB_NOALLOC_CFL(3, true); }
+    else if (sim == 1) IB_NOALLOC_CFL(1, false);
+    else if (sim == 2) IB_NOALLOC_CFL(2, false);
+    else IB_NOALLOC_CFL(3, false);
+#undef IB_NOALLOC_CFL
+    return check_launch();
+}

@@ -101,6 +101,9 @@ EXPORTS = {
                                            ctypes.POINTER(IbGeometry), ctypes.c_int,
                                            ctypes.POINTER(ctypes.c_double), ctypes.c_void_p,
                                            ctypes.c_void_p]),
+    "ib_cflTimestepNoAlloc": (ctypes.c_int, [ctypes.POINTER(IbFluid), ctypes.c_double,
+                                             ctypes.POINTER(IbGeometry), ctypes.c_int, ctypes.c_void_p,
+                                             ctypes.c_void_p]),
     "ib_freezeAndPtot": (ctypes.c_int, [ctypes.POINTER(IbFluid), ctypes.c_double, ctypes.c_int,
                                         ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
                                         ctypes.c_void_p]),

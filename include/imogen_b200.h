@@ -188,6 +188,20 @@ IB_API int ib_cflTimestep(const ib_fluid *fluid, const double *cs, const ib_geom
 IB_API int ib_cflTimestepFused(const ib_fluid *fluid, double gamma, const ib_geometry *geo, int method,
                         double *tau_host, double *tau_device, void *stream);
 
+/* No counterpart in the reference.  The same timestep as ib_cflTimestepFused, for callers that
+ * cannot let the library allocate device memory: an application that has reserved the GPU's
+ * memory for its own allocator, or a loop that must not pay for the device-wide
+ * synchronisation cudaMalloc/cudaFree can cause.  The reduction's scratch is a fixed array built
+ * into the library (about 64 KB on every GPU that loads it, kept until exit), so the call
+ * allocates nothing; the result goes to *tau_device (caller-owned device memory) and the call
+ * does not synchronise.  Limit: at most 134,217,728 cells (8192 reduction blocks of 16384
+ * cells); larger grids return IB_ERROR_INVALID_ARGS.  The first call on a device looks up the
+ * array's device address, so make that first call outside any stream capture.  All calls on a
+ * device share the array (its counter is cleared at the start of each call): calls that overlap
+ * on the GPU, e.g. on two streams, race. */
+IB_API int ib_cflTimestepNoAlloc(const ib_fluid *fluid, double gamma, const ib_geometry *geo, int method,
+                                 double *tau_device, void *stream);
+
 /* Replaces the freezeAndPtot mex for hydro (gpuclass/freezeAndPtot.cu:32-147, kernel
  * :229-290): ptot[N] = gas pressure (raising E where c_s < cs_min), freeze[ny*nz] = max over
  * each x row of |px|/rho + c_s. */
