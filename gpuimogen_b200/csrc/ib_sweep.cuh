@@ -497,11 +497,15 @@ __host__ __device__ __forceinline__ size_t tile_smem_bytes(int Lc, size_t ft)
     return sizeof(double) * (5 * TR * W + 5 * TR1 * W + 2 * 5 * 4 * W) + ft * 3 * 5 * TR * W;
 }
 
+// One sweep of W pencils by one CTA.  colbase[c] = offset of pencil c's first cell, colok[c] =
+// whether pencil c exists, stride = distance between consecutive cells of a pencil, n = pencil
+// length, S = slab pitch.  tsm = dynamic shared memory of tile_smem_bytes<W>(Lc).  Must be
+// called by all threads of the CTA.
 template <int METHOD, int SLOPE, typename FT, int DIR, int W>
-__global__ void __launch_bounds__(256, 4) sweep_tile_kernel(TileArgs a, FluidConsts<FT> c)
+__device__ __forceinline__ void tile_sweep(double *qbase, int64_t S, const int64_t *colbase, const bool *colok,
+                                           int64_t stride, int n, int Lc, double lambda, const FluidConsts<FT> &c,
+                                           double *tsm)
 {
-    extern __shared__ __align__(16) double tsm[];
-    const int Lc = a.Lc, n = a.n;
     const int TR = Lc + 8, TR1 = Lc + 4;
     double *U0t = tsm;                       // [5][TR][W]
     double *U1t = U0t + 5 * TR * W;          // [5][TR1][W]
@@ -510,34 +514,13 @@ __global__ void __launch_bounds__(256, 4) sweep_tile_kernel(TileArgs a, FluidCon
     FT *PA = reinterpret_cast<FT *>(first + 5 * 4 * W);  // [5][TR][W]
     FT *PB = PA + 5 * TR * W;
     FT *PC = PB + 5 * TR * W;
-    const int64_t S = a.slab;
-    const double lambda = a.lambda;
     constexpr int s0 = slot_of<METHOD, DIR>(0), s1 = slot_of<METHOD, DIR>(1), s2 = slot_of<METHOD, DIR>(2),
                   s3 = slot_of<METHOD, DIR>(3), s4 = slot_of<METHOD, DIR>(4);
     const int slots[5] = {s0, s1, s2, s3, s4};
-
-    // base offset of my W columns
-    __shared__ int64_t colbase[W];
-    __shared__ bool colok[W];
-    int64_t stride;
-    if (DIR == 1) stride = 1;
-    else if (DIR == 2) stride = a.nx;
-    else stride = (int64_t)a.nx * a.ny;
-    if (threadIdx.x < W) {
-        int64_t p = (int64_t)blockIdx.x * W + threadIdx.x;
-        colok[threadIdx.x] = p < a.npencil;
-        if (p >= a.npencil) p = 0;
-        int64_t b;
-        if (DIR == 1) b = p * a.nx;
-        else if (DIR == 2) b = (p % a.nx) + (int64_t)a.nx * a.ny * (p / a.nx);
-        else b = p;
-        colbase[threadIdx.x] = b;
-    }
-    __syncthreads();
+    auto IDX = [&](int k, int r, int col, int R) { return (k * R + r) * W + col; };
 
     const int nchunks = (n + Lc - 1) / Lc;
     const bool single = (nchunks == 1);
-    auto IDX = [&](int k, int r, int col, int R) { return (k * R + r) * W + col; };
 
     for (int ch = 0; ch < nchunks; ch++) {
         const int cb = ch * Lc;
@@ -547,7 +530,7 @@ __global__ void __launch_bounds__(256, 4) sweep_tile_kernel(TileArgs a, FluidCon
         for (int it = threadIdx.x; it < tr * W; it += blockDim.x) {
             const int r = it / W, col = it - r * W;
             const int cell = mod_n(cb - 4 + r, n);
-            const double *src = a.q + colbase[col] + (int64_t)cell * stride;
+            const double *src = qbase + colbase[col] + (int64_t)cell * stride;
 #pragma unroll
             for (int k = 0; k < 5; k++) U0t[IDX(k, r, col, TR)] = src[slots[k] * S];
         }
@@ -557,7 +540,7 @@ __global__ void __launch_bounds__(256, 4) sweep_tile_kernel(TileArgs a, FluidCon
             for (int it = threadIdx.x; it < 4 * W; it += blockDim.x) {
                 const int r = it / W, col = it - r * W;
                 if (!colok[col]) continue;
-                double *dst = a.q + colbase[col] + (int64_t)(cb - 4 + r) * stride;
+                double *dst = qbase + colbase[col] + (int64_t)(cb - 4 + r) * stride;
 #pragma unroll
                 for (int k = 0; k < 5; k++) dst[slots[k] * S] = pend[IDX(k, r, col, 4)];
             }
@@ -664,7 +647,7 @@ __global__ void __launch_bounds__(256, 4) sweep_tile_kernel(TileArgs a, FluidCon
 #pragma unroll
                 for (int k = 0; k < 5; k++) pend[IDX(k, pr, col, 4)] = out[k];
             } else if (colok[col]) {
-                double *dst = a.q + colbase[col] + (int64_t)cell * stride;
+                double *dst = qbase + colbase[col] + (int64_t)cell * stride;
 #pragma unroll
                 for (int k = 0; k < 5; k++) dst[slots[k] * S] = out[k];
             }
@@ -676,8 +659,8 @@ __global__ void __launch_bounds__(256, 4) sweep_tile_kernel(TileArgs a, FluidCon
         for (int it = threadIdx.x; it < 4 * W; it += blockDim.x) {
             const int r = it / W, col = it - r * W;
             if (!colok[col]) continue;
-            double *dl = a.q + colbase[col] + (int64_t)(cbl + lenl - 4 + r) * stride;
-            double *df = a.q + colbase[col] + (int64_t)r * stride;
+            double *dl = qbase + colbase[col] + (int64_t)(cbl + lenl - 4 + r) * stride;
+            double *df = qbase + colbase[col] + (int64_t)r * stride;
 #pragma unroll
             for (int k = 0; k < 5; k++) {
                 dl[slots[k] * S] = pend[IDX(k, r, col, 4)];
@@ -685,6 +668,31 @@ __global__ void __launch_bounds__(256, 4) sweep_tile_kernel(TileArgs a, FluidCon
             }
         }
     }
+    __syncthreads();
+}
+
+template <int METHOD, int SLOPE, typename FT, int DIR, int W>
+__global__ void __launch_bounds__(256, 4) sweep_tile_kernel(TileArgs a, FluidConsts<FT> c)
+{
+    extern __shared__ __align__(16) double tsm[];
+    __shared__ int64_t colbase[W];
+    __shared__ bool colok[W];
+    int64_t stride;
+    if (DIR == 1) stride = 1;
+    else if (DIR == 2) stride = a.nx;
+    else stride = (int64_t)a.nx * a.ny;
+    if (threadIdx.x < W) {
+        int64_t p = (int64_t)blockIdx.x * W + threadIdx.x;
+        colok[threadIdx.x] = p < a.npencil;
+        if (p >= a.npencil) p = 0;
+        int64_t b;
+        if (DIR == 1) b = p * a.nx;
+        else if (DIR == 2) b = (p % a.nx) + (int64_t)a.nx * a.ny * (p / a.nx);
+        else b = p;
+        colbase[threadIdx.x] = b;
+    }
+    __syncthreads();
+    tile_sweep<METHOD, SLOPE, FT, DIR, W>(a.q, a.slab, colbase, colok, stride, a.n, a.Lc, a.lambda, c, tsm);
 }
 
 }  // namespace ib

@@ -10,6 +10,11 @@
  * reference kernels are SIMT FP64; their per-thread expressions are reproduced here per cell).
  * The transposes the reference performs between sweeps (cudaArrayRotateB.cu) only move data,
  * so the oracle sweeps each pencil in place with the matching stride instead.
+ *
+ * Pinned: tests/test_golden_cpu.py checks this oracle bit for bit against golden vectors made by
+ * the reference's own kernels compiled with -fmad=false (tests/golden/make_golden.py,
+ * oracle/ref_harness/) for HLL, HLLC and Xin-Jin fluid steps, the CFL timestep and the LogTrap
+ * drag integrators.
  */
 #include "imogen_oracle.h"
 

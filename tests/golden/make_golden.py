@@ -1,0 +1,154 @@
+"""Generate golden vectors with the reference's own GPU code (run on a machine with a GPU).
+
+Loads the reference libraries built by oracle/ref_harness/Makefile (oracle/_ref/), which compile
+imogenproject/gpuImogen's gpuclass sources unchanged for sm_100a, runs small seeded cases through
+the reference's entry points (performFluidUpdate_3D, computeLocalCFLTimestep +
+calculateSoundspeed, sourcefunction_2FluidDrag) and writes one .npz per case:
+
+    input  (5, slab) float64    initial state (seeded generators in gpuimogen_b200/problems.py)
+    params                      method, limiter, gamma, rho_min, c_iso, h, bc, cfl, niter
+    out_fast / dts_fast         reference built as it builds itself (FMA contraction on)
+    out_strict / dts_strict     reference built with -fmad=false (comparable bit for bit)
+
+Boundary conditions are limited to circular, const and mirror: the reference's outflow and linear
+extrapolation kernels write outside their rows (cudaStatics.cu / boundaryConds.cu), so they are not
+run here.
+
+Usage: python tests/golden/make_golden.py OUTDIR
+"""
+import ctypes
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from gpuimogen_b200 import problems  # noqa: E402
+
+REF = os.path.join(ROOT, "oracle", "_ref")
+BC = {"circular": 0, "mirror": 1, "const": 4}
+
+TG = [5 / 3.0, 3.3e-27, 8.4e-6, 0.7, 2.4e-19, 0.2, 1.381e-23, -1.0]
+TD = [1.01, 3e-11, 0.0, 0.0, np.pi * 25e-12, 0.0, 1.381e-23, 0.1]
+
+
+def lib(limiter, strict):
+    name = "libimogen_ref_%s%s.so" % (limiter, "_strict" if strict else "")
+    L = ctypes.CDLL(os.path.join(REF, name))
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.ref_run.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int64, ctypes.c_double,
+                          ctypes.c_double, ctypes.c_double, ctypes.c_int, dp, ip, ctypes.c_double, ctypes.c_int, dp]
+    L.ref_cfl.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int64, ctypes.c_double,
+                          ctypes.c_int, dp, dp]
+    L.ref_drag.argtypes = [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int64, dp, dp,
+                           ctypes.c_double, ctypes.c_int]
+    return L
+
+
+def P(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+FLUID_CASES = [
+    # name, generator, shape, method, limiter, gamma, c_iso, bc, cfl, niter
+    ("kh_hllc_mc", "kh", (20, 16, 12), 2, "mc", 5 / 3.0, -1.0, ["circular"] * 6, 0.4, 5),
+    ("smooth_hllc_ospre_bc", "smooth", (18, 14, 10), 2, "ospre", 1.4, -1.0,
+     ["const", "const", "mirror", "mirror", "const", "mirror"], 0.4, 4),
+    ("jumpy_hllc_mc", "jumpy", (16, 12, 10), 2, "mc", 1.4, -1.0, ["circular"] * 6, 0.3, 3),
+    ("jumpy_hll_ospre_bc", "jumpy", (16, 12, 10), 1, "ospre", 1.4, -1.0,
+     ["mirror", "mirror", "const", "const", "circular", "circular"], 0.3, 3),
+    ("iso_hll_ospre", "smooth", (16, 12, 1), 1, "ospre", 1.4, 0.3, ["circular"] * 6, 0.3, 4),
+    ("sod_hll_const", "sod", (256, 1, 1), 1, "ospre", 1.4, -1.0, ["const"] * 6, 0.4, 25),
+    ("sod_hllc_const", "sod", (256, 1, 1), 2, "mc", 1.4, -1.0, ["const"] * 6, 0.4, 25),
+    ("sod_xj_const", "sod", (256, 1, 1), 3, "ospre", 1.4, -1.0, ["const"] * 6, 0.4, 25),
+]
+# No multi-dimensional Xin-Jin case: on a 32x32x1 periodic grid the reference's Xin-Jin prediction
+# kernel (cukern_XinJinHydro_step, cudaFluidStep.cu:421, launched with a 32x4 block) made an illegal
+# memory access on a B200, so the reference's Xin-Jin path is only run in 1-D here.
+
+
+def make_input(gen, shape, gamma):
+    if gen == "kh":
+        return problems.kelvin_helmholtz(shape, gamma=gamma, seed=7)
+    if gen == "smooth":
+        return problems.random_smooth(shape, gamma=gamma, seed=23, amp=0.3)
+    if gen == "jumpy":
+        return problems.random_jumpy(shape, gamma=gamma, seed=29)
+    if gen == "sod":
+        return problems.sod(shape[0], gamma)
+    raise ValueError(gen)
+
+
+def main(outdir):
+    os.makedirs(outdir, exist_ok=True)
+    index = {}
+    for name, gen, shape, method, limiter, gamma, c_iso, bc, cfl, niter in FLUID_CASES:
+        q0 = make_input(gen, shape, gamma)
+        h = np.array([1.0 / s for s in shape])
+        bca = (ctypes.c_int * 6)(*[BC[b] for b in bc])
+        rec = {"input": q0}
+        for strict in (False, True):
+            q = q0.copy()
+            dts = np.zeros(niter)
+            rc = lib(limiter, strict).ref_run(P(q), shape[0], shape[1], shape[2], q.shape[1], gamma, 1e-5, c_iso,
+                                               method, P(h), bca, cfl, niter, P(dts))
+            assert rc == 0, (name, rc)
+            tag = "strict" if strict else "fast"
+            rec["out_" + tag] = q
+            rec["dts_" + tag] = dts
+        meta = dict(kind="fluid", gen=gen, shape=list(shape), method=method, limiter=limiter, gamma=gamma,
+                    rho_min=1e-5, c_iso=c_iso, bc=bc, cfl=cfl, niter=niter)
+        np.savez_compressed(os.path.join(outdir, name + ".npz"), meta=json.dumps(meta), **rec)
+        index[name] = meta
+        print("wrote", name, flush=True)
+
+    # CFL timesteps
+    cfl_rec = {}
+    for gen, shape, gamma in (("jumpy", (17, 13, 9), 1.4), ("smooth", (40, 30, 1), 5 / 3.0), ("sod", (300, 1, 1), 1.4)):
+        q = make_input(gen, shape, gamma)
+        h = np.array([0.02, 0.03, 0.05])
+        for method in (1, 2, 3):
+            for strict in (False, True):
+                t = ctypes.c_double(0)
+                rc = lib("ospre", strict).ref_cfl(P(q), shape[0], shape[1], shape[2], q.shape[1], gamma, method, P(h),
+                                                  ctypes.byref(t))
+                assert rc == 0
+                cfl_rec["%s_m%d_%s" % (gen, method, "strict" if strict else "fast")] = t.value
+    np.savez_compressed(os.path.join(outdir, "cfl.npz"), values=json.dumps(cfl_rec))
+    print("wrote cfl", flush=True)
+
+    # two-fluid drag, LogTrap2 / LogTrap3
+    shape = (16, 8, 1)
+    n = 128
+    rng = np.random.Generator(np.random.Philox(41))
+    cube = (1, 8, 16)
+    rho_g = 1.0 + 0.1 * rng.uniform(-1, 1, n)
+    gas = problems.pack(shape, rho_g.reshape(cube), 0, (rho_g * rng.uniform(-1e-2, 1e-2, n)).reshape(cube),
+                        (rho_g * rng.uniform(-1e-2, 1e-2, n)).reshape(cube), 0)
+    gas[1, :n] = 1.0 / (5 / 3.0 - 1) + 0.5 * (gas[2, :n] ** 2 + gas[3, :n] ** 2) / rho_g
+    rho_d = rho_g * 10 ** rng.uniform(-2, 0, n)
+    dust = problems.pack(shape, rho_d.reshape(cube), 0, (rho_d * rng.uniform(-2e-2, 2e-2, n)).reshape(cube), 0, 0)
+    dust[1, :n] = 0.5 * dust[2, :n] ** 2 / rho_d + 1e-4 * rho_d
+    drag = {"gas": gas, "dust": dust}
+    tg, td = np.array(TG), np.array(TD)
+    for method in (4, 5):
+        for strict in (False, True):
+            g, d = gas.copy(), dust.copy()
+            rc = lib("ospre", strict).ref_drag(P(g), P(d), shape[0], shape[1], shape[2], g.shape[1], P(tg), P(td),
+                                               0.05, method)
+            assert rc == 0
+            tag = "m%d_%s" % (method, "strict" if strict else "fast")
+            drag["gas_" + tag] = g
+            drag["dust_" + tag] = d
+    np.savez_compressed(os.path.join(outdir, "drag.npz"), meta=json.dumps({"shape": list(shape), "tg": TG, "td": TD,
+                                                                          "dt": 0.05}), **drag)
+    print("wrote drag", flush=True)
+    with open(os.path.join(outdir, "index.json"), "w") as f:
+        json.dump(index, f, indent=1)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__)))
