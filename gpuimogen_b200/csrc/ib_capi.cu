@@ -94,6 +94,16 @@ double *Scratch::cfl_tau()
     return tau_;
 }
 
+unsigned int *Scratch::wait_flag()
+{
+    std::lock_guard<std::mutex> g(g_scratch_mu);
+    if (!wait_flag_) {
+        if (cudaMalloc(&wait_flag_, sizeof(unsigned int)) != cudaSuccess) { wait_flag_ = nullptr; return nullptr; }
+        if (cudaMemset(wait_flag_, 0, sizeof(unsigned int)) != cudaSuccess) return nullptr;
+    }
+    return wait_flag_;
+}
+
 double *Scratch::bytes(size_t nbytes)
 {
     std::lock_guard<std::mutex> g(g_scratch_mu);
@@ -232,6 +242,20 @@ const char *ib_status_string(int status)
 int ib_last_cuda_error(void) { return g_last_cuda_error; }
 
 long long ib_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int ib_device_wait_status(int clear)
+{
+    unsigned int *f = ib::scratch().wait_flag();
+    if (!f) return IB_ERROR_NOMEM;
+    unsigned int v = 0;
+    int rc = ib::check_cuda(cudaMemcpy(&v, f, sizeof(v), cudaMemcpyDeviceToHost));
+    if (rc) return rc;
+    if (clear && v) {
+        rc = ib::check_cuda(cudaMemset(f, 0, sizeof(unsigned int)));
+        if (rc) return rc;
+    }
+    return (int)v;
+}
 
 int ib_cudaFluidStep(ib_fluid *fluid, const ib_geometry *geo, const double *params, int nparams,
                      const ib_numerics *num, void *stream)

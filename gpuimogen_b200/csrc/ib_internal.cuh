@@ -23,6 +23,7 @@ public:
     unsigned int *cfl_counter();
     double *cfl_tau();
     double *bytes(size_t nbytes);  // general scratch (reused between calls on the device)
+    unsigned int *wait_flag();     // set by a kernel whose bounded wait ran out (zeroed once)
 
 private:
     double *partial_ = nullptr;
@@ -31,6 +32,7 @@ private:
     double *tau_ = nullptr;
     double *gen_ = nullptr;
     size_t gen_n_ = 0;
+    unsigned int *wait_flag_ = nullptr;
 };
 Scratch &scratch();
 

@@ -18,6 +18,7 @@
 #pragma once
 
 #include "ib_common.cuh"
+#include "ib_tma.cuh"
 
 namespace ib {
 
@@ -317,6 +318,183 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
             for (int k = 0; k < 5; k++) q[(int64_t)slot_of<METHOD, 1>(k) * S + i] = u1[m][k];
         }
     }
+}
+
+// ------------------------------------------------------------------------------------------
+// TMA-fed pencil pipeline: a persistent CTA walks pencil blocks b = blockIdx.x, +gridDim.x, ...
+// Each block is W adjacent whole pencils (x: one row, W = 1).  Thread 0 keeps two TMA loads
+// in flight (double-buffered U0 tiles, one mbarrier each), so the next block's 5 slabs arrive
+// while this one is computed; results leave through a TMA store from a third tile.  The tile
+// layout is the TMA box's: [memory slab k][cell i][column] with the column fastest.  The
+// arithmetic per cell is the row kernel's.
+// Dynamic shared memory: 3 tiles of 5*W*n doubles (each rounded to 128 B) + 2 planes of
+// 5*W*n elements of FT.
+// ------------------------------------------------------------------------------------------
+struct PipeArgs {
+    int n;              // pencil length
+    int npw;            // pencil blocks per line of x (nx / W; 1 for x sweeps)
+    int64_t nblocks;    // pencil blocks in the grid
+    double lambda;
+    unsigned int *err;  // set to 1 when a TMA wait ran out
+};
+
+__host__ __device__ __forceinline__ size_t pipe_tile_bytes(int n, int W)
+{
+    return ((size_t)40 * n * W + 127) / 128 * 128;
+}
+
+template <int DIR>
+__device__ __forceinline__ void pipe_load(void *dst, const CUtensorMap *tm, int64_t b, int npw, int W, uint64_t *bar)
+{
+    if (DIR == 1) tma_load_3d(dst, tm, 0, (int)b, 0, bar);
+    else tma_load_4d(dst, tm, (int)(b % npw) * W, 0, (int)(b / npw), 0, bar);
+}
+
+template <int DIR>
+__device__ __forceinline__ void pipe_store(const CUtensorMap *tm, const void *src, int64_t b, int npw, int W)
+{
+    if (DIR == 1) tma_store_3d(tm, src, 0, (int)b, 0);
+    else tma_store_4d(tm, src, (int)(b % npw) * W, 0, (int)(b / npw), 0);
+}
+
+template <int METHOD, int SLOPE, typename FT, int DIR, int W>
+__global__ void __launch_bounds__(512, 2)
+    sweep_pipe_kernel(const __grid_constant__ CUtensorMap tm, PipeArgs a, FluidConsts<FT> c)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[2];
+    const int n = a.n;
+    const int NW = n * W;
+    const size_t tb = pipe_tile_bytes(n, W);
+    double *U[2] = {reinterpret_cast<double *>(smem_raw), reinterpret_cast<double *>(smem_raw + tb)};
+    double *O = reinterpret_cast<double *>(smem_raw + 2 * tb);
+    FT *SA = reinterpret_cast<FT *>(smem_raw + 3 * tb);
+    FT *SB = SA + 5 * NW;
+    const uint32_t tile_tx = (uint32_t)(40 * NW);
+    constexpr int s0 = slot_of<METHOD, DIR>(0), s1 = slot_of<METHOD, DIR>(1), s2 = slot_of<METHOD, DIR>(2),
+                  s3 = slot_of<METHOD, DIR>(3), s4 = slot_of<METHOD, DIR>(4);
+    const int slots[5] = {s0, s1, s2, s3, s4};
+    const int col = (W == 1) ? 0 : (int)(threadIdx.x % W);
+    const int i = (int)(threadIdx.x / W);
+    const bool act = i < n;
+    const int il = (i == 0) ? n - 1 : i - 1, ir = (i == n - 1) ? 0 : i + 1;
+    auto SI = [&](int k, int j) { return (k * n + j) * W + col; };
+    const double lambda = a.lambda;
+    const int64_t step = gridDim.x;
+    const bool leader = threadIdx.x == 0;
+
+    if (leader) {
+        prefetch_tmap(&tm);
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    // issued0/1: a load into tile 0/1 is in flight (leader's bookkeeping, for draining)
+    bool issued0 = false, issued1 = false;
+    if (leader) {
+        const int64_t b0 = blockIdx.x, b1 = blockIdx.x + step;
+        if (b0 < a.nblocks) {
+            mbar_arrive_expect_tx(&full[0], tile_tx);
+            pipe_load<DIR>(U[0], &tm, b0, a.npw, W, &full[0]);
+            issued0 = true;
+        }
+        if (b1 < a.nblocks) {
+            mbar_arrive_expect_tx(&full[1], tile_tx);
+            pipe_load<DIR>(U[1], &tm, b1, a.npw, W, &full[1]);
+            issued1 = true;
+        }
+    }
+    uint32_t phase0 = 0, phase1 = 0;
+    int it = 0;
+    for (int64_t b = blockIdx.x; b < a.nblocks; b += step, it++) {
+        const int t = it & 1;
+        double *Ut = U[t];
+        const uint32_t par = t ? phase1 : phase0;
+        const bool ok = mbar_wait(&full[t], par);
+        if (t) phase1 ^= 1; else phase0 ^= 1;
+        double u0[5], u1[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) u0[k] = act ? Ut[SI(slots[k], i)] : 1.0;
+        if (!__syncthreads_and(ok)) {
+            // a tile never arrived: report, drain what is still in flight, leave
+            if (leader) {
+                atomicOr(a.err, 1u);
+                mbar_wait(&full[t], par);  // give the late tile one more bounded wait
+                if (t == 0 && issued1) mbar_wait(&full[1], phase1);
+                if (t == 1 && issued0) mbar_wait(&full[0], phase0);
+                bulk_wait_all();
+            }
+            return;
+        }
+        // tile t is free again: prefetch the block after next into it
+        if (leader) {
+            const int64_t bn = b + 2 * step;
+            if (bn < a.nblocks) {
+                fence_proxy_async_smem();
+                mbar_arrive_expect_tx(&full[t], tile_tx);
+                pipe_load<DIR>(Ut, &tm, bn, a.npw, W, &full[t]);
+            } else {
+                if (t == 0) issued0 = false; else issued1 = false;
+            }
+        }
+        V5<FT> keep;
+#pragma unroll
+        for (int stage = 0; stage < 2; stage++) {
+            double *u = (stage == 0) ? u0 : u1;
+            if (act) {
+                V5<FT> w = stage_prims<METHOD, DIR, FT>(u, c);
+#pragma unroll
+                for (int k = 0; k < 5; k++) SA[SI(k, i)] = w.a[k];
+            }
+            __syncthreads();
+            if (act) {
+                V5<FT> w, dl, dr, L;
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    w.a[k] = SA[SI(k, i)];
+                    dl.a[k] = w.a[k] - SA[SI(k, il)];
+                    dr.a[k] = SA[SI(k, ir)] - w.a[k];
+                }
+                stage_faces<METHOD, SLOPE, FT>(c, w, dl, dr, L, keep);
+#pragma unroll
+                for (int k = 0; k < 5; k++) SB[SI(k, i)] = L.a[k];
+            }
+            __syncthreads();
+            if (act) {
+                V5<FT> Lr;
+#pragma unroll
+                for (int k = 0; k < 5; k++) Lr.a[k] = SB[SI(k, ir)];
+                keep = stage_flux<METHOD, FT>(c, keep, Lr);
+#pragma unroll
+                for (int k = 0; k < 5; k++) SA[SI(k, i)] = keep.a[k];
+            }
+            __syncthreads();
+            if (act) {
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    double df = (double)keep.a[k] - (double)SA[SI(k, il)];
+                    if (stage == 0) u1[k] = u0[k] - lambda * df;
+                    else u1[k] = .5 * (u1[k] + u0[k] - lambda * df);
+                }
+            }
+            if (stage == 0) __syncthreads();
+        }
+        // the previous block's store must have read O before O is overwritten
+        if (leader) bulk_wait_read_all();
+        __syncthreads();
+        if (act) {
+#pragma unroll
+            for (int k = 0; k < 5; k++) O[SI(slots[k], i)] = u1[k];
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (leader) {
+            pipe_store<DIR>(&tm, O, b, a.npw, W);
+            bulk_commit();
+        }
+    }
+    if (leader) bulk_wait_all();
 }
 
 // The HLL corrector adds (fluid after the floors of the predictor's pressure pass) and

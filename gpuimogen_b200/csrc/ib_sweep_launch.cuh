@@ -28,7 +28,9 @@ int launch_tile_dw(double *q, int64_t slab, const int grid[3], double lambda, co
     TileArgs a{q, slab, grid[0], grid[1], grid[2], n, npencil, Lc, lambda};
     const size_t shm = tile_smem_bytes<W>(Lc, sizeof(FT));
     static int attr_bytes = 0;
-    if ((int)shm > 48 * 1024 && (int)shm > attr_bytes) {
+    // opt in whenever the size grows: without it the limit is 48 KB including the static
+    // shared memory and the 1 KB the driver reserves per block (48640 B at 256-cell pencils fails)
+    if ((int)shm > attr_bytes) {
         int rc = check_cuda(cudaFuncSetAttribute(sweep_tile_kernel<METHOD, SLOPE, FT, DIR, W>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
         if (rc) return rc;
@@ -36,6 +38,63 @@ int launch_tile_dw(double *q, int64_t slab, const int grid[3], double lambda, co
     }
     const unsigned nblk = (unsigned)((npencil + W - 1) / W);
     sweep_tile_kernel<METHOD, SLOPE, FT, DIR, W><<<nblk, 256, shm, st>>>(a, c);
+    return check_launch();
+}
+
+// TMA-fed persistent pipeline (sweep_pipe_kernel): W whole pencils of length n <= 256 per
+// block, W*n <= 512 threads.  Returns IB_ERROR_NOIMPLEMENT (caller falls back) when the grid
+// does not meet TMA's rules: x even (16-byte strides and box rows), W dividing nx.
+template <int METHOD, int SLOPE, typename FT, int DIR, int W>
+int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c, cudaStream_t st)
+{
+    const int nx = grid[0], ny = grid[1], nz = grid[2];
+    const int n = grid[DIR - 1];
+    if (n > 256 || W * n > 512 || (nx & 1) || nx % W) return IB_ERROR_NOIMPLEMENT;
+    if (((uintptr_t)q & 15) || (slab * 8) % 16) return IB_ERROR_NOIMPLEMENT;
+    CUtensorMap tm;
+    uint64_t dims[4], strides[3];
+    uint32_t box[4];
+    int rank;
+    int64_t nblocks;
+    const int npw = (DIR == 1) ? 1 : nx / W;
+    if (DIR == 1) {
+        rank = 3;
+        dims[0] = nx; dims[1] = (uint64_t)ny * nz; dims[2] = 5;
+        strides[0] = (uint64_t)nx * 8; strides[1] = (uint64_t)slab * 8;
+        box[0] = nx; box[1] = 1; box[2] = 5;
+        nblocks = (int64_t)ny * nz;
+    } else {
+        rank = 4;
+        const uint64_t other = (DIR == 2) ? nz : ny;
+        dims[0] = nx; dims[1] = n; dims[2] = other; dims[3] = 5;
+        strides[0] = (DIR == 2) ? (uint64_t)nx * 8 : (uint64_t)nx * ny * 8;
+        strides[1] = (DIR == 2) ? (uint64_t)nx * ny * 8 : (uint64_t)nx * 8;
+        strides[2] = (uint64_t)slab * 8;
+        box[0] = W; box[1] = n; box[2] = 1; box[3] = 5;
+        nblocks = (int64_t)npw * other;
+    }
+    if (nblocks >= (int64_t)1 << 31) return IB_ERROR_NOIMPLEMENT;
+    int rc = encode_tmap_f64(&tm, q, rank, dims, strides, box);
+    if (rc) return rc;
+    unsigned int *err = scratch().wait_flag();
+    if (!err) return IB_ERROR_NOMEM;
+    const int nt = ((W * n + 31) / 32) * 32;
+    const size_t shm = 3 * pipe_tile_bytes(n, W) + (size_t)10 * W * n * sizeof(FT);
+    auto kern = sweep_pipe_kernel<METHOD, SLOPE, FT, DIR, W>;
+    static int attr_bytes = 0;
+    if ((int)shm > attr_bytes) {
+        rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        if (rc) return rc;
+        attr_bytes = (int)shm;
+    }
+    int per_sm = 0;
+    rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, shm));
+    if (rc) return rc;
+    if (per_sm < 1) return IB_ERROR_NOIMPLEMENT;
+    const int64_t want = (int64_t)per_sm * num_sms();
+    const unsigned nblk = (unsigned)std::min<int64_t>(want, nblocks);
+    PipeArgs a{n, npw, nblocks, lambda, err};
+    kern<<<nblk, nt, shm, st>>>(tm, a, c);
     return check_launch();
 }
 
@@ -57,12 +116,34 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
     const int64_t N = (int64_t)nx * ny * nz;
     if (n <= 0 || N <= 0) return IB_SUCCESSFUL;
 
+    static const bool use_pipe = [] {
+        const char *e = getenv("IMOGEN_B200_PIPE");  // 0 = the non-TMA kernels only
+        return !(e && e[0] == '0');
+    }();
+    // x rows load contiguously and the row kernel below is faster for them; y and z pencils
+    // go through the TMA-fed pipeline (IMOGEN_B200_PIPE=x also sends x rows there)
+    static const int pipe_x = [] {
+        const char *e = getenv("IMOGEN_B200_PIPE");
+        return (e && e[0] == 'x') ? 1 : 0;
+    }();
+    if (use_pipe && n <= 256 && (dir > 1 || pipe_x)) {
+        int rc;
+        if (dir == 1) rc = launch_pipe<METHOD, SLOPE, FT, 1, 1>(q, slab, grid, lambda, c, st);
+        else if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2>(q, slab, grid, lambda, c, st);
+        else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2>(q, slab, grid, lambda, c, st);
+        if (rc != IB_ERROR_NOIMPLEMENT) return rc;
+    }
+
     if (dir == 1 && nx <= 1024) {
         // one CTA per row, one or two cells per thread
         SweepArgs a{q, slab, nx, ny, nz, lambda};
         const int64_t rows = (int64_t)ny * nz;
         const size_t shm = (size_t)10 * nx * sizeof(FT);
-        if (nx <= 512) {
+        static const int xcpt = [] {
+            const char *e = getenv("IMOGEN_B200_XCPT");  // 2 = two cells per thread for all rows
+            return (e && e[0] == '2') ? 2 : 1;
+        }();
+        if (nx <= 512 && xcpt == 1) {
             int nt = ((nx + 31) / 32) * 32;
             sweep_row_kernel<METHOD, SLOPE, FT, 1><<<(unsigned)rows, nt, shm, st>>>(a, c);
         } else {

@@ -101,6 +101,7 @@ EXPORTS = {
                                            ctypes.POINTER(IbGeometry), ctypes.c_int,
                                            ctypes.POINTER(ctypes.c_double), ctypes.c_void_p,
                                            ctypes.c_void_p]),
+    "ib_device_wait_status": (ctypes.c_int, [ctypes.c_int]),
     "ib_cflTimestepNoAlloc": (ctypes.c_int, [ctypes.POINTER(IbFluid), ctypes.c_double,
                                              ctypes.POINTER(IbGeometry), ctypes.c_int, ctypes.c_void_p,
                                              ctypes.c_void_p]),
@@ -169,6 +170,11 @@ def _check(where, status):
 def launch_count():
     """Kernels launched through the library so far in this process."""
     return int(_lib().ib_launch_count())
+
+
+def device_wait_status(clear=False):
+    """0 when no bounded device wait of the TMA-fed sweeps has run out since the last clear."""
+    return int(_lib().ib_device_wait_status(1 if clear else 0))
 
 
 def slab_pitch(nx, ny, nz):

@@ -158,6 +158,13 @@ IB_API int ib_last_cuda_error(void);
 /* Number of kernels this process has launched through the library (all devices). */
 IB_API long long ib_launch_count(void);
 
+/* Health of the TMA-fed sweep kernels on the current device (no reference counterpart: the
+ * reference has no asynchronous copies).  Their waits for a tile are bounded; a wait that runs
+ * out makes the kernel leave early and sets a flag, which this call reads (synchronising with
+ * the device): 0 = no wait ran out, 1 = one did and the state of that sweep is invalid, < 0 =
+ * status code.  clear != 0 resets the flag. */
+IB_API int ib_device_wait_status(int clear);
+
 /* Replaces the cudaFluidStep mex (gpuclass/cudaFluidStep.cu:161-227): one SSPRK2 directional
  * sweep of one fluid, in place, without boundary fill.
  * params = [dt, purehydro, gamma, rho_min, method (1 HLL | 2 HLLC | 3 XJ), direction (1..3)

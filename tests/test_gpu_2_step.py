@@ -233,3 +233,55 @@ def test_kelvin_helmholtz_product_vs_oracle(cuda, ib, po):
         assert abs(dt - dt_ref) <= 1e-13 * dt_ref
     err = rel_l1(host(fl), ref, n)
     assert np.all(err <= 1e-12), err
+
+
+@pytest.mark.parametrize("method", [2, 1])
+def test_tma_pipeline_many_blocks_per_cta(cuda, ib, po, method):
+    """Grids with more pencil blocks than resident CTAs, so every persistent CTA of the TMA-fed
+    sweeps cycles through both prefetch tiles several times: strict build bit-exact against the
+    oracle, and no bounded device wait ran out."""
+    shape = (64, 48, 40)
+    n = shape[0] * shape[1] * shape[2]
+    q = problems.random_jumpy(shape, gamma=1.4, seed=53)
+    h = [1.0 / s for s in shape]
+    sp = po.step_params(0.0, h, 1.4, rho_min=1e-5, method=method, slope="mc")
+    ref = q.copy()
+    ib.use_variant("strict")
+    try:
+        ib.device_wait_status(clear=True)
+        fl = to_fluid(q, shape, bc="circular", gamma=1.4)
+        geo = ib.Geometry(shape, h)
+        for it in range(2):
+            sp.dt = 0.3 * po.cfl_timestep(ref, shape, 1.4, h, method)
+            for sd in (1, -1):
+                po.fluid_step_3d(ref, shape, sp, ["circular"] * 6, sd, it)
+                ib.fluidstep([fl], geo, [sp.dt, 1, sd, it, method], ib.numerics(slope="mc"))
+        out = host(fl)
+        assert ib.device_wait_status() == 0
+    finally:
+        ib.use_variant("product")
+    assert bits_equal(out, ref, n), first_diff(out, ref, n)
+
+
+@pytest.mark.parametrize("shape", [(5, 256, 6), (7, 6, 256), (6, 300, 4)])
+def test_tile_path_long_pencils(cuda, ib, po, shape):
+    """y/z pencils that the TMA-fed sweeps do not take (odd nx, or longer than 256 cells) run
+    through the chunked tile kernel: several chunks per pencil, strict build bit-exact."""
+    n = shape[0] * shape[1] * shape[2]
+    q = problems.random_smooth(shape, gamma=1.4, seed=61, amp=0.3)
+    h = [1.0 / s for s in shape]
+    sp = po.step_params(0.0, h, 1.4, rho_min=1e-5, method=2, slope="mc")
+    ref = q.copy()
+    ib.use_variant("strict")
+    try:
+        fl = to_fluid(q, shape, bc="circular", gamma=1.4)
+        geo = ib.Geometry(shape, h)
+        for it in range(2):
+            sp.dt = 0.4 * po.cfl_timestep(ref, shape, 1.4, h, 2)
+            for sd in (1, -1):
+                po.fluid_step_3d(ref, shape, sp, ["circular"] * 6, sd, it)
+                ib.fluidstep([fl], geo, [sp.dt, 1, sd, it, 2], ib.numerics(slope="mc"))
+        out = host(fl)
+    finally:
+        ib.use_variant("product")
+    assert bits_equal(out, ref, n), first_diff(out, ref, n)
