@@ -25,6 +25,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 SOURCES = [
     "ib_capi.cu",
     "ib_tma.cu",
+    "ib_ensemble.cu",
     "ib_sweep_hllc64.cu",
     "ib_sweep_hllc32.cu",
     "ib_sweep_hll64.cu",
@@ -33,7 +34,7 @@ SOURCES = [
     "ib_boundary.cu",
     "ib_drag.cu",
 ]
-HEADERS = ["ib_common.cuh", "ib_internal.cuh", "ib_sweep.cuh", "ib_sweep_launch.cuh", "ib_tma.cuh"]
+HEADERS = ["ib_common.cuh", "ib_internal.cuh", "ib_sweep.cuh", "ib_sweep_launch.cuh", "ib_tma.cuh", "ib_bc.cuh", "ib_cfl.cuh"]
 
 BASE_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",

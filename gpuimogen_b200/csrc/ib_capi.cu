@@ -104,6 +104,15 @@ unsigned int *Scratch::wait_flag()
     return wait_flag_;
 }
 
+unsigned int *Scratch::ensemble_counter()
+{
+    std::lock_guard<std::mutex> g(g_scratch_mu);
+    if (!ens_counter_) {
+        if (cudaMalloc(&ens_counter_, sizeof(unsigned int)) != cudaSuccess) { ens_counter_ = nullptr; return nullptr; }
+    }
+    return ens_counter_;
+}
+
 double *Scratch::bytes(size_t nbytes)
 {
     std::lock_guard<std::mutex> g(g_scratch_mu);

@@ -24,6 +24,7 @@ public:
     double *cfl_tau();
     double *bytes(size_t nbytes);  // general scratch (reused between calls on the device)
     unsigned int *wait_flag();     // set by a kernel whose bounded wait ran out (zeroed once)
+    unsigned int *ensemble_counter();  // work counter of the ensemble kernel
 
 private:
     double *partial_ = nullptr;
@@ -33,6 +34,7 @@ private:
     double *gen_ = nullptr;
     size_t gen_n_ = 0;
     unsigned int *wait_flag_ = nullptr;
+    unsigned int *ens_counter_ = nullptr;
 };
 Scratch &scratch();
 

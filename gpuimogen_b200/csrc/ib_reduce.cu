@@ -9,18 +9,10 @@
 #include <cstdio>
 #include <mutex>
 
+#include "ib_cfl.cuh"
 #include "ib_internal.cuh"
 
 namespace ib {
-
-// c_s^2 = gamma(gamma-1)(E - p^2/2rho)/rho, clamped at 0 (cudaSoundspeed.cu:184-191)
-__device__ __forceinline__ double soundspeed_cell(double rho, double E, double px, double py, double pz, double gg1)
-{
-    double rhoinv = 1 / rho;
-    double csq = gg1 * (E - .5 * (px * px + py * py + pz * pz) * rhoinv) * rhoinv;
-    if (csq < 0.0) csq = 0.0;
-    return sqrt(csq);
-}
 
 __global__ void soundspeed_kernel(const double *__restrict__ q, int64_t slab, int64_t n, double gg1,
                                   double *__restrict__ cs)
@@ -29,40 +21,6 @@ __global__ void soundspeed_kernel(const double *__restrict__ q, int64_t slab, in
         cs[x] = soundspeed_cell(q[x], q[x + slab], q[x + 2 * slab], q[x + 3 * slab], q[x + 4 * slab], gg1);
     }
 }
-
-// Signal-crossing time of one cell (cflTimestep.cu:254-340).  sim = spatial dimension.
-template <int SIM, bool XJ>
-__device__ __forceinline__ double cfl_cell(double rho, double px, double py, double pz, double cs, double hmin,
-                                           double hx, double hy, double hz)
-{
-    double u;
-    if constexpr (!XJ) {
-        double p;
-        if constexpr (SIM == 1) {
-            p = fabs(px);
-        } else {
-            double pp = px * px;
-            pp = pp + py * py;
-            if constexpr (SIM > 2) pp = pp + pz * pz;
-            p = sqrt(pp);
-        }
-        u = p / rho + cs;
-        u = hmin / u;
-    } else {
-        double v;
-        u = hx / (fabs(px) / rho + cs);
-        v = hy / (fabs(py) / rho + cs);
-        u = (u < v) ? u : v;
-        if constexpr (SIM > 2) {
-            v = hz / (fabs(pz) / rho + cs);
-            u = (u < v) ? u : v;
-        }
-    }
-    return u;
-}
-
-// NaN-ignoring minimum, as the reference's ternaries: a NaN candidate never replaces the running value
-__device__ __forceinline__ double min_keep(double cur, double cand) { return (cand < cur) ? cand : cur; }
 
 template <int SIM, bool XJ, bool FUSED>
 __global__ void __launch_bounds__(256) cfl_kernel(const double *__restrict__ q, const double *__restrict__ cs_in,

@@ -82,6 +82,18 @@ class IbThermo(ctypes.Structure):
                 ("c_isothermal", ctypes.c_double)]
 
 
+class IbEnsemble(ctypes.Structure):
+    _fields_ = [("q", ctypes.c_void_p), ("slab_pitch", ctypes.c_int64), ("offsets", ctypes.c_void_p),
+                ("h", ctypes.c_void_p), ("order", ctypes.c_void_p), ("t_out", ctypes.c_void_p),
+                ("iters_out", ctypes.c_void_p), ("nproblems", ctypes.c_int32), ("bc", ctypes.c_int32 * 2),
+                ("reserved", ctypes.c_int32)]
+
+
+class IbEnsembleTuning(ctypes.Structure):
+    _fields_ = [("threads", ctypes.c_int32), ("chunk", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
 EXPORTS = {
     "ib_slab_pitch": (ctypes.c_int64, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
     "ib_status_string": (ctypes.c_char_p, [ctypes.c_int]),
@@ -102,6 +114,10 @@ EXPORTS = {
                                            ctypes.POINTER(ctypes.c_double), ctypes.c_void_p,
                                            ctypes.c_void_p]),
     "ib_device_wait_status": (ctypes.c_int, [ctypes.c_int]),
+    "ib_riemannEnsemble": (ctypes.c_int, [ctypes.POINTER(IbEnsemble), ctypes.POINTER(IbFluidThermo), ctypes.c_int,
+                                          ctypes.c_double, ctypes.c_double, ctypes.c_int32,
+                                          ctypes.POINTER(IbNumerics), ctypes.POINTER(IbEnsembleTuning),
+                                          ctypes.c_void_p]),
     "ib_cflTimestepNoAlloc": (ctypes.c_int, [ctypes.POINTER(IbFluid), ctypes.c_double,
                                              ctypes.POINTER(IbGeometry), ctypes.c_int, ctypes.c_void_p,
                                              ctypes.c_void_p]),

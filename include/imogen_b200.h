@@ -235,6 +235,48 @@ IB_API int ib_cudaSource2FluidDrag(ib_fluid *gas, ib_fluid *dust, const ib_therm
                             const ib_thermo *thermo_dust, const ib_geometry *geo,
                             const double *params, int nparams, void *stream);
 
+/* ---------------------------------------------------------------------------------------------
+ * Batched ensemble of independent 1-D problems (no single reference counterpart: each problem
+ * is what the reference runs as a 1-D fluid, the main loop of imogen.m:115-139 with
+ * TimeManager.m:124-186,270-277 deciding dt, performFluidUpdate_3D's 1-D shortcut
+ * flux.cu:52-68 for each half step and cflTimestep.cu:107-252 for tau).  Every problem runs on
+ * its own clock to its own end, all in one kernel launch.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct ib_ensemble {
+    double *q;                /* device: 5 slabs [rho, E, px, py, pz] of slab_pitch doubles; problem p
+                                 occupies cells offsets[p] .. offsets[p+1]-1 of every slab */
+    int64_t slab_pitch;
+    const int64_t *offsets;   /* device, nproblems + 1 entries, increasing, each problem >= 9 cells */
+    const double *h;          /* device, cell width of each problem */
+    const int32_t *order;     /* device, order in which CTAs pick problems (a permutation of
+                                 0..nproblems-1, e.g. longest first), or NULL for 0, 1, ... */
+    double *t_out;            /* device, simulated time each problem reached */
+    int32_t *iters_out;       /* device, iterations each problem took */
+    int32_t nproblems;
+    int32_t bc[2];            /* -x and +x boundary modes (IB_BC_*), halo depth 4 */
+    int32_t reserved;
+} ib_ensemble;
+
+/* Launch shape of the ensemble kernel (what the autotuner chooses); NULL or zeros = defaults
+ * (256 threads, chunk 248 cells, as many CTAs per SM as fit). */
+typedef struct ib_ensemble_tuning {
+    int32_t threads;          /* 128, 256 or 512 */
+    int32_t chunk;            /* cells per shared-memory chunk, 8 .. threads - 8 */
+    int32_t ctas_per_sm;      /* 0 = occupancy limit */
+    int32_t reserved;
+} ib_ensemble_tuning;
+
+/* Runs every problem of the ensemble to t_end (or itermax iterations) with the HLL or HLLC
+ * method (1 or 2): per iteration tau = CFL reduction over the problem, dt = cfl * tau clipped so
+ * that t + 2 dt <= t_end, forward and backward SSPRK2 sweep each followed by the boundary fill,
+ * t += 2 dt (compensated).  num selects slope limiter (Ospre or MC) and precision (FP64 or the
+ * FP32-flux form for HLLC).  One persistent launch: CTAs take problems from a device work
+ * counter; the call does not synchronise and can be captured in a CUDA graph after a first
+ * call outside capture (the first call allocates the counter). */
+IB_API int ib_riemannEnsemble(const ib_ensemble *e, const ib_fluid_thermo *thermo, int method, double cfl,
+                              double t_end, int32_t itermax, const ib_numerics *num,
+                              const ib_ensemble_tuning *tuning, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
