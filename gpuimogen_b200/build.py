@@ -26,6 +26,8 @@ SOURCES = [
     "ib_capi.cu",
     "ib_tma.cu",
     "ib_ensemble.cu",
+    "ib_mlp.cu",
+    "ib_drag_learned.cu",
     "ib_sweep_hllc64.cu",
     "ib_sweep_hllc32.cu",
     "ib_sweep_hll64.cu",
@@ -34,7 +36,7 @@ SOURCES = [
     "ib_boundary.cu",
     "ib_drag.cu",
 ]
-HEADERS = ["ib_common.cuh", "ib_internal.cuh", "ib_sweep.cuh", "ib_sweep_launch.cuh", "ib_tma.cuh", "ib_bc.cuh", "ib_cfl.cuh"]
+HEADERS = ["ib_common.cuh", "ib_internal.cuh", "ib_sweep.cuh", "ib_sweep_launch.cuh", "ib_tma.cuh", "ib_bc.cuh", "ib_cfl.cuh", "ib_drag.cuh", "ib_tcgen05.cuh"]
 
 BASE_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",

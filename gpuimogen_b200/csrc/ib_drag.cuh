@@ -1,0 +1,142 @@
+// ib_drag.cuh -- drag law and LogTrap update shared by the exact and the learned drag kernels
+// (gpuclass/cudaSource2FluidDrag.cu).
+#pragma once
+
+#include <cmath>
+
+#include "ib_common.cuh"
+
+namespace ib {
+
+struct DragParams {
+    double visc0, viscpow, lampow, alpha, beta, delta, epsilon;
+};
+
+// allregimeCdrag (cudaSource2FluidDrag.cu:819-833)
+__device__ __forceinline__ double allregime_cdrag(double Re, double Kn)
+{
+    double cunningham = 1 + Kn * (1.142 + 1 * 0.558 * exp(-0.999 / Kn));
+    double C_drag = (3 / Re + .45 * pow(Re, -.319) + .0509 * Re / (8710 + Re)) / cunningham;
+    return C_drag;
+}
+
+// cukern_GasDustDrag_GeneralLinearCore with srcBlock 0 (cudaSource2FluidDrag.cu:836-890)
+__device__ __forceinline__ double drag_k(const DragParams &d, double rhoA, double rhoB, double magdv, double u, bool &skip)
+{
+    if (magdv < 1e-9) { skip = true; return 0; }
+    skip = false;
+    double Tn = d.alpha * u;
+    double Re = d.delta * rhoA * magdv * pow(Tn, d.viscpow);
+    double Kn = d.beta * pow(Tn, d.lampow) / rhoA;
+    double Cd_hat = allregime_cdrag(Re, Kn);
+    return Cd_hat * magdv * (rhoA + rhoB) * d.epsilon;
+}
+
+// LogTrap effective rate k_eff of one cell from rho_gas g0, rho_dust d0, |dv| t0 and specific
+// internal energy t1 (cukern_LogTrapSolve, cudaSource2FluidDrag.cu:1531-1660); the update then
+// scales dv by exp(-t k_eff).
+template <int ORDER>
+__device__ __forceinline__ double logtrap_keff(const DragParams &d, double g0, double d0, double t0, double t1, double t)
+{
+    double mu, k, dv_i, dv_t, dvsq, duint, t2;
+    bool skip;
+    mu = d0 / (g0 + d0);
+    k = drag_k(d, g0, d0, t0, t1, skip);
+    t2 = skip ? 0 : k;
+    k = t2;
+    dv_i = t0;
+    dv_t = dv_i * exp(-t * k);
+    dvsq = dv_t * dv_t;
+    duint = -.5 * dv_i * dv_i * mu * expm1(-2 * k * t);
+    t0 = sqrt(dvsq);
+    t1 += duint;
+    k = drag_k(d, g0, d0, t0, t1, skip);
+    if (!skip) t2 += k;
+    if (ORDER == 3) {
+        t1 -= duint;
+        k = .25 * (t2);
+        dv_t = dv_i * exp(-t * k);
+        dvsq = dv_t * dv_t;
+        duint = -0.5 * dv_i * dv_i * mu * expm1(-2 * k * t);
+        t0 = sqrt(dvsq);
+        t1 += duint;
+        k = drag_k(d, g0, d0, t0, t1, skip);
+        t0 = skip ? 0 : k;
+        k = (0.16666666666666666667 * t2 + 0.66666666666666666667 * t0);
+    } else {
+        k = .5 * t2;
+    }
+    return k;
+}
+
+// Relative-velocity features of one cell: |dv| and the gas specific internal energy
+// (cukern_prepareForERK_h0, cudaSource2FluidDrag.cu:1883-1908).
+__device__ __forceinline__ void drag_features(double g0, double gE, double g2, double g3, double g4, double d0, double d2,
+                                              double d3, double d4, double &magdv, double &u)
+{
+    double dv, dvsq, press;
+    dv = (g2) / g0 - d2 / d0;
+    dvsq = dv * dv;
+    dv = (g3) / g0 - d3 / d0;
+    dvsq += dv * dv;
+    dv = (g4) / g0 - d4 / d0;
+    dvsq += dv * dv;
+    press = (gE - .5 * (g2 * g2 + g3 * g3 + g4 * g4) / g0);
+    magdv = sqrt(dvsq);
+    u = press / g0;
+}
+
+// Momentum exchange about the centre-of-mass velocity with dv -> dv exp(-t k), gas energy
+// absorbing the dust's kinetic-energy change (cudaSource2FluidDrag.cu:1660-1686).
+__device__ __forceinline__ void drag_apply(double *g, double *ds, int64_t S, double g0, double gE, double g2, double g3,
+                                           double g4, double d0, double d2, double d3, double d4, double t, double k)
+{
+    double mu, rhoginv, pdustsq, vstick, dv_i, dv_t, qq;
+    mu = d0 / (g0 + d0);
+    mu = mu * g0;
+    rhoginv = 1.0 / g0;
+
+    pdustsq = -d2 * d2;
+    vstick = (g2 + d2) / (g0 + d0);
+    dv_i = (g2) * rhoginv - d2 / d0;
+    dv_t = dv_i * exp(-t * k);
+    g[2 * S] = g0 * vstick + dv_t * mu;
+    ds[2 * S] = qq = d0 * vstick - dv_t * mu;
+    pdustsq += qq * qq;
+
+    pdustsq -= d3 * d3;
+    vstick = (g3 + d3) / (g0 + d0);
+    dv_i = (g3) * rhoginv - d3 / d0;
+    dv_t = dv_i * exp(-t * k);
+    g[3 * S] = g0 * vstick + dv_t * mu;
+    ds[3 * S] = qq = d0 * vstick - dv_t * mu;
+    pdustsq += qq * qq;
+
+    pdustsq -= d4 * d4;
+    vstick = (g4 + d4) / (g0 + d0);
+    dv_i = (g4) * rhoginv - d4 / d0;
+    dv_t = dv_i * exp(-t * k);
+    g[4 * S] = g0 * vstick + dv_t * mu;
+    ds[4 * S] = qq = d0 * vstick - dv_t * mu;
+    pdustsq += qq * qq;
+
+    g[S] = gE - .5 * pdustsq / d0;
+}
+
+// Drag constants dragparams[0..6] (cudaSource2FluidDrag.cu:196-218).
+inline DragParams drag_constants(const ib_thermo *tg, const ib_thermo *td)
+{
+    const double gam = tg->gamma;
+    const double ddust = sqrt(td->sigma0 / 3.141592653589793);
+    DragParams d;
+    d.visc0 = tg->mu0;
+    d.viscpow = -tg->mu_t_index;
+    d.lampow = tg->sigma_t_index;
+    d.alpha = tg->mass * (gam - 1.0) / (298.15 * tg->k_bolt);
+    d.beta = sqrt(2.0) * tg->mass / (tg->sigma0 * ddust);
+    d.delta = ddust / tg->mu0;
+    d.epsilon = td->sigma0 / (1.0 * td->mass);
+    return d;
+}
+
+}  // namespace ib

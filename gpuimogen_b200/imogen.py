@@ -82,6 +82,17 @@ class IbThermo(ctypes.Structure):
                 ("c_isothermal", ctypes.c_double)]
 
 
+class IbDragModel(ctypes.Structure):
+    _fields_ = [("params", ctypes.c_void_p), ("feature_shift", ctypes.c_float * 5),
+                ("feature_scale", ctypes.c_float * 5), ("out_shift", ctypes.c_float), ("out_scale", ctypes.c_float),
+                ("domain_lo", ctypes.c_float * 5), ("domain_hi", ctypes.c_float * 5)]
+
+
+# drag-decay MLP parameter layout (include/imogen_b200.h, IB_MLP_*)
+MLP_IN, MLP_HID, MLP_NPARAM = 16, 64, 9473
+MLP_OFF = {"W1": 0, "B1": 1024, "W2": 1088, "B2": 5184, "W3": 5248, "B3": 9344, "W4": 9408, "B4": 9472}
+
+
 class IbEnsemble(ctypes.Structure):
     _fields_ = [("q", ctypes.c_void_p), ("slab_pitch", ctypes.c_int64), ("offsets", ctypes.c_void_p),
                 ("h", ctypes.c_void_p), ("order", ctypes.c_void_p), ("t_out", ctypes.c_void_p),
@@ -114,6 +125,22 @@ EXPORTS = {
                                            ctypes.POINTER(ctypes.c_double), ctypes.c_void_p,
                                            ctypes.c_void_p]),
     "ib_device_wait_status": (ctypes.c_int, [ctypes.c_int]),
+    "ib_mlpWorkspaceFloats": (ctypes.c_int64, [ctypes.c_int64]),
+    "ib_mlpLossGrad": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "ib_mlpForward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                     ctypes.c_void_p]),
+    "ib_mlpInferTC": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                     ctypes.c_void_p]),
+    "ib_mlpAdam": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                  ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                  ctypes.c_void_p]),
+    "ib_dragDecayExact": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(IbThermo),
+                                         ctypes.POINTER(IbThermo), ctypes.c_void_p, ctypes.c_void_p]),
+    "ib_cudaSource2FluidDragLearned": (ctypes.c_int, [ctypes.POINTER(IbFluid), ctypes.POINTER(IbFluid),
+                                                      ctypes.POINTER(IbThermo), ctypes.POINTER(IbThermo),
+                                                      ctypes.POINTER(IbDragModel), ctypes.c_double, ctypes.c_void_p,
+                                                      ctypes.c_void_p]),
     "ib_riemannEnsemble": (ctypes.c_int, [ctypes.POINTER(IbEnsemble), ctypes.POINTER(IbFluidThermo), ctypes.c_int,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                                           ctypes.POINTER(IbNumerics), ctypes.POINTER(IbEnsembleTuning),

@@ -277,6 +277,74 @@ IB_API int ib_riemannEnsemble(const ib_ensemble *e, const ib_fluid_thermo *therm
                               double t_end, int32_t itermax, const ib_numerics *num,
                               const ib_ensemble_tuning *tuning, void *stream);
 
+/* ---------------------------------------------------------------------------------------------
+ * Learned drag (no reference counterpart: it stands in for the LogTrap2 integrator of
+ * cudaSource2FluidDrag.cu:709-795 and keeps that integrator as fallback and judge).
+ *
+ * The LogTrap2 update of a cell is fixed by one number, the decay exponent s = dt * k_eff of
+ * the gas-dust relative velocity (dv -> dv * exp(-s) about the centre-of-mass velocity, the gas
+ * absorbing the kinetic energy lost).  A small MLP predicts log s from five features:
+ *   x = ((log rho_gas, log rho_dust, log |dv|, log u, log dt) - feature_shift) * feature_scale,
+ *   u = specific internal energy of the gas (temperature), padded with zeros to 16 inputs;
+ *   3 hidden layers of 64 ReLU units, linear output y, log s = out_shift + out_scale * y.
+ * Parameters are one FP32 vector laid out as below (FP32 master copy for training; inference
+ * runs in BF16 on the tensor cores with FP32 accumulation).
+ * ------------------------------------------------------------------------------------------- */
+#define IB_MLP_IN 16
+#define IB_MLP_HID 64
+#define IB_MLP_OFF_W1 0       /* [64][16] */
+#define IB_MLP_OFF_B1 1024    /* [64] */
+#define IB_MLP_OFF_W2 1088    /* [64][64], row = output unit */
+#define IB_MLP_OFF_B2 5184
+#define IB_MLP_OFF_W3 5248
+#define IB_MLP_OFF_B3 9344
+#define IB_MLP_OFF_W4 9408    /* [64] */
+#define IB_MLP_OFF_B4 9472    /* [1] */
+#define IB_MLP_NPARAM 9473
+
+/* Training kernels (FP32).  x: n x 16 row-major features, target: n values of the normalised
+ * log s.  ib_mlpLossGrad computes the mean squared error over the n samples and its gradient
+ * with respect to every parameter (grad: IB_MLP_NPARAM floats; partial: device workspace of
+ * ib_mlpWorkspaceFloats(n) floats); loss_out (device, 1 float) may be NULL.  ib_mlpForward writes
+ * the n outputs y.  ib_mlpAdam takes one Adam step (m, v: moment buffers, step >= 1). */
+IB_API int64_t ib_mlpWorkspaceFloats(int64_t n);
+IB_API int ib_mlpLossGrad(const float *params, const float *x, const float *target, int64_t n, float *grad,
+                          float *loss_out, float *partial, void *stream);
+IB_API int ib_mlpForward(const float *params, const float *x, int64_t n, float *y, void *stream);
+IB_API int ib_mlpAdam(float *params, const float *grad, float *m, float *v, int64_t nparam, float lr, float beta1,
+                      float beta2, float eps, int step, void *stream);
+
+/* The same network on the tensor cores (tcgen05, BF16 weights and activations, FP32
+ * accumulation): y[i] for n rows of normalised features x (n x 16). */
+IB_API int ib_mlpInferTC(const float *params, const float *x, int64_t n, float *y, void *stream);
+
+/* Exact training targets: for n samples with features f = (rho_gas, rho_dust, |dv|, u, dt)
+ * (device, n x 5 doubles, the raw values) the LogTrap2 decay exponent s = dt * k_eff of
+ * cudaSource2FluidDrag.cu:1531-1686 with the drag constants of thermo_gas/thermo_dust; s = 0 where
+ * |dv| < 1e-9 (the reference's no-drag cut). */
+IB_API int ib_dragDecayExact(const double *features, int64_t n, const ib_thermo *thermo_gas,
+                             const ib_thermo *thermo_dust, double *s_out, void *stream);
+
+/* Model handed to the learned drag step: params (device, IB_MLP_NPARAM FP32; converted to BF16
+ * per call) and the normalisation. domain_lo/hi bound the five raw log-features the model was
+ * trained on; cells outside take the exact path. */
+typedef struct ib_drag_model {
+    const float *params;
+    float feature_shift[5], feature_scale[5];
+    float out_shift, out_scale;
+    float domain_lo[5], domain_hi[5];
+} ib_drag_model;
+
+/* Two-fluid drag over dt with the learned decay (same in-place update and argument meaning as
+ * ib_cudaSource2FluidDrag with method LogTrap2): per cell the MLP runs on the tensor cores
+ * (tcgen05, BF16 x BF16 -> FP32 in tensor memory) and the exact FP64 LogTrap2 takes over where
+ * the cell fails the check: features outside the trained domain, or a predicted decay that is
+ * not finite.  fallback_count (device, one unsigned long long, added to; may be NULL) counts
+ * those cells. */
+IB_API int ib_cudaSource2FluidDragLearned(ib_fluid *gas, ib_fluid *dust, const ib_thermo *thermo_gas,
+                                          const ib_thermo *thermo_dust, const ib_drag_model *model, double dt,
+                                          unsigned long long *fallback_count, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
