@@ -92,6 +92,8 @@ __device__ __forceinline__ void drag_apply(double *g, double *ds, int64_t S, dou
                                            double g4, double d0, double d2, double d3, double d4, double t, double k)
 {
     double mu, rhoginv, pdustsq, vstick, dv_i, dv_t, qq;
+    // the reference evaluates exp(-t k) once per axis with the same argument; once is the same value
+    const double decay = exp(-t * k);
     mu = d0 / (g0 + d0);
     mu = mu * g0;
     rhoginv = 1.0 / g0;
@@ -99,7 +101,7 @@ __device__ __forceinline__ void drag_apply(double *g, double *ds, int64_t S, dou
     pdustsq = -d2 * d2;
     vstick = (g2 + d2) / (g0 + d0);
     dv_i = (g2) * rhoginv - d2 / d0;
-    dv_t = dv_i * exp(-t * k);
+    dv_t = dv_i * decay;
     g[2 * S] = g0 * vstick + dv_t * mu;
     ds[2 * S] = qq = d0 * vstick - dv_t * mu;
     pdustsq += qq * qq;
@@ -107,7 +109,7 @@ __device__ __forceinline__ void drag_apply(double *g, double *ds, int64_t S, dou
     pdustsq -= d3 * d3;
     vstick = (g3 + d3) / (g0 + d0);
     dv_i = (g3) * rhoginv - d3 / d0;
-    dv_t = dv_i * exp(-t * k);
+    dv_t = dv_i * decay;
     g[3 * S] = g0 * vstick + dv_t * mu;
     ds[3 * S] = qq = d0 * vstick - dv_t * mu;
     pdustsq += qq * qq;
@@ -115,12 +117,105 @@ __device__ __forceinline__ void drag_apply(double *g, double *ds, int64_t S, dou
     pdustsq -= d4 * d4;
     vstick = (g4 + d4) / (g0 + d0);
     dv_i = (g4) * rhoginv - d4 / d0;
-    dv_t = dv_i * exp(-t * k);
+    dv_t = dv_i * decay;
     g[4 * S] = g0 * vstick + dv_t * mu;
     ds[4 * S] = qq = d0 * vstick - dv_t * mu;
     pdustsq += qq * qq;
 
     g[S] = gE - .5 * pdustsq / d0;
+}
+
+// cukern_GasDustDrag_GeneralAccel (cudaSource2FluidDrag.cu:898-931): -d|dv|/dt at |dv| = w; the
+// gas is credited with the relative kinetic energy dissipated since w0 unless INI.
+template <bool INI>
+__device__ __forceinline__ double drag_accel(const DragParams &d, double rhoA, double rhoB, double w0, double u0, double w)
+{
+    double u;
+    if (INI) u = u0;
+    else u = u0 + .5 * rhoB * (w0 * w0 - w * w) / (rhoA + rhoB);
+    const double Tn = d.alpha * u;
+    const double Re = d.delta * rhoA * w * pow(Tn, d.viscpow);
+    const double Kn = d.beta * pow(Tn, d.lampow) / rhoA;
+    const double Cd_hat = allregime_cdrag(Re, Kn);
+    return -(Cd_hat * w * w * (rhoA + rhoB) * d.epsilon);
+}
+
+// cukern_findInitialDeltaV (cudaSource2FluidDrag.cu:1014-1050): w0 = |dv|, u0 = e_int / rho_gas
+__device__ __forceinline__ void drag_initial_dv(const double *g, const double *ds, int64_t S, double &w0, double &u0)
+{
+    double u, q, dvsq, rhoginv, rhodinv, momsq;
+    rhoginv = 1 / g[0];
+    rhodinv = 1 / ds[0];
+    q = g[2 * S];
+    u = q * rhoginv - ds[2 * S] * rhodinv;
+    momsq = q * q;
+    dvsq = u * u;
+    q = g[3 * S];
+    u = q * rhoginv - ds[3 * S] * rhodinv;
+    momsq += q * q;
+    dvsq += u * u;
+    q = g[4 * S];
+    u = q * rhoginv - ds[4 * S] * rhodinv;
+    momsq += q * q;
+    dvsq += u * u;
+    w0 = sqrt(dvsq);
+    u0 = (g[S] - .5 * momsq * rhoginv) * rhoginv;
+}
+
+// cukern_applyFinalDeltaV (cudaSource2FluidDrag.cu:1160-1229)
+__device__ __forceinline__ void drag_apply_final_dv(double *g, double *ds, int64_t S, double wf)
+{
+    double vstick[3], dvhat[3], a, b, c, p1, p2, dustmom, dustmomfin;
+    const double rhog = g[0], rhod = ds[0];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        p1 = g[(2 + k) * S];
+        p2 = ds[(2 + k) * S];
+        vstick[k] = (p1 + p2) / (rhog + rhod);
+        dvhat[k] = p1 / rhog - p2 / rhod;
+    }
+    a = wf / sqrt(dvhat[0] * dvhat[0] + dvhat[1] * dvhat[1] + dvhat[2] * dvhat[2]);
+    dvhat[0] *= a;
+    dvhat[1] *= a;
+    dvhat[2] *= a;
+    b = rhog * rhod / (rhog + rhod);
+    dustmom = ds[2 * S] * ds[2 * S];
+    g[2 * S] = rhog * vstick[0] + dvhat[0] * b;
+    ds[2 * S] = c = rhod * vstick[0] - dvhat[0] * b;
+    dustmomfin = c * c;
+    dustmom += ds[3 * S] * ds[3 * S];
+    g[3 * S] = rhog * vstick[1] + dvhat[1] * b;
+    ds[3 * S] = c = rhod * vstick[1] - dvhat[1] * b;
+    dustmomfin += c * c;
+    dustmom += ds[4 * S] * ds[4 * S];
+    g[4 * S] = rhog * vstick[2] + dvhat[2] * b;
+    ds[4 * S] = c = rhod * vstick[2] - dvhat[2] * b;
+    dustmomfin += c * c;
+    g[S] += .5 * (dustmom - dustmomfin) / ds[0];
+    ds[S] = .5 * dustmomfin / ds[0] + 1e-4 * ds[0];
+}
+
+// cukern_ETDRK1 without the pressure-gradient term (cudaSource2FluidDrag.cu:1426-1510) with the
+// drag rate k at t = 0; k > 0.
+__device__ __forceinline__ void drag_apply_etdrk1(double *gas, double *dust, int64_t S, double t, double k)
+{
+    double rhoginv, mu, pdustsq, vstick, dv_i, dv_t, q, dpdt;
+    rhoginv = 1.0 / gas[0];
+    mu = gas[0] * dust[0] / (gas[0] + dust[0]);
+    pdustsq = 0;
+#pragma unroll
+    for (int ax = 2; ax <= 4; ax++) {
+        pdustsq -= dust[ax * S] * dust[ax * S];
+        vstick = (gas[ax * S] + dust[ax * S]) / (gas[0] + dust[0]);
+        dpdt = 0;
+        dv_i = (gas[ax * S]) * rhoginv - dust[ax * S] / dust[0];
+        dpdt *= mu * rhoginv;
+        dv_t = dpdt / k + (dv_i - dpdt / k) * exp(-t * k);
+        gas[ax * S] = gas[0] * vstick + dv_t * mu;
+        dust[ax * S] = q = dust[0] * vstick - dv_t * mu;
+        pdustsq += q * q;
+    }
+    gas[S] -= .5 * pdustsq / dust[0];
 }
 
 // Drag constants dragparams[0..6] (cudaSource2FluidDrag.cu:196-218).

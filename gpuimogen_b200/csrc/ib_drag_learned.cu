@@ -250,11 +250,15 @@ static int launch_mlp_tc(const LearnedArgs &a, cudaStream_t st)
     if (!attr) {
         if ((rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm))))
             return rc;
+        if ((rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100))))
+            return rc;
         attr = true;
     }
     int per_sm = 0;
     if ((rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, LT, shm)))) return rc;
-    per_sm = std::max(1, std::min(per_sm, 8));  // 8 x 64 tensor-memory columns = all 512
+    // 4 CTAs of 128 threads fit by registers and shared memory; 8 x 64 tensor-memory columns are
+    // all 512 of an SM.  CTAs never wait on each other, so a grid above residency only queues.
+    per_sm = std::max(4, std::min(per_sm, 8));
     const int64_t ntiles = (a.n + LT - 1) / LT;
     const unsigned grid = (unsigned)std::min<int64_t>(ntiles, (int64_t)per_sm * num_sms());
     kern<<<grid, LT, shm, st>>>(a);

@@ -1156,14 +1156,165 @@ void or_drag_logtrap_cells(double *gas, double *dust, int64_t n, int64_t slab,
     for (i = 0; i < n; i++) logtrap_cell(gas + i, dust + i, slab, dp, dt, order);
 }
 
+/* cukern_GasDustDrag_GeneralAccel (cudaSource2FluidDrag.cu:898-931): -d|dv|/dt at |dv| = w.
+ * ini = 1 uses the initial specific internal energy u0 as is (ONLY_DV_INI); otherwise the gas
+ * is credited with the relative kinetic energy dissipated since w0. */
+static double drag_accel(const double dp[11], double rhoA, double rhoB, double w0, double u0, double w, int ini)
+{
+    double u, Tn, Re, Kn, Cd_hat, accel;
+    if (ini) u = u0;
+    else u = u0 + .5 * rhoB * (w0 * w0 - w * w) / (rhoA + rhoB);
+    Tn = dp[3] * u;
+    Re = dp[5] * rhoA * w * pow(Tn, dp[1]);
+    Kn = dp[4] * pow(Tn, dp[2]) / rhoA;
+    Cd_hat = allregime_cdrag(Re, Kn);
+    accel = Cd_hat * w * w * (rhoA + rhoB) * dp[6];
+    return -accel;
+}
+
+/* cukern_findInitialDeltaV (cudaSource2FluidDrag.cu:1014-1050): w0 = |dv|, u0 = e_int / rho_gas */
+static void initial_dv(const double *g, const double *d, long S, double *w0, double *u0)
+{
+    double u, q, dvsq, rhoginv, rhodinv, momsq;
+    rhoginv = 1 / g[0];
+    rhodinv = 1 / d[0];
+    q = g[2 * S];
+    u = q * rhoginv - d[2 * S] * rhodinv;
+    momsq = q * q;
+    dvsq = u * u;
+    q = g[3 * S];
+    u = q * rhoginv - d[3 * S] * rhodinv;
+    momsq += q * q;
+    dvsq += u * u;
+    q = g[4 * S];
+    u = q * rhoginv - d[4 * S] * rhodinv;
+    momsq += q * q;
+    dvsq += u * u;
+    *w0 = sqrt(dvsq);
+    *u0 = (g[S] - .5 * momsq * rhoginv) * rhoginv;
+}
+
+/* cukern_applyFinalDeltaV (cudaSource2FluidDrag.cu:1160-1229): relative velocity rescaled to
+ * magnitude wf about the centre-of-mass velocity, gas energy credited with the dust's kinetic
+ * energy loss, dust energy reset to p^2/2rho + 1e-4 rho. */
+static void apply_final_dv(double *g, double *d, long S, double wf)
+{
+    double vstick[3], dvhat[3], rhog, rhod, a, b, c, p1, p2, dustmom, dustmomfin;
+    int k;
+    rhog = g[0];
+    rhod = d[0];
+    for (k = 0; k < 3; k++) {
+        p1 = g[(2 + k) * S];
+        p2 = d[(2 + k) * S];
+        vstick[k] = (p1 + p2) / (rhog + rhod);
+        dvhat[k] = p1 / rhog - p2 / rhod;
+    }
+    a = wf / sqrt(dvhat[0] * dvhat[0] + dvhat[1] * dvhat[1] + dvhat[2] * dvhat[2]);
+    dvhat[0] *= a;
+    dvhat[1] *= a;
+    dvhat[2] *= a;
+    b = rhog * rhod / (rhog + rhod);
+    dustmom = d[2 * S] * d[2 * S];
+    g[2 * S] = rhog * vstick[0] + dvhat[0] * b;
+    d[2 * S] = c = rhod * vstick[0] - dvhat[0] * b;
+    dustmomfin = c * c;
+    dustmom += d[3 * S] * d[3 * S];
+    g[3 * S] = rhog * vstick[1] + dvhat[1] * b;
+    d[3 * S] = c = rhod * vstick[1] - dvhat[1] * b;
+    dustmomfin += c * c;
+    dustmom += d[4 * S] * d[4 * S];
+    g[4 * S] = rhog * vstick[2] + dvhat[2] * b;
+    d[4 * S] = c = rhod * vstick[2] - dvhat[2] * b;
+    dustmomfin += c * c;
+    g[S] += .5 * (dustmom - dustmomfin) / d[0];
+    d[S] = .5 * dustmomfin / d[0] + 1e-4 * d[0];
+}
+
+/* solveDragEMP (cudaSource2FluidDrag.cu:305-370) and solveDragRK4 (:372-475) on one cell: the
+ * scalar ODE d|dv|/dt = -accel(|dv|) by the explicit midpoint or the classic RK4 tableau, stage
+ * by stage as the reference's kernels store them (tmp slab 0 = w0, 2 = accumulator, 3 = f,
+ * 4 = stage), then the final update.  Cells with |dv| < 1e-9 are left unchanged (the reference
+ * divides by |dv| there and writes NaN). */
+static void rk_cell(double *g, double *d, long S, const double dp[11], double dt, int rk4)
+{
+    double w0, u0, f, acc, stage, wf;
+    initial_dv(g, d, S, &w0, &u0);
+    if (w0 < 1e-9) return;
+    f = drag_accel(dp, g[0], d[0], w0, u0, w0, 1);
+    if (!rk4) {
+        stage = w0 + .5 * dt * f;
+        acc = 0 * f;
+        f = drag_accel(dp, g[0], d[0], w0, u0, stage, 0);
+        wf = w0 + dt * (acc + 1.0 * f);
+    } else {
+        stage = w0 + 0.5 * dt * f;
+        acc = 1.0 * f;
+        f = drag_accel(dp, g[0], d[0], w0, u0, stage, 0);
+        stage = w0 + 0.5 * dt * f;
+        acc += 2.0 * f;
+        f = drag_accel(dp, g[0], d[0], w0, u0, stage, 0);
+        stage = w0 + 1.0 * dt * f;
+        acc += 2.0 * f;
+        f = drag_accel(dp, g[0], d[0], w0, u0, stage, 0);
+        wf = w0 + (dt / 6.0) * (acc + 1.0 * f);
+    }
+    apply_final_dv(g, d, S, wf);
+}
+
+/* solveDragETDRK1 without the pressure-gradient term (cudaSource2FluidDrag.cu:477-560, kernel
+ * cukern_ETDRK1 :1426-1510): exponential Euler with the drag rate at t = 0.  Cells with
+ * |dv| < 1e-9 (k = 0) are left unchanged (the reference evaluates 0/0 there). */
+static void etdrk1_cell(double *gas, double *dust, long S, const double dp[11], double t)
+{
+    double dv, dvsq, press, t0, t1, k, rhoginv, mu, pdustsq, vstick, dv_i, dv_t, q, dpdt;
+    int skip, ax;
+    dv = (gas[2 * S]) / gas[0] - dust[2 * S] / dust[0];
+    dvsq = dv * dv;
+    dv = (gas[3 * S]) / gas[0] - dust[3 * S] / dust[0];
+    dvsq += dv * dv;
+    dv = (gas[4 * S]) / gas[0] - dust[4 * S] / dust[0];
+    dvsq += dv * dv;
+    press = (gas[S] - .5 * (gas[2 * S] * gas[2 * S] + gas[3 * S] * gas[3 * S] + gas[4 * S] * gas[4 * S]) / gas[0]);
+    t0 = sqrt(dvsq);
+    t1 = press / gas[0];
+    k = drag_k(dp, gas[0], dust[0], t0, t1, &skip);
+    if (skip) return;
+    rhoginv = 1.0 / gas[0];
+    mu = gas[0] * dust[0] / (gas[0] + dust[0]);
+    pdustsq = 0;
+    for (ax = 2; ax <= 4; ax++) {
+        pdustsq -= dust[ax * S] * dust[ax * S];
+        vstick = (gas[ax * S] + dust[ax * S]) / (gas[0] + dust[0]);
+        dpdt = 0;
+        dv_i = (gas[ax * S]) * rhoginv - dust[ax * S] / dust[0];
+        dpdt *= mu * rhoginv;
+        dv_t = dpdt / k + (dv_i - dpdt / k) * exp(-t * k);
+        gas[ax * S] = gas[0] * vstick + dv_t * mu;
+        dust[ax * S] = q = dust[0] * vstick - dv_t * mu;
+        pdustsq += q * q;
+    }
+    gas[S] -= .5 * pdustsq / dust[0];
+}
+
 int or_drag_2fluid(double *gas, double *dust, const or_grid *g, const double tg[8],
                    const double td[8], double dt, int method)
 {
     double dp[11];
     long N = (long)g->nx * g->ny * g->nz;
     or_drag_params(tg, td, dt, dp);
+    long i;
     if (method == 4 || method == 5) {
         or_drag_logtrap_cells(gas, dust, N, g->slab, dp, dt, method == 4 ? 2 : 3);
+        return OR_OK;
+    }
+    if (method == 0 || method == 1) {
+#pragma omp parallel for schedule(static)
+        for (i = 0; i < N; i++) rk_cell(gas + i, dust + i, g->slab, dp, dt, method == 1);
+        return OR_OK;
+    }
+    if (method == 2) {
+#pragma omp parallel for schedule(static)
+        for (i = 0; i < N; i++) etdrk1_cell(gas + i, dust + i, g->slab, dp, dt);
         return OR_OK;
     }
     return OR_ERR_NOIMPL;

@@ -148,7 +148,7 @@ def test_statics_fade(cuda, ib, po):
     assert np.array_equal(out[0, :n], ref[0, :n])
 
 
-@pytest.mark.parametrize("method", [4, 5])
+@pytest.mark.parametrize("method", [0, 1, 2, 4, 5])
 def test_drag_logtrap_matches_oracle(cuda, ib, po, method):
     shape = (64, 32, 1)
     n = 64 * 32
@@ -176,6 +176,18 @@ def test_drag_logtrap_matches_oracle(cuda, ib, po, method):
     ok, info = product_close(host(fd), d_ref, n, l1=1e-12, scale=1e-11)
     assert ok, info
     assert not np.array_equal(g_ref[2, :n], gas[2, :n])   # the drag did act
+
+
+def test_drag_etdrk2_not_implemented(cuda, ib):
+    shape = (16, 8, 1)
+    q = np.zeros((5, ib.slab_pitch(*shape)))
+    q[0] = 1.0
+    q[1] = 1.0
+    fg, fd = to_fluid(q, shape), to_fluid(q.copy(), shape)
+    tg = [5 / 3.0, 3.3e-27, 8.4e-6, 0.7, 2.4e-19, 0.2, 1.381e-23, -1]
+    td = [1.01, 3e-11, 0, 0, math.pi * 25e-12, 0, 1.381e-23, 0.1]
+    with pytest.raises(ib.ImogenError):
+        ib.cudaSource2FluidDrag(fg, fd, tg, td, ib.Geometry(shape), [0.05, 3])
 
 
 def test_sod_gpu_matches_oracle_and_exact(cuda, ib, po):
