@@ -18,14 +18,18 @@ namespace ib {
 
 constexpr int LT = 128;  // cells per tile, threads per CTA, MMA M
 constexpr int NH = IB_MLP_HID;
+constexpr int KH = NH + 16;  // hidden-layer K: 64 activations + a 16-column block holding the bias
 
+// Shared memory of one CTA.  Biases ride inside the MMAs: input columns 14 and 15 of A0, and
+// columns 64 and 65 of A1, hold the constant 1, and the matching weight columns hold the bias
+// split into a BF16 high part and a BF16 remainder (about 16 significant bits together).
 struct LearnedSmem {
     alignas(128) unsigned char W1[NH * 16 * 2];
-    alignas(128) unsigned char W2[NH * NH * 2];
-    alignas(128) unsigned char W3[NH * NH * 2];
+    alignas(128) unsigned char W2[NH * KH * 2];
+    alignas(128) unsigned char W3[NH * KH * 2];
     alignas(128) unsigned char A0[LT * 16 * 2];
-    alignas(128) unsigned char A1[LT * NH * 2];
-    float b1[NH], b2[NH], b3[NH], w4[NH];
+    alignas(128) unsigned char A1[LT * KH * 2];
+    float w4[NH];
     float b4;
     uint32_t tmem;
     alignas(8) uint64_t bar;
@@ -34,7 +38,7 @@ struct LearnedSmem {
 struct LearnedArgs {
     const float *params;
     float fshift[5], fscale[5], oshift, oscale, lo[5], hi[5];
-    const float *xin;  // mode 0: n x 16 features
+    const float *xin;  // mode 0: n x 16 features (columns 14 and 15 are ignored)
     float *yout;       // mode 0: n outputs
     double *gas, *dust;
     int64_t S;
@@ -45,37 +49,71 @@ struct LearnedArgs {
     unsigned int *err;
 };
 
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi)
+{
+    __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t *>(&h);
+}
+
+// relu(lo), relu(hi) -> BF16x2 in one conversion (lo in the low half)
+__device__ __forceinline__ uint32_t relu_bf16x2(float lo, float hi)
+{
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+
 __device__ __forceinline__ void store_bf16x8(unsigned char *dst, const float *v)
 {
     uint4 u;
-    __nv_bfloat162 h0 = __floats2bfloat162_rn(v[0], v[1]), h1 = __floats2bfloat162_rn(v[2], v[3]);
-    __nv_bfloat162 h2 = __floats2bfloat162_rn(v[4], v[5]), h3 = __floats2bfloat162_rn(v[6], v[7]);
-    u.x = *reinterpret_cast<uint32_t *>(&h0);
-    u.y = *reinterpret_cast<uint32_t *>(&h1);
-    u.z = *reinterpret_cast<uint32_t *>(&h2);
-    u.w = *reinterpret_cast<uint32_t *>(&h3);
+    u.x = pack_bf16x2(v[0], v[1]);
+    u.y = pack_bf16x2(v[2], v[3]);
+    u.z = pack_bf16x2(v[4], v[5]);
+    u.w = pack_bf16x2(v[6], v[7]);
     *reinterpret_cast<uint4 *>(dst) = u;
 }
 
-// bias + ReLU of this thread's 64 accumulators -> BF16 row r of A1 (K = 64)
-__device__ __forceinline__ void hidden_to_a1(unsigned char *A1, int r, float *h, const float *b)
+__device__ __forceinline__ void put_bf16(unsigned char *base, uint32_t off, float v)
 {
-#pragma unroll
-    for (int g = 0; g < 8; g++) {
-        float v[8];
-#pragma unroll
-        for (int e = 0; e < 8; e++) v[e] = fmaxf(h[8 * g + e] + b[8 * g + e], 0.f);
-        store_bf16x8(A1 + core_offset(r, 8 * g, NH), v);
+    *reinterpret_cast<__nv_bfloat16 *>(base + off) = __float2bfloat16_rn(v);
+}
+
+// Weight matrix [64 out][K] -> BF16 core-matrix layout, bias split into columns bcol, bcol + 1
+__device__ void load_weights(unsigned char *W, const float *src, int kin, int K, int bcol, const float *bias)
+{
+    for (int i = threadIdx.x; i < NH * K; i += blockDim.x) {
+        const int j = i / K, k = i % K;
+        float v = 0.f;
+        if (k < kin) v = src[j * kin + k];
+        if (k == bcol || k == bcol + 1) {
+            const float b = bias[j];
+            const float hi = __bfloat162float(__float2bfloat16_rn(b));
+            v = (k == bcol) ? hi : b - hi;
+        }
+        put_bf16(W, core_offset(j, k, K), v);
     }
 }
 
-__device__ __forceinline__ void tmem_row64(uint32_t taddr, float *h)
+// this thread's accumulator row (16 columns at a time) -> ReLU -> BF16 row r of A1
+__device__ __forceinline__ void hidden_to_a1(unsigned char *A1, int r, uint32_t taddr)
 {
-    tmem_ld16(taddr, h);
-    tmem_ld16(taddr + 16, h + 16);
-    tmem_ld16(taddr + 32, h + 32);
-    tmem_ld16(taddr + 48, h + 48);
-    tmem_wait_ld();
+#pragma unroll
+    for (int c = 0; c < NH; c += 16) {
+        float h[16];
+        tmem_ld16(taddr + c, h);
+        tmem_wait_ld();
+        uint4 u0, u1;
+        u0.x = relu_bf16x2(h[0], h[1]);
+        u0.y = relu_bf16x2(h[2], h[3]);
+        u0.z = relu_bf16x2(h[4], h[5]);
+        u0.w = relu_bf16x2(h[6], h[7]);
+        u1.x = relu_bf16x2(h[8], h[9]);
+        u1.y = relu_bf16x2(h[10], h[11]);
+        u1.z = relu_bf16x2(h[12], h[13]);
+        u1.w = relu_bf16x2(h[14], h[15]);
+        *reinterpret_cast<uint4 *>(A1 + core_offset(r, c, KH)) = u0;
+        *reinterpret_cast<uint4 *>(A1 + core_offset(r, c + 8, KH)) = u1;
+    }
 }
 
 // All threads: make this thread's shared-memory writes visible to the tensor cores and order its
@@ -89,6 +127,27 @@ __device__ __forceinline__ bool tc_sync(bool ok)
     return ok;
 }
 
+// Learned-path update: the exact integrator's momentum exchange and gas heating (drag_apply) with
+// decay factor exp(-s), written with one reciprocal per density instead of per-axis divisions.
+__device__ __forceinline__ void drag_apply_learned(double *g, double *ds, int64_t S, double g0, double gE,
+                                                   const double gm[3], double d0, const double dm[3],
+                                                   const double dvv[3], double rdi, double decay)
+{
+    const double rsum = 1.0 / (g0 + d0);
+    const double mu = g0 * d0 * rsum;
+    double pd = 0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const double vstick = (gm[k] + dm[k]) * rsum;
+        const double dvt = dvv[k] * decay;
+        const double q = d0 * vstick - dvt * mu;
+        g[(2 + k) * S] = g0 * vstick + dvt * mu;
+        ds[(2 + k) * S] = q;
+        pd += q * q - dm[k] * dm[k];
+    }
+    g[S] = gE - .5 * pd * rdi;
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(LT, 4) mlp_tc_kernel(LearnedArgs a)
 {
@@ -96,20 +155,14 @@ __global__ void __launch_bounds__(LT, 4) mlp_tc_kernel(LearnedArgs a)
     LearnedSmem &s = *reinterpret_cast<LearnedSmem *>(learned_smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5;
     const float *p = a.params;
-    for (int i = tid; i < NH * 16; i += LT) {
-        const int j = i / 16, k = i % 16;
-        *reinterpret_cast<__nv_bfloat16 *>(s.W1 + core_offset(j, k, 16)) = __float2bfloat16_rn(p[IB_MLP_OFF_W1 + i]);
-    }
-    for (int i = tid; i < NH * NH; i += LT) {
-        const int j = i / NH, k = i % NH;
-        *reinterpret_cast<__nv_bfloat16 *>(s.W2 + core_offset(j, k, NH)) = __float2bfloat16_rn(p[IB_MLP_OFF_W2 + i]);
-        *reinterpret_cast<__nv_bfloat16 *>(s.W3 + core_offset(j, k, NH)) = __float2bfloat16_rn(p[IB_MLP_OFF_W3 + i]);
-    }
-    for (int i = tid; i < NH; i += LT) {
-        s.b1[i] = p[IB_MLP_OFF_B1 + i];
-        s.b2[i] = p[IB_MLP_OFF_B2 + i];
-        s.b3[i] = p[IB_MLP_OFF_B3 + i];
-        s.w4[i] = p[IB_MLP_OFF_W4 + i];
+    load_weights(s.W1, p + IB_MLP_OFF_W1, 16, 16, 14, p + IB_MLP_OFF_B1);
+    load_weights(s.W2, p + IB_MLP_OFF_W2, NH, KH, NH, p + IB_MLP_OFF_B2);
+    load_weights(s.W3, p + IB_MLP_OFF_W3, NH, KH, NH, p + IB_MLP_OFF_B3);
+    for (int i = tid; i < NH; i += LT) s.w4[i] = p[IB_MLP_OFF_W4 + i];
+    {   // constant columns of A1: [1, 1, 0 x 14] after the 64 activations
+        const float one8[8] = {1.f, 1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, zero8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        store_bf16x8(s.A1 + core_offset(tid, NH, KH), one8);
+        store_bf16x8(s.A1 + core_offset(tid, NH + 8, KH), zero8);
     }
     if (tid == 0) {
         s.b4 = p[IB_MLP_OFF_B4];
@@ -121,28 +174,40 @@ __global__ void __launch_bounds__(LT, 4) mlp_tc_kernel(LearnedArgs a)
     const uint32_t tmem = s.tmem;
     const uint32_t my_row = tmem + ((uint32_t)(warp * 32) << 16);
     const uint32_t id = idesc_bf16_f32(LT, NH);
+    const uint64_t dA0 = smem_desc(s.A0, 128, 256), dW1 = smem_desc(s.W1, 128, 256);
     uint32_t phase = 0;
     bool ok = true;
     const int64_t ntiles = (a.n + LT - 1) / LT;
-    float h[NH];
 
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int64_t i = tile * LT + tid;
         const bool live = i < a.n;
-        // ---- features ----
+        // ---- features: columns 0..13 (drag: 0..4), 14 and 15 = 1 for the bias ----
         float f[16];
 #pragma unroll
         for (int k = 0; k < 16; k++) f[k] = 0.f;
         bool indom = live;
-        double g0 = 1, gE = 0, g2 = 0, g3 = 0, g4 = 0, d0 = 1, d2 = 0, d3 = 0, d4 = 0, magdv = 0, u = 0;
+        double g0 = 1, gE = 0, d0 = 1, gm[3] = {0, 0, 0}, dm[3] = {0, 0, 0}, dvv[3] = {0, 0, 0}, rdi = 1, magdv = 0;
         if (MODE == 0) {
             if (live)
-                for (int k = 0; k < IB_MLP_IN; k++) f[k] = a.xin[i * IB_MLP_IN + k];
+                for (int k = 0; k < 14; k++) f[k] = a.xin[i * IB_MLP_IN + k];
         } else if (live) {
-            double *g = a.gas + i, *ds = a.dust + i;
-            g0 = g[0]; gE = g[a.S]; g2 = g[2 * a.S]; g3 = g[3 * a.S]; g4 = g[4 * a.S];
-            d0 = ds[0]; d2 = ds[2 * a.S]; d3 = ds[3 * a.S]; d4 = ds[4 * a.S];
-            drag_features(g0, gE, g2, g3, g4, d0, d2, d3, d4, magdv, u);
+            const double *g = a.gas + i, *ds = a.dust + i;
+            g0 = g[0]; gE = g[a.S];
+            d0 = ds[0];
+#pragma unroll
+            for (int k = 0; k < 3; k++) { gm[k] = g[(2 + k) * a.S]; dm[k] = ds[(2 + k) * a.S]; }
+            const double rgi = 1.0 / g0;
+            rdi = 1.0 / d0;
+            double dvsq = 0, momsq = 0;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                dvv[k] = gm[k] * rgi - dm[k] * rdi;
+                dvsq += dvv[k] * dvv[k];
+                momsq += gm[k] * gm[k];
+            }
+            magdv = sqrt(dvsq);
+            const double u = (gE - .5 * momsq * rgi) * rgi;
             const float raw[5] = {logf((float)g0), logf((float)d0), logf((float)magdv), logf((float)u),
                                   logf((float)a.dt)};
 #pragma unroll
@@ -155,69 +220,84 @@ __global__ void __launch_bounds__(LT, 4) mlp_tc_kernel(LearnedArgs a)
                 for (int k = 0; k < 5; k++) f[k] = 0.f;
             }
         }
+        f[14] = 1.f;
+        f[15] = 1.f;
         store_bf16x8(s.A0 + core_offset(tid, 0, 16), f);
         store_bf16x8(s.A0 + core_offset(tid, 8, 16), f + 8);
         ok = tc_sync(ok);
         if (!ok) break;
-        // ---- layer 1: [128 x 16] x [16 -> 64] ----
+        // ---- layer 1: [128 x 16] x [16 -> 64], bias in columns 14-15 ----
         if (tid == 0) {
-            tc_mma_bf16(tmem, smem_desc(s.A0, 128, 256), smem_desc(s.W1, 128, 256), id, 0);
+            tc_mma_bf16(tmem, dA0, dW1, id, 0);
             tc_commit(&s.bar);
         }
         ok = mbar_wait(&s.bar, phase);
         phase ^= 1;
         tc_fence_after();
-        tmem_row64(my_row, h);
-        hidden_to_a1(s.A1, tid, h, s.b1);
+        hidden_to_a1(s.A1, tid, my_row);
         ok = tc_sync(ok);
         if (!ok) break;
-        // ---- layers 2 and 3: [128 x 64] x [64 -> 64] as 4 MMAs of K = 16 ----
+        // ---- layers 2 and 3: [128 x 80] x [80 -> 64] as 5 MMAs of K = 16 ----
         for (int layer = 0; layer < 2; layer++) {
             const unsigned char *W = layer ? s.W3 : s.W2;
             if (tid == 0) {
 #pragma unroll
-                for (int kk = 0; kk < 4; kk++)
-                    tc_mma_bf16(tmem, smem_desc(s.A1 + kk * 256, 128, 1024), smem_desc(W + kk * 256, 128, 1024), id,
-                                kk > 0);
+                for (int kk = 0; kk < KH / 16; kk++)
+                    tc_mma_bf16(tmem, smem_desc(s.A1 + kk * 256, 128, KH * 16), smem_desc(W + kk * 256, 128, KH * 16),
+                                id, kk > 0);
                 tc_commit(&s.bar);
             }
             ok = mbar_wait(&s.bar, phase);
             phase ^= 1;
             tc_fence_after();
-            tmem_row64(my_row, h);
-            if (layer == 0) hidden_to_a1(s.A1, tid, h, s.b2);
-            ok = tc_sync(ok);
-            if (!ok) break;
+            if (layer == 0) {
+                hidden_to_a1(s.A1, tid, my_row);
+                ok = tc_sync(ok);
+                if (!ok) break;
+            }
         }
         if (!ok) break;
-        // ---- output: y = b4 + w4 . relu(h + b3) ----
+        // ---- output: y = b4 + w4 . relu(h3) (FP32, straight from tensor memory) ----
         float y = s.b4;
 #pragma unroll
-        for (int j = 0; j < NH; j++) y = fmaf(s.w4[j], fmaxf(h[j] + s.b3[j], 0.f), y);
+        for (int c = 0; c < NH; c += 16) {
+            float h[16];
+            tmem_ld16(my_row + c, h);
+            tmem_wait_ld();
+#pragma unroll
+            for (int j = 0; j < 16; j++) y = fmaf(s.w4[c + j], fmaxf(h[j], 0.f), y);
+        }
         if (MODE == 0) {
             if (live) a.yout[i] = y;
         } else {
-            double k_use = 0.0, t_use = 1.0;
             bool fb = false;
             if (live) {
+                double decay = 1.0;
                 if (magdv < 1e-9) {
-                    k_use = 0.0;  // the exact integrator's no-drag cut
+                    fb = true;  // the exact integrator's no-drag cut: let it handle the cell
                 } else if (indom) {
                     const float sp = expf(a.oshift + a.oscale * y);
-                    if (isfinite(sp)) k_use = (double)sp;
+                    if (isfinite(sp)) decay = exp(-(double)sp);
                     else fb = true;
                 } else {
                     fb = true;
                 }
+                double *g = a.gas + i, *ds = a.dust + i;
                 if (fb) {
-                    k_use = logtrap_keff<2>(a.d, g0, d0, magdv, u, a.dt);
-                    t_use = a.dt;
+                    const double g2 = gm[0], g3 = gm[1], g4 = gm[2], d2 = dm[0], d3 = dm[1], d4 = dm[2];
+                    double t0, t1;
+                    drag_features(g0, gE, g2, g3, g4, d0, d2, d3, d4, t0, t1);
+                    const double k = logtrap_keff<2>(a.d, g0, d0, t0, t1, a.dt);
+                    drag_apply(g, ds, a.S, g0, gE, g2, g3, g4, d0, d2, d3, d4, a.dt, k);
+                } else {
+                    drag_apply_learned(g, ds, a.S, g0, gE, gm, d0, dm, dvv, rdi, decay);
                 }
-                drag_apply(a.gas + i, a.dust + i, a.S, g0, gE, g2, g3, g4, d0, d2, d3, d4, t_use, k_use);
             }
-            const unsigned m = __ballot_sync(0xffffffffu, fb);
+            const unsigned m = __ballot_sync(0xffffffffu, fb && magdv >= 1e-9);
             if ((tid & 31) == 0 && m && a.fallbacks) atomicAdd(a.fallbacks, (unsigned long long)__popc(m));
         }
+        // every thread's tensor-memory reads are done before the next tile's MMAs overwrite them
+        tc_fence_before();
     }
     if (!ok && tid == 0) {
         atomicOr(a.err, 2u);

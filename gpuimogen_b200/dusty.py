@@ -94,18 +94,23 @@ def time_run(run, steps, warm=2):
     return a.elapsed_time(b), tm
 
 
-def time_drag(run, reps=20):
+def time_drag(run, reps=10):
+    """Mean time of one drag call on the initial state (each call on a fresh copy of it; only the
+    calls are inside the CUDA-event intervals)."""
     dt = 4e-5
     fl = [run.gas, run.dust]
-    run.drag(fl, dt)
-    torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record()
-    for _ in range(reps):
+    total = 0.0
+    for r in range(reps + 1):
+        run.reset()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
         run.drag(fl, dt)
-    b.record()
-    torch.cuda.synchronize()
-    return a.elapsed_time(b) / reps
+        b.record()
+        torch.cuda.synchronize()
+        if r:
+            total += a.elapsed_time(b)
+    run.reset()
+    return total / reps
 
 
 def study(n=2048, steps=500, samples=10_000_000, epochs=10, seed=5, verbose=False):

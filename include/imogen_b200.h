@@ -285,7 +285,9 @@ IB_API int ib_riemannEnsemble(const ib_ensemble *e, const ib_fluid_thermo *therm
  * the gas-dust relative velocity (dv -> dv * exp(-s) about the centre-of-mass velocity, the gas
  * absorbing the kinetic energy lost).  A small MLP predicts log s from five features:
  *   x = ((log rho_gas, log rho_dust, log |dv|, log u, log dt) - feature_shift) * feature_scale,
- *   u = specific internal energy of the gas (temperature), padded with zeros to 16 inputs;
+ *   u = specific internal energy of the gas (temperature), padded with zeros to 16 inputs
+ *   (inputs 14 and 15 are reserved: the tensor-core inference feeds the first-layer bias
+ *   through them, so they must stay zero in training data);
  *   3 hidden layers of 64 ReLU units, linear output y, log s = out_shift + out_scale * y.
  * Parameters are one FP32 vector laid out as below (FP32 master copy for training; inference
  * runs in BF16 on the tensor cores with FP32 accumulation).
@@ -315,7 +317,8 @@ IB_API int ib_mlpAdam(float *params, const float *grad, float *m, float *v, int6
                       float beta2, float eps, int step, void *stream);
 
 /* The same network on the tensor cores (tcgen05, BF16 weights and activations, FP32
- * accumulation): y[i] for n rows of normalised features x (n x 16). */
+ * accumulation, biases as BF16 high + low parts): y[i] for n rows of normalised features
+ * x (n x 16; columns 14 and 15 are ignored). */
 IB_API int ib_mlpInferTC(const float *params, const float *x, int64_t n, float *y, void *stream);
 
 /* Exact training targets: for n samples with features f = (rho_gas, rho_dust, |dv|, u, dt)

@@ -19,7 +19,9 @@ def random_params(seed):
     for a, b in (("B1", "W2"), ("B2", "W3"), ("B3", "W4")):
         p[ib.imogen.MLP_OFF[a]:ib.imogen.MLP_OFF[b]] = 0.1 * torch.randn(64, generator=g)
     p[ib.imogen.MLP_OFF["B4"]] = 0.3
-    p[ib.imogen.MLP_OFF["W1"]:ib.imogen.MLP_OFF["B1"]] = 0.5 * torch.randn(1024, generator=g)  # all 16 inputs live
+    w1 = 0.5 * torch.randn(64, 16, generator=g)
+    w1[:, 14:] = 0  # inputs 14 and 15 are reserved for the bias on the tensor cores
+    p[ib.imogen.MLP_OFF["W1"]:ib.imogen.MLP_OFF["B1"]] = w1.reshape(-1)  # inputs 0..13 live
     return p.cuda()
 
 
@@ -50,7 +52,9 @@ def test_tensor_core_inference_matches_bf16_emulation(cuda, ib):
     emulation of that arithmetic and against the FP32 network."""
     p = random_params(11)
     n = 1000  # not a multiple of the 128-cell tile
-    x = torch.randn(n, 16, generator=torch.Generator().manual_seed(13)).cuda()
+    x = torch.randn(n, 16, generator=torch.Generator().manual_seed(13))
+    x[:, 14:] = 0
+    x = x.cuda()
     y = ld.forward_tc(p, x).cpu().numpy().astype(np.float64)
     y_bf = mo.forward_bf16(p.cpu().numpy(), x.cpu().numpy())
     y32, _ = mo.forward(p.cpu().numpy(), x.cpu().numpy())
