@@ -58,8 +58,14 @@ def _newest_input():
     return max(os.path.getmtime(p) for p in paths)
 
 
+# Files whose single-precision arithmetic is only the FP32-flux form: FP32 division and square
+# root there use the hardware approximations (FP64 arithmetic is unaffected by these flags).
+FP32_FAST = ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
+PER_FILE = {"ib_sweep_hllc32.cu": FP32_FAST, "ib_ensemble.cu": FP32_FAST}
+
+
 def _compile(src, obj, extra):
-    cmd = [NVCC] + BASE_FLAGS + extra + ["-c", os.path.join(CSRC, src), "-o", obj]
+    cmd = [NVCC] + BASE_FLAGS + extra + PER_FILE.get(src, []) + ["-c", os.path.join(CSRC, src), "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("nvcc failed for %s:\n%s\n%s" % (src, " ".join(cmd), r.stderr))
