@@ -333,6 +333,8 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
 struct PipeArgs {
     int n;              // pencil length
     int npw;            // pencil blocks per line of x (nx / W; 1 for x sweeps)
+    int bh;             // rows per TMA box along the pencil (n, or n / 2 for pencils above 256)
+    int nh;             // boxes per pencil and slab (1 or 2)
     int64_t nblocks;    // pencil blocks in the grid
     double lambda;
     unsigned int *err;  // set to 1 when a TMA wait ran out
@@ -343,22 +345,27 @@ __host__ __device__ __forceinline__ size_t pipe_tile_bytes(int n, int W)
     return ((size_t)40 * n * W + 127) / 128 * 128;
 }
 
+// The tile of block b is one TMA box.  x sweeps: rank 3 (x, row, slab), box (n, 1, 5).  y/z sweeps:
+// rank 5 (x, row within half, half, other axis, slab), box (W, bh, nh, 1, 5), so pencils of up to
+// 512 cells arrive in one copy laid out [slab][cell][column].
 template <int DIR>
-__device__ __forceinline__ void pipe_load(void *dst, const CUtensorMap *tm, int64_t b, int npw, int W, uint64_t *bar)
+__device__ __forceinline__ void pipe_load(double *dst, const CUtensorMap *tm, int64_t b, const PipeArgs &a, int W,
+                                          uint64_t *bar)
 {
     if (DIR == 1) tma_load_3d(dst, tm, 0, (int)b, 0, bar);
-    else tma_load_4d(dst, tm, (int)(b % npw) * W, 0, (int)(b / npw), 0, bar);
+    else tma_load_5d(dst, tm, (int)(b % a.npw) * W, 0, 0, (int)(b / a.npw), 0, bar);
 }
 
 template <int DIR>
-__device__ __forceinline__ void pipe_store(const CUtensorMap *tm, const void *src, int64_t b, int npw, int W)
+__device__ __forceinline__ void pipe_store(const CUtensorMap *tm, const double *src, int64_t b, const PipeArgs &a,
+                                           int W)
 {
     if (DIR == 1) tma_store_3d(tm, src, 0, (int)b, 0);
-    else tma_store_4d(tm, src, (int)(b % npw) * W, 0, (int)(b / npw), 0);
+    else tma_store_5d(tm, src, (int)(b % a.npw) * W, 0, 0, (int)(b / a.npw), 0);
 }
 
-template <int METHOD, int SLOPE, typename FT, int DIR, int W>
-__global__ void __launch_bounds__(512, 2)
+template <int METHOD, int SLOPE, typename FT, int DIR, int W, int CPT>
+__global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
     sweep_pipe_kernel(const __grid_constant__ CUtensorMap tm, PipeArgs a, FluidConsts<FT> c)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -375,9 +382,16 @@ __global__ void __launch_bounds__(512, 2)
                   s3 = slot_of<METHOD, DIR>(3), s4 = slot_of<METHOD, DIR>(4);
     const int slots[5] = {s0, s1, s2, s3, s4};
     const int col = (W == 1) ? 0 : (int)(threadIdx.x % W);
-    const int i = (int)(threadIdx.x / W);
-    const bool act = i < n;
-    const int il = (i == 0) ? n - 1 : i - 1, ir = (i == n - 1) ? 0 : i + 1;
+    const int rows_per_pass = blockDim.x / W;
+    int ci[CPT], il[CPT], ir[CPT];
+    bool act[CPT];
+#pragma unroll
+    for (int m = 0; m < CPT; m++) {
+        ci[m] = (int)(threadIdx.x / W) + m * rows_per_pass;
+        act[m] = ci[m] < n;
+        il[m] = (ci[m] == 0) ? n - 1 : ci[m] - 1;
+        ir[m] = (ci[m] == n - 1) ? 0 : ci[m] + 1;
+    }
     auto SI = [&](int k, int j) { return (k * n + j) * W + col; };
     const double lambda = a.lambda;
     const int64_t step = gridDim.x;
@@ -390,18 +404,17 @@ __global__ void __launch_bounds__(512, 2)
         fence_mbar_init();
     }
     __syncthreads();
-    // issued0/1: a load into tile 0/1 is in flight (leader's bookkeeping, for draining)
-    bool issued0 = false, issued1 = false;
+    bool issued0 = false, issued1 = false;  // leader's bookkeeping of loads in flight
     if (leader) {
         const int64_t b0 = blockIdx.x, b1 = blockIdx.x + step;
         if (b0 < a.nblocks) {
             mbar_arrive_expect_tx(&full[0], tile_tx);
-            pipe_load<DIR>(U[0], &tm, b0, a.npw, W, &full[0]);
+            pipe_load<DIR>(U[0], &tm, b0, a, W, &full[0]);
             issued0 = true;
         }
         if (b1 < a.nblocks) {
             mbar_arrive_expect_tx(&full[1], tile_tx);
-            pipe_load<DIR>(U[1], &tm, b1, a.npw, W, &full[1]);
+            pipe_load<DIR>(U[1], &tm, b1, a, W, &full[1]);
             issued1 = true;
         }
     }
@@ -413,9 +426,11 @@ __global__ void __launch_bounds__(512, 2)
         const uint32_t par = t ? phase1 : phase0;
         const bool ok = mbar_wait(&full[t], par);
         if (t) phase1 ^= 1; else phase0 ^= 1;
-        double u0[5], u1[5];
+        double u0[CPT][5], u1[CPT][5];
 #pragma unroll
-        for (int k = 0; k < 5; k++) u0[k] = act ? Ut[SI(slots[k], i)] : 1.0;
+        for (int m = 0; m < CPT; m++)
+#pragma unroll
+            for (int k = 0; k < 5; k++) u0[m][k] = act[m] ? Ut[SI(slots[k], ci[m])] : 1.0;
         if (!__syncthreads_and(ok)) {
             // a tile never arrived: report, drain what is still in flight, leave
             if (leader) {
@@ -433,49 +448,61 @@ __global__ void __launch_bounds__(512, 2)
             if (bn < a.nblocks) {
                 fence_proxy_async_smem();
                 mbar_arrive_expect_tx(&full[t], tile_tx);
-                pipe_load<DIR>(Ut, &tm, bn, a.npw, W, &full[t]);
+                pipe_load<DIR>(Ut, &tm, bn, a, W, &full[t]);
             } else {
                 if (t == 0) issued0 = false; else issued1 = false;
             }
         }
-        V5<FT> keep;
+        V5<FT> keep[CPT];
 #pragma unroll
         for (int stage = 0; stage < 2; stage++) {
-            double *u = (stage == 0) ? u0 : u1;
-            if (act) {
-                V5<FT> w = stage_prims<METHOD, DIR, FT>(u, c);
+            double (*u)[5] = (stage == 0) ? u0 : u1;
 #pragma unroll
-                for (int k = 0; k < 5; k++) SA[SI(k, i)] = w.a[k];
-            }
-            __syncthreads();
-            if (act) {
-                V5<FT> w, dl, dr, L;
+            for (int m = 0; m < CPT; m++) {
+                if (act[m]) {
+                    V5<FT> w = stage_prims<METHOD, DIR, FT>(u[m], c);
 #pragma unroll
-                for (int k = 0; k < 5; k++) {
-                    w.a[k] = SA[SI(k, i)];
-                    dl.a[k] = w.a[k] - SA[SI(k, il)];
-                    dr.a[k] = SA[SI(k, ir)] - w.a[k];
+                    for (int k = 0; k < 5; k++) SA[SI(k, ci[m])] = w.a[k];
                 }
-                stage_faces<METHOD, SLOPE, FT>(c, w, dl, dr, L, keep);
-#pragma unroll
-                for (int k = 0; k < 5; k++) SB[SI(k, i)] = L.a[k];
             }
             __syncthreads();
-            if (act) {
-                V5<FT> Lr;
 #pragma unroll
-                for (int k = 0; k < 5; k++) Lr.a[k] = SB[SI(k, ir)];
-                keep = stage_flux<METHOD, FT>(c, keep, Lr);
+            for (int m = 0; m < CPT; m++) {
+                if (act[m]) {
+                    V5<FT> w, dl, dr, L;
 #pragma unroll
-                for (int k = 0; k < 5; k++) SA[SI(k, i)] = keep.a[k];
+                    for (int k = 0; k < 5; k++) {
+                        w.a[k] = SA[SI(k, ci[m])];
+                        dl.a[k] = w.a[k] - SA[SI(k, il[m])];
+                        dr.a[k] = SA[SI(k, ir[m])] - w.a[k];
+                    }
+                    stage_faces<METHOD, SLOPE, FT>(c, w, dl, dr, L, keep[m]);
+#pragma unroll
+                    for (int k = 0; k < 5; k++) SB[SI(k, ci[m])] = L.a[k];
+                }
             }
             __syncthreads();
-            if (act) {
 #pragma unroll
-                for (int k = 0; k < 5; k++) {
-                    double df = (double)keep.a[k] - (double)SA[SI(k, il)];
-                    if (stage == 0) u1[k] = u0[k] - lambda * df;
-                    else u1[k] = .5 * (u1[k] + u0[k] - lambda * df);
+            for (int m = 0; m < CPT; m++) {
+                if (act[m]) {
+                    V5<FT> Lr;
+#pragma unroll
+                    for (int k = 0; k < 5; k++) Lr.a[k] = SB[SI(k, ir[m])];
+                    keep[m] = stage_flux<METHOD, FT>(c, keep[m], Lr);
+#pragma unroll
+                    for (int k = 0; k < 5; k++) SA[SI(k, ci[m])] = keep[m].a[k];
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < CPT; m++) {
+                if (act[m]) {
+#pragma unroll
+                    for (int k = 0; k < 5; k++) {
+                        double df = (double)keep[m].a[k] - (double)SA[SI(k, il[m])];
+                        if (stage == 0) u1[m][k] = u0[m][k] - lambda * df;
+                        else u1[m][k] = .5 * (u1[m][k] + u0[m][k] - lambda * df);
+                    }
                 }
             }
             if (stage == 0) __syncthreads();
@@ -483,14 +510,17 @@ __global__ void __launch_bounds__(512, 2)
         // the previous block's store must have read O before O is overwritten
         if (leader) bulk_wait_read_all();
         __syncthreads();
-        if (act) {
 #pragma unroll
-            for (int k = 0; k < 5; k++) O[SI(slots[k], i)] = u1[k];
+        for (int m = 0; m < CPT; m++) {
+            if (act[m]) {
+#pragma unroll
+                for (int k = 0; k < 5; k++) O[SI(slots[k], ci[m])] = u1[m][k];
+            }
         }
         fence_proxy_async_smem();
         __syncthreads();
         if (leader) {
-            pipe_store<DIR>(&tm, O, b, a.npw, W);
+            pipe_store<DIR>(&tm, O, b, a, W);
             bulk_commit();
         }
     }

@@ -41,19 +41,22 @@ int launch_tile_dw(double *q, int64_t slab, const int grid[3], double lambda, co
     return check_launch();
 }
 
-// TMA-fed persistent pipeline (sweep_pipe_kernel): W whole pencils of length n <= 256 per
-// block, W*n <= 512 threads.  Returns IB_ERROR_NOIMPLEMENT (caller falls back) when the grid
-// does not meet TMA's rules: x even (16-byte strides and box rows), W dividing nx.
-template <int METHOD, int SLOPE, typename FT, int DIR, int W>
+// TMA-fed persistent pipeline (sweep_pipe_kernel): W whole pencils of length n <= 512 per
+// block, W*n <= CPT*512 threads' cells.  Returns IB_ERROR_NOIMPLEMENT (caller falls back) when
+// the grid does not meet TMA's rules: x even (16-byte strides and box rows), W dividing nx,
+// pencils above 256 cells even (two box rows of n/2).
+template <int METHOD, int SLOPE, typename FT, int DIR, int W, int CPT>
 int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c, cudaStream_t st)
 {
     const int nx = grid[0], ny = grid[1], nz = grid[2];
     const int n = grid[DIR - 1];
-    if (n > 256 || W * n > 512 || (nx & 1) || nx % W) return IB_ERROR_NOIMPLEMENT;
+    if (n > 512 || (n > 256 && (n & 1)) || W * n > CPT * 512 || (nx & 1) || nx % W) return IB_ERROR_NOIMPLEMENT;
+    if (DIR == 1 && n > 256) return IB_ERROR_NOIMPLEMENT;
     if (((uintptr_t)q & 15) || (slab * 8) % 16) return IB_ERROR_NOIMPLEMENT;
+    const int bh = (n > 256) ? n / 2 : n, nh = (n > 256) ? 2 : 1;
     CUtensorMap tm;
-    uint64_t dims[4], strides[3];
-    uint32_t box[4];
+    uint64_t dims[5], strides[4];
+    uint32_t box[5];
     int rank;
     int64_t nblocks;
     const int npw = (DIR == 1) ? 1 : nx / W;
@@ -64,13 +67,13 @@ int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const
         box[0] = nx; box[1] = 1; box[2] = 5;
         nblocks = (int64_t)ny * nz;
     } else {
-        rank = 4;
+        rank = 5;
         const uint64_t other = (DIR == 2) ? nz : ny;
-        dims[0] = nx; dims[1] = n; dims[2] = other; dims[3] = 5;
-        strides[0] = (DIR == 2) ? (uint64_t)nx * 8 : (uint64_t)nx * ny * 8;
-        strides[1] = (DIR == 2) ? (uint64_t)nx * ny * 8 : (uint64_t)nx * 8;
-        strides[2] = (uint64_t)slab * 8;
-        box[0] = W; box[1] = n; box[2] = 1; box[3] = 5;
+        const uint64_t rs = (DIR == 2) ? (uint64_t)nx * 8 : (uint64_t)nx * ny * 8;   // along the pencil
+        const uint64_t os = (DIR == 2) ? (uint64_t)nx * ny * 8 : (uint64_t)nx * 8;   // across pencils
+        dims[0] = nx; dims[1] = bh; dims[2] = nh; dims[3] = other; dims[4] = 5;
+        strides[0] = rs; strides[1] = rs * bh; strides[2] = os; strides[3] = (uint64_t)slab * 8;
+        box[0] = W; box[1] = bh; box[2] = nh; box[3] = 1; box[4] = 5;
         nblocks = (int64_t)npw * other;
     }
     if (nblocks >= (int64_t)1 << 31) return IB_ERROR_NOIMPLEMENT;
@@ -78,9 +81,10 @@ int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const
     if (rc) return rc;
     unsigned int *err = scratch().wait_flag();
     if (!err) return IB_ERROR_NOMEM;
-    const int nt = ((W * n + 31) / 32) * 32;
+    const int nt = ((W * n + CPT - 1) / CPT + 31) / 32 * 32;  // a multiple of 32, hence of W
+    if (nt > 512) return IB_ERROR_NOIMPLEMENT;
     const size_t shm = 3 * pipe_tile_bytes(n, W) + (size_t)10 * W * n * sizeof(FT);
-    auto kern = sweep_pipe_kernel<METHOD, SLOPE, FT, DIR, W>;
+    auto kern = sweep_pipe_kernel<METHOD, SLOPE, FT, DIR, W, CPT>;
     static int attr_bytes = 0;
     if ((int)shm > attr_bytes) {
         rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
@@ -93,7 +97,7 @@ int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const
     if (per_sm < 1) return IB_ERROR_NOIMPLEMENT;
     const int64_t want = (int64_t)per_sm * num_sms();
     const unsigned nblk = (unsigned)std::min<int64_t>(want, nblocks);
-    PipeArgs a{n, npw, nblocks, lambda, err};
+    PipeArgs a{n, npw, bh, nh, nblocks, lambda, err};
     kern<<<nblk, nt, shm, st>>>(tm, a, c);
     return check_launch();
 }
@@ -126,11 +130,22 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
         const char *e = getenv("IMOGEN_B200_PIPE");
         return (e && e[0] == 'x') ? 1 : 0;
     }();
-    if (use_pipe && n <= 256 && (dir > 1 || pipe_x)) {
-        int rc;
-        if (dir == 1) rc = launch_pipe<METHOD, SLOPE, FT, 1, 1>(q, slab, grid, lambda, c, st);
-        else if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2>(q, slab, grid, lambda, c, st);
-        else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2>(q, slab, grid, lambda, c, st);
+    if (use_pipe && n <= 512 && (dir > 1 || pipe_x)) {
+        int rc = IB_ERROR_NOIMPLEMENT;
+        // z pencils of large x-y planes: blocks 4 columns wide (32-byte rows), which the memory
+        // system serves far better than 16-byte rows at megabyte strides
+        const bool wide = (dir == 3) && ((int64_t)nx * ny * 8 > (1 << 20));
+        if (dir == 1) {
+            if (n <= 256) rc = launch_pipe<METHOD, SLOPE, FT, 1, 1, 1>(q, slab, grid, lambda, c, st);
+        } else if (n <= 256 && !wide) {
+            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1>(q, slab, grid, lambda, c, st);
+            else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1>(q, slab, grid, lambda, c, st);
+        } else if (n <= 256) {
+            rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2>(q, slab, grid, lambda, c, st);
+        } else {
+            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 2>(q, slab, grid, lambda, c, st);
+            else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 2>(q, slab, grid, lambda, c, st);
+        }
         if (rc != IB_ERROR_NOIMPLEMENT) return rc;
     }
 

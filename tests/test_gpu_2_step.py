@@ -297,3 +297,28 @@ def test_tile_path_long_pencils(cuda, ib, po, shape):
     finally:
         ib.use_variant("product")
     assert bits_equal(out, ref, n), first_diff(out, ref, n)
+
+
+@pytest.mark.parametrize("shape", [(6, 300, 4), (8, 512, 3), (388, 340, 12)])
+def test_pipeline_long_pencils_and_wide_z_blocks(cuda, ib, po, shape):
+    """TMA pipeline shapes beyond the basic one: y pencils of 257-512 cells (two box rows, two
+    cells per thread) and z sweeps of large x-y planes (blocks four columns wide)."""
+    n = shape[0] * shape[1] * shape[2]
+    q = problems.random_smooth(shape, gamma=1.4, seed=67, amp=0.3)
+    h = [1.0 / s for s in shape]
+    sp = po.step_params(0.0, h, 1.4, rho_min=1e-5, method=2, slope="mc")
+    ref = q.copy()
+    ib.use_variant("strict")
+    try:
+        ib.device_wait_status(clear=True)
+        fl = to_fluid(q, shape, bc="circular", gamma=1.4)
+        geo = ib.Geometry(shape, h)
+        sp.dt = 0.4 * po.cfl_timestep(ref, shape, 1.4, h, 2)
+        for sd in (1, -1):
+            po.fluid_step_3d(ref, shape, sp, ["circular"] * 6, sd, 0)
+            ib.fluidstep([fl], geo, [sp.dt, 1, sd, 0, 2], ib.numerics(slope="mc"))
+        out = host(fl)
+        assert ib.device_wait_status() == 0
+    finally:
+        ib.use_variant("product")
+    assert bits_equal(out, ref, n), first_diff(out, ref, n)
