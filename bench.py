@@ -35,6 +35,12 @@ GAMMA = 5.0 / 3.0
 CFL = 0.4
 METHOD = 2  # HLLC
 METRIC = "Mcell-updates/s"
+# DRAM bytes per cell of one sweep launch (dram__bytes_read.sum + dram__bytes_write.sum / cells),
+# from the ncu capture summarised in profiles/sweep_pipe_kernels_kh192_fp64.md (KH 192^3, state
+# larger than L2; the traffic scales with the cells swept, so it is applied per cell here).
+TRAFFIC_B_PER_CELL = {"x_row": (283.22 + 236.16) * 1e6 / 192 ** 3,
+                      "y_pipe": (284.39 + 241.22) * 1e6 / 192 ** 3,
+                      "z_pipe": (284.54 + 241.27) * 1e6 / 192 ** 3}
 
 
 def parse():
@@ -241,7 +247,7 @@ def main():
     peak, peak_kind = measured_peaks()
     kern = {}
     reps = max(3, min(10, args.steps))
-    for d, name in ((1, "x_row"), (2, "y_march"), (3, "z_march")):
+    for d, name in ((1, "x_row"), (2, "y_pipe"), (3, "z_pipe")):
         dt = tm.dTime
         ib.cudaFluidStep(fl, geo, [dt, 1, GAMMA, 1e-5, METHOD, d], num)  # warm
         a = torch.cuda.Event(enable_timing=True)
@@ -264,13 +270,13 @@ def main():
     torch.cuda.synchronize()
     kern["cfl"] = a.elapsed_time(b) / reps
     # share per iteration: 2 x-row launches, 2 y, 2 z, 1 cfl
-    share = {"x_row": 2 * kern["x_row"], "y_march": 2 * kern["y_march"], "z_march": 2 * kern["z_march"],
+    share = {"x_row": 2 * kern["x_row"], "y_pipe": 2 * kern["y_pipe"], "z_pipe": 2 * kern["z_pipe"],
              "cfl": kern["cfl"]}
     dom = max(share, key=share.get)
     alg_bytes = (80 if dom != "cfl" else 40) * cells
     achieved = alg_bytes / (kern[dom] / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": dom, "peak_source": peak_kind,
+                "traffic": (TRAFFIC_B_PER_CELL.get(dom, 0) * cells) or None, "kernel": dom, "peak_source": peak_kind,
                 "per_kernel_ms": kern, "step_alg_bytes_per_cell": 480 + 40,
                 "step_frac": (520 * cells) / (ms_max / args.steps / 1e3) / 1e9 / peak}
 
