@@ -424,14 +424,9 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
         const int t = it & 1;
         double *Ut = U[t];
         const uint32_t par = t ? phase1 : phase0;
-        const bool ok = mbar_wait(&full[t], par);
+        const bool ok = mbar_wait_cta(&full[t], par);  // uniform across the CTA
         if (t) phase1 ^= 1; else phase0 ^= 1;
-        double u0[CPT][5], u1[CPT][5];
-#pragma unroll
-        for (int m = 0; m < CPT; m++)
-#pragma unroll
-            for (int k = 0; k < 5; k++) u0[m][k] = act[m] ? Ut[SI(slots[k], ci[m])] : 1.0;
-        if (!__syncthreads_and(ok)) {
+        if (!ok) {
             // a tile never arrived: report, drain what is still in flight, leave
             if (leader) {
                 atomicOr(a.err, 1u);
@@ -442,17 +437,11 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
             }
             return;
         }
-        // tile t is free again: prefetch the block after next into it
-        if (leader) {
-            const int64_t bn = b + 2 * step;
-            if (bn < a.nblocks) {
-                fence_proxy_async_smem();
-                mbar_arrive_expect_tx(&full[t], tile_tx);
-                pipe_load<DIR>(Ut, &tm, bn, a, W, &full[t]);
-            } else {
-                if (t == 0) issued0 = false; else issued1 = false;
-            }
-        }
+        double u0[CPT][5], u1[CPT][5];
+#pragma unroll
+        for (int m = 0; m < CPT; m++)
+#pragma unroll
+            for (int k = 0; k < 5; k++) u0[m][k] = act[m] ? Ut[SI(slots[k], ci[m])] : 1.0;
         V5<FT> keep[CPT];
 #pragma unroll
         for (int stage = 0; stage < 2; stage++) {
@@ -466,6 +455,17 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
                 }
             }
             __syncthreads();
+            if (stage == 0 && leader) {
+                // every thread has read tile t: prefetch the block after next into it
+                const int64_t bn = b + 2 * step;
+                if (bn < a.nblocks) {
+                    fence_proxy_async_smem();
+                    mbar_arrive_expect_tx(&full[t], tile_tx);
+                    pipe_load<DIR>(Ut, &tm, bn, a, W, &full[t]);
+                } else {
+                    if (t == 0) issued0 = false; else issued1 = false;
+                }
+            }
 #pragma unroll
             for (int m = 0; m < CPT; m++) {
                 if (act[m]) {

@@ -66,6 +66,18 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
     return false;
 }
 
+// CTA-wide wait with one poller: thread 0 polls (bounded), the CTA meets at a barrier that also
+// agrees on the outcome, and every thread then takes its own acquire of the completed phase (a
+// test that succeeds at once), so the other threads sleep in the barrier instead of polling.
+__device__ __forceinline__ bool mbar_wait_cta(uint64_t *bar, uint32_t parity)
+{
+    bool ok = true;
+    if (threadIdx.x == 0) ok = mbar_wait(bar, parity);
+    ok = __syncthreads_and(ok);
+    if (ok) ok = mbar_wait(bar, parity);
+    return ok;
+}
+
 // Tiled TMA loads into this CTA's shared memory, completing on `bar` (rank 3 and 4).
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, uint64_t *bar)
 {
