@@ -66,6 +66,21 @@ def dist_init(n_gpus):
     return world, rank, local
 
 
+def max_over_ranks(ms, world, device):
+    """The slowest rank's time: every rank contributes its own and all get the maximum."""
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world, cells, steps, ms_max):
+    """Whole-job Mcell-updates/s of `world` replicas that each advanced `cells` for `steps`."""
+    return world * cells * steps / (ms_max / 1e3) / 1e6
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons during the timed region."""
 
@@ -237,11 +252,8 @@ def main():
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
     barrier()
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * cells * args.steps / (ms_max / 1e3) / 1e6
+    ms_max = max_over_ranks(ms, world, dev)
+    value = job_value(world, cells, args.steps, ms_max)
 
     # ---------------- per-kernel roofline (same stream, CUDA events) ----------------
     peak, peak_kind = measured_peaks()
@@ -297,10 +309,7 @@ def main():
     b.record(stream)
     torch.cuda.synchronize()
     e2e_ms = a.elapsed_time(b)
-    t2 = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-    e2e_val = world * cells * e2e_steps / (float(t2.item()) / 1e3) / 1e6
+    e2e_val = job_value(world, cells, e2e_steps, max_over_ranks(e2e_ms, world, dev))
     nbytes = 5 * slab * 8
 
     # ---------------- CPU baseline (rank 0, N = 1 only) ----------------
