@@ -223,13 +223,13 @@ struct SweepArgs {
 #ifndef IB_ROW_MINB
 #define IB_ROW_MINB 2
 #endif
-template <int METHOD, int SLOPE, typename FT, int CPT>
+template <int METHOD, int SLOPE, typename FT, int CPT, int NFIX = 0>
 __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_kernel(SweepArgs a, FluidConsts<FT> c)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = NFIX ? NFIX : a.nx;  // NFIX: the row length fixed at compile time
     FT *SA = reinterpret_cast<FT *>(smem_raw);
-    FT *SB = SA + 5 * a.nx;
-    const int n = a.nx;
+    FT *SB = SA + 5 * n;
     const int64_t row = blockIdx.x;
     double *q = a.q + row * n;
     const int64_t S = a.slab;
@@ -364,13 +364,13 @@ __device__ __forceinline__ void pipe_store(const CUtensorMap *tm, const double *
     else tma_store_5d(tm, src, (int)(b % a.npw) * W, 0, 0, (int)(b / a.npw), 0);
 }
 
-template <int METHOD, int SLOPE, typename FT, int DIR, int W, int CPT>
+template <int METHOD, int SLOPE, typename FT, int DIR, int W, int CPT, int NFIX = 0>
 __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
     sweep_pipe_kernel(const __grid_constant__ CUtensorMap tm, PipeArgs a, FluidConsts<FT> c)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full[2];
-    const int n = a.n;
+    const int n = NFIX ? NFIX : a.n;  // NFIX: the pencil length fixed at compile time
     const int NW = n * W;
     const size_t tb = pipe_tile_bytes(n, W);
     double *U[2] = {reinterpret_cast<double *>(smem_raw), reinterpret_cast<double *>(smem_raw + tb)};

@@ -45,7 +45,7 @@ int launch_tile_dw(double *q, int64_t slab, const int grid[3], double lambda, co
 // block, W*n <= CPT*512 threads' cells.  Returns IB_ERROR_NOIMPLEMENT (caller falls back) when
 // the grid does not meet TMA's rules: x even (16-byte strides and box rows), W dividing nx,
 // pencils above 256 cells even (two box rows of n/2).
-template <int METHOD, int SLOPE, typename FT, int DIR, int W, int CPT>
+template <int METHOD, int SLOPE, typename FT, int DIR, int W, int CPT, int NFIX = 0>
 int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c, cudaStream_t st)
 {
     const int nx = grid[0], ny = grid[1], nz = grid[2];
@@ -84,7 +84,8 @@ int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const
     const int nt = ((W * n + CPT - 1) / CPT + 31) / 32 * 32;  // a multiple of 32, hence of W
     if (nt > 512) return IB_ERROR_NOIMPLEMENT;
     const size_t shm = 3 * pipe_tile_bytes(n, W) + (size_t)10 * W * n * sizeof(FT);
-    auto kern = sweep_pipe_kernel<METHOD, SLOPE, FT, DIR, W, CPT>;
+    if (NFIX && n != NFIX) return IB_ERROR_NOIMPLEMENT;
+    auto kern = sweep_pipe_kernel<METHOD, SLOPE, FT, DIR, W, CPT, NFIX>;
     static int attr_bytes = 0;
     if ((int)shm > attr_bytes) {
         rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
@@ -137,11 +138,22 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
         const bool wide = (dir == 3) && ((int64_t)nx * ny * 8 > (1 << 20));
         if (dir == 1) {
             if (n <= 256) rc = launch_pipe<METHOD, SLOPE, FT, 1, 1, 1>(q, slab, grid, lambda, c, st);
+        } else if (n == 256 && !wide) {
+            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1, 256>(q, slab, grid, lambda, c, st);
+            else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1, 256>(q, slab, grid, lambda, c, st);
+        } else if (n == 128 && !wide) {
+            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1, 128>(q, slab, grid, lambda, c, st);
+            else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1, 128>(q, slab, grid, lambda, c, st);
         } else if (n <= 256 && !wide) {
             if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1>(q, slab, grid, lambda, c, st);
             else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1>(q, slab, grid, lambda, c, st);
+        } else if (n == 256) {
+            rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2, 256>(q, slab, grid, lambda, c, st);
         } else if (n <= 256) {
             rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2>(q, slab, grid, lambda, c, st);
+        } else if (n == 512) {
+            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 2, 512>(q, slab, grid, lambda, c, st);
+            else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 2, 512>(q, slab, grid, lambda, c, st);
         } else {
             if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 2>(q, slab, grid, lambda, c, st);
             else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 2>(q, slab, grid, lambda, c, st);
@@ -160,7 +172,11 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
         }();
         if (nx <= 512 && xcpt == 1) {
             int nt = ((nx + 31) / 32) * 32;
-            sweep_row_kernel<METHOD, SLOPE, FT, 1><<<(unsigned)rows, nt, shm, st>>>(a, c);
+            // common row lengths get the length at compile time (cheaper shared-memory indexing)
+            if (nx == 256) sweep_row_kernel<METHOD, SLOPE, FT, 1, 256><<<(unsigned)rows, nt, shm, st>>>(a, c);
+            else if (nx == 512) sweep_row_kernel<METHOD, SLOPE, FT, 1, 512><<<(unsigned)rows, nt, shm, st>>>(a, c);
+            else if (nx == 128) sweep_row_kernel<METHOD, SLOPE, FT, 1, 128><<<(unsigned)rows, nt, shm, st>>>(a, c);
+            else sweep_row_kernel<METHOD, SLOPE, FT, 1><<<(unsigned)rows, nt, shm, st>>>(a, c);
         } else {
             int nt = (((nx + 1) / 2 + 31) / 32) * 32;
             static bool attr_set = false;  // rows above 512 cells need more than 48 KB
