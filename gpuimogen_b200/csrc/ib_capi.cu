@@ -434,7 +434,6 @@ int ib_cudaSource2FluidDrag(ib_fluid *gas, ib_fluid *dust, const ib_thermo *tg, 
     if (gas->grid.nx != dust->grid.nx || gas->grid.ny != dust->grid.ny || gas->grid.nz != dust->grid.nz ||
         gas->grid.slab_pitch != dust->grid.slab_pitch)
         return IB_ERROR_INVALID_ARGS;
-    (void)geo;
     const double dt = params[0];
     const int method = (int)params[1];
     if (method < IB_DRAG_EMP || method > IB_DRAG_LOGTRAP3) return IB_ERROR_INVALID_ARGS;
@@ -453,8 +452,14 @@ int ib_cudaSource2FluidDrag(ib_fluid *gas, ib_fluid *dust, const ib_thermo *tg, 
     dp[8] = (gam - 1.0);
     dp[9] = .25 * td->sigma0 / td->mass;
     dp[10] = 16 * (gam - 1.0) / 3.0;
-    const int64_t n = (int64_t)gas->grid.nx * gas->grid.ny * gas->grid.nz;
-    return launch_drag(gas->q, dust->q, gas->grid.slab_pitch, n, dp, dt, method, (cudaStream_t)stream);
+    const int grid[3] = {gas->grid.nx, gas->grid.ny, gas->grid.nz};
+    if (method == IB_DRAG_ETDRK2) {
+        // the pressure gradient needs the cell sizes (prepareForExpMethod, cudaSource2FluidDrag.cu:1728-1741)
+        if (!geo) return IB_ERROR_NULL_POINTER;
+        if (geo->shape != 0) return IB_ERROR_NOIMPLEMENT;  // cylindrical gradients: out of scope
+    }
+    return launch_drag(gas->q, dust->q, gas->grid.slab_pitch, grid, geo ? geo->h : nullptr, dp, dt, method,
+                       (cudaStream_t)stream);
 }
 
 }  // extern "C"

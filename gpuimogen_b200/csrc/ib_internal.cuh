@@ -53,7 +53,7 @@ int launch_fluid_boundary(double *q, int64_t slab, const int grid[3], const int3
 int launch_array_boundary(double *phi, const int grid[3], int mode, int dir, int side, int vec_component, int halo,
                           cudaStream_t st);
 int launch_statics(double *phi, const ib_statics *st_list, int64_t numel, cudaStream_t st);
-int launch_drag(double *gas, double *dust, int64_t slab, int64_t n, const double dp[11], double dt, int method,
-                cudaStream_t st);
+int launch_drag(double *gas, double *dust, int64_t slab, const int grid[3], const double h[3], const double dp[11],
+                double dt, int method, cudaStream_t st);
 
 }  // namespace ib

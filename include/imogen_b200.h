@@ -230,7 +230,9 @@ IB_API int ib_setFluidBoundary(ib_fluid *fluid, int direction, void *stream);
 
 /* Replaces the cudaSource2FluidDrag mex (gpuclass/cudaSource2FluidDrag.cu:125-181 ->
  * sourcefunction_2FluidDrag :189-246): gas-dust drag over dt, in place.
- * params = [dt, method (IB_DRAG_*)]. */
+ * params = [dt, method (IB_DRAG_*)].  geo is read by ETDRK2 only (its pressure gradient uses the
+ * cell sizes h, periodic central differences); it may be NULL for the other methods.  ETDRK2 uses
+ * the library's scratch memory (one slab). */
 IB_API int ib_cudaSource2FluidDrag(ib_fluid *gas, ib_fluid *dust, const ib_thermo *thermo_gas,
                             const ib_thermo *thermo_dust, const ib_geometry *geo,
                             const double *params, int nparams, void *stream);

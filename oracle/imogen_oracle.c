@@ -1296,8 +1296,118 @@ static void etdrk1_cell(double *gas, double *dust, long S, const double dp[11], 
     gas[S] -= .5 * pdustsq / dust[0];
 }
 
+/* solveDragETDRK2 (cudaSource2FluidDrag.cu:575-690), exponential midpoint, as the reference
+ * compiles it (ACCOUNT_GRADP and EXPO_DOTR undefined, :56-63):
+ *   prepareForExpMethod, spaceOrder 2 (:1728-1866): per cell [|dv|, e_int/rho, G_x, G_y, G_z] with
+ *     G the periodic central difference (gamma-1)/(2h) (e_int(+1) - e_int(-1)) of the gas internal
+ *     energy density e_int = E - p^2/2rho (gas2press :1870-1873).  Three layouts: 3-D
+ *     (cukern_prepareForERK3D_h2 :1913-2000, |dv|^2 summed x, y, z), x-y (nz = 1,
+ *     cukern_prepareForERK2D_h2 :2123-2180, summed z, x, y, G_z = 0) and x-z (ny = 1 < nz,
+ *     cukern_prepareForERKRZ_h2 :2238-2290, summed y, x, z, G_y = 0);
+ *   k0 = GeneralLinearCore (:836-890) of (|dv|, e_int/rho);
+ *   cukern_ExpMidpoint_partA (:1247-1312) with t = dt: per axis a = G rho^-1 / k0,
+ *     dv(t) = a + (dv - a) exp(-k0 t) (the x axis adds t G to the gas momentum first; the z axis
+ *     reads the dust y momentum, both as the reference does), the new |dv| and e_int/rho plus the
+ *     drag heating;
+ *   k1 = GeneralLinearCore of those; cukern_ExpMidpoint_partB (:1325-1420) with t = dt and no
+ *     pressure-gradient term: dv <- dv exp(-k1 t) about the centre-of-mass velocity, gas E loses
+ *     the dust kinetic-energy gain.
+ * findMidGradP2 (:2395-2520) rewrites only the gradient slabs, which no later kernel reads, so it
+ * is not restated.  Cells where k0 or k1 is zero (|dv| < 1e-9) are left unchanged: the reference
+ * evaluates 0/0 there. */
+static int drag_etdrk2(double *gas, double *dust, const or_grid *g, const double dp[11], double t,
+                       const double h[3])
+{
+    const long nx = g->nx, ny = g->ny, nz = g->nz, S = g->slab, N = nx * ny * nz;
+    const int three_d = nz > 1 && ny > 1, xz = nz > 1 && ny == 1;
+    const double lamx = dp[8] / (2.0 * h[0]), lamy = dp[8] / (2.0 * h[1]), lamz = dp[8] / (2.0 * h[2]);
+    double *P = (double *)malloc(sizeof(double) * (size_t)(N > 0 ? N : 1));
+    long i;
+    if (!P) return OR_ERR_INVALID;
+#pragma omp parallel for schedule(static)
+    for (i = 0; i < N; i++)
+        P[i] = (gas[S + i] - .5 * (gas[2 * S + i] * gas[2 * S + i] + gas[3 * S + i] * gas[3 * S + i] +
+                                   gas[4 * S + i] * gas[4 * S + i]) / gas[i]);
+#pragma omp parallel for schedule(static)
+    for (i = 0; i < N; i++) {
+        const long x = i % nx, y = (i / nx) % ny, z = i / (nx * ny);
+        const long xm = (x + nx - 1) % nx, xp = (x + 1) % nx;
+        const long ym = (y + ny - 1) % ny, yp = (y + 1) % ny;
+        const long zm = (z + nz - 1) % nz, zp = (z + 1) % nz;
+        double *gs = gas + i, *ds = dust + i;
+        double dvx, dvy, dvz, dvsq, G[3], t0, t1, k, rhoginv, a0, dv_i, dv_t, duint, mu, pdustsq, vstick, dpdt,
+            q;
+        int skip, ax;
+        G[0] = lamx * (P[z * nx * ny + y * nx + xp] - P[z * nx * ny + y * nx + xm]);
+        dvx = (gs[2 * S]) / gs[0] - ds[2 * S] / ds[0];
+        dvy = (gs[3 * S]) / gs[0] - ds[3 * S] / ds[0];
+        dvz = (gs[4 * S]) / gs[0] - ds[4 * S] / ds[0];
+        if (three_d) {
+            G[1] = lamy * (P[z * nx * ny + yp * nx + x] - P[z * nx * ny + ym * nx + x]);
+            G[2] = lamz * (P[zp * nx * ny + y * nx + x] - P[zm * nx * ny + y * nx + x]);
+            dvsq = dvx * dvx;
+            dvsq += dvy * dvy;
+            dvsq += dvz * dvz;
+        } else if (xz) {
+            G[1] = 0.0;
+            G[2] = lamz * (P[zp * nx + x] - P[zm * nx + x]);
+            dvsq = dvy * dvy;
+            dvsq += dvx * dvx;
+            dvsq += dvz * dvz;
+        } else {
+            G[1] = lamy * (P[yp * nx + x] - P[ym * nx + x]);
+            G[2] = 0.0;
+            dvsq = dvz * dvz;
+            dvsq += dvx * dvx;
+            dvsq += dvy * dvy;
+        }
+        t0 = sqrt(dvsq);
+        t1 = P[i] / gs[0];
+        k = drag_k(dp, gs[0], ds[0], t0, t1, &skip);
+        if (skip) continue;
+        /* partA */
+        rhoginv = 1.0 / gs[0];
+        dvsq = 0;
+        duint = 0;
+        for (ax = 0; ax < 3; ax++) {
+            a0 = G[ax];
+            if (ax == 0) dv_i = (gs[2 * S] + t * a0) * rhoginv - ds[2 * S] / ds[0];
+            else dv_i = (gs[(2 + ax) * S]) * rhoginv - ds[3 * S] / ds[0];
+            a0 *= rhoginv / k;
+            dv_t = a0 + (dv_i - a0) * exp(-t * k);
+            if (ax == 0) dvsq = dv_t * dv_t;
+            else dvsq += dv_t * dv_t;
+            q = k * a0 * a0 * t - 2 * a0 * (dv_i - a0) * expm1(-k * t) - (dv_i - a0) * (dv_i - a0) * expm1(-2 * k * t);
+            if (ax == 0) duint = q;
+            else duint += q;
+        }
+        t0 = sqrt(dvsq);
+        t1 += dp[8] * duint * rhoginv;
+        k = drag_k(dp, gs[0], ds[0], t0, t1, &skip);
+        if (skip) continue;
+        /* partB */
+        mu = gs[0] * ds[0] / (gs[0] + ds[0]);
+        pdustsq = 0;
+        for (ax = 2; ax <= 4; ax++) {
+            if (ax == 2) pdustsq = -ds[2 * S] * ds[2 * S];
+            else pdustsq -= ds[ax * S] * ds[ax * S];
+            vstick = (gs[ax * S] + ds[ax * S]) / (gs[0] + ds[0]);
+            dpdt = 0;
+            dv_i = (gs[ax * S]) * rhoginv - ds[ax * S] / ds[0];
+            dpdt *= mu * rhoginv;
+            dv_t = dpdt / k + (dv_i - dpdt / k) * exp(-t * k);
+            gs[ax * S] = gs[0] * vstick + dv_t * mu;
+            ds[ax * S] = q = ds[0] * vstick - dv_t * mu;
+            pdustsq += q * q;
+        }
+        gs[S] -= .5 * pdustsq / ds[0];
+    }
+    free(P);
+    return OR_OK;
+}
+
 int or_drag_2fluid(double *gas, double *dust, const or_grid *g, const double tg[8],
-                   const double td[8], double dt, int method)
+                   const double td[8], double dt, int method, const double *h)
 {
     double dp[11];
     long N = (long)g->nx * g->ny * g->nz;
@@ -1316,6 +1426,10 @@ int or_drag_2fluid(double *gas, double *dust, const or_grid *g, const double tg[
 #pragma omp parallel for schedule(static)
         for (i = 0; i < N; i++) etdrk1_cell(gas + i, dust + i, g->slab, dp, dt);
         return OR_OK;
+    }
+    if (method == 3) {
+        if (!h) return OR_ERR_INVALID;
+        return drag_etdrk2(gas, dust, g, dp, dt, h);
     }
     return OR_ERR_NOIMPL;
 }

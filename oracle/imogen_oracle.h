@@ -89,9 +89,10 @@ void or_statics_fade(double *phi, const double *statics, int64_t n, int64_t pitc
 
 /* Two-fluid drag (cudaSource2FluidDrag.cu).  thermo arrays: [gamma, mass, mu0, muTindex,
  * sigma0, sigmaTindex, kBolt, Cisothermal].  method 0 EMP, 1 RK4, 2 ETDRK1, 3 ETDRK2,
- * 4 LogTrap2, 5 LogTrap3. */
+ * 4 LogTrap2, 5 LogTrap3.  h = cell sizes [hx, hy, hz], read by ETDRK2 only (its pressure
+ * gradient); may be NULL for the other methods. */
 int or_drag_2fluid(double *gas, double *dust, const or_grid *g, const double thermo_gas[8],
-                   const double thermo_dust[8], double dt, int method);
+                   const double thermo_dust[8], double dt, int method, const double *h);
 
 /* Drag constants the reference uploads (cudaSource2FluidDrag.cu:203-218). */
 void or_drag_params(const double thermo_gas[8], const double thermo_dust[8], double dt,

@@ -60,7 +60,7 @@ def lib():
                                         ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.or_statics_fade.argtypes = [dp, dp, ctypes.c_int64, ctypes.c_int64]
         L.or_drag_2fluid.argtypes = [dp, dp, ctypes.POINTER(Grid), dp, dp, ctypes.c_double,
-                                     ctypes.c_int]
+                                     ctypes.c_int, dp]
         L.or_drag_params.argtypes = [dp, dp, ctypes.c_double, dp]
         L.or_drag_logtrap_cells.argtypes = [dp, dp, ctypes.c_int64, ctypes.c_int64, dp,
                                             ctypes.c_double, ctypes.c_int]
@@ -156,10 +156,12 @@ def drag_params(thermo_gas, thermo_dust, dt):
     return out
 
 
-def drag_2fluid(gas, dust, shape, thermo_gas, thermo_dust, dt, method):
+def drag_2fluid(gas, dust, shape, thermo_gas, thermo_dust, dt, method, h=None):
+    """Drag over dt in place; h = cell sizes (default 1/n per axis), used by ETDRK2 only."""
     g = grid(shape, gas.shape[1])
     tg = np.ascontiguousarray(thermo_gas, dtype=np.float64)
     td = np.ascontiguousarray(thermo_dust, dtype=np.float64)
-    rc = lib().or_drag_2fluid(_p(gas), _p(dust), ctypes.byref(g), _p(tg), _p(td), dt, method)
+    hh = np.ascontiguousarray([1.0 / s for s in shape] if h is None else h, dtype=np.float64)
+    rc = lib().or_drag_2fluid(_p(gas), _p(dust), ctypes.byref(g), _p(tg), _p(td), dt, method, _p(hh))
     if rc:
         raise RuntimeError("or_drag_2fluid rc=%d" % rc)

@@ -14,7 +14,7 @@ Boundary conditions are limited to circular, const and mirror: the reference's o
 extrapolation kernels write outside their rows (cudaStatics.cu / boundaryConds.cu), so they are not
 run here.
 
-Usage: python tests/golden/make_golden.py OUTDIR
+Usage: python tests/golden/make_golden.py OUTDIR [--etdrk2-only]
 """
 import ctypes
 import json
@@ -83,8 +83,53 @@ def make_input(gen, shape, gamma):
     raise ValueError(gen)
 
 
-def main(outdir):
+# ETDRK2 (exponential midpoint) differentiates the gas internal energy, so its states carry a
+# seeded pressure field; one per layout the reference distinguishes: x-y plane, 3-D, x-z plane
+# (ny = 1 < nz) and 1-D.  Cell sizes are 1/n per axis as the harness's geometry sets them.
+ETDRK2_SHAPES = [(16, 8, 1), (8, 6, 5), (12, 1, 6), (32, 1, 1)]
+
+
+def etdrk2_state(shape, seed):
+    n = shape[0] * shape[1] * shape[2]
+    rng = np.random.Generator(np.random.Philox(seed))
+    S = (n + 31) // 32 * 32
+    gas, dust = np.zeros((5, S)), np.zeros((5, S))
+    gas[0, :n] = 1.0 + 0.1 * rng.uniform(-1, 1, n)
+    dust[0, :n] = gas[0, :n] * 10 ** rng.uniform(-2, 0, n)
+    for k in (2, 3, 4):
+        gas[k, :n] = gas[0, :n] * rng.uniform(-1e-2, 1e-2, n)
+        dust[k, :n] = dust[0, :n] * rng.uniform(-2e-2, 2e-2, n)
+    P = 1.0 + 0.2 * rng.uniform(-1, 1, n)
+    gas[1, :n] = P / (5 / 3.0 - 1) + 0.5 * (gas[2, :n] ** 2 + gas[3, :n] ** 2 + gas[4, :n] ** 2) / gas[0, :n]
+    dust[1, :n] = 0.5 * (dust[2, :n] ** 2 + dust[3, :n] ** 2 + dust[4, :n] ** 2) / dust[0, :n] + 1e-4 * dust[0, :n]
+    return gas, dust
+
+
+def etdrk2_golden(outdir):
+    rec = {}
+    for j, shape in enumerate(ETDRK2_SHAPES):
+        gas, dust = etdrk2_state(shape, 61 + j)
+        key = "%dx%dx%d" % shape
+        rec["gas_" + key], rec["dust_" + key] = gas, dust
+        for case, tdv in (("", TD), ("stiff_", TD_STIFF)):
+            for strict in (False, True):
+                g, d = gas.copy(), dust.copy()
+                rc = lib("ospre", strict).ref_drag(P(g), P(d), shape[0], shape[1], shape[2], g.shape[1],
+                                                   P(np.array(TG)), P(np.array(tdv)), 0.05, 3)
+                assert rc == 0, (shape, rc)
+                tag = "%s%s_%s" % (case, key, "strict" if strict else "fast")
+                rec["gas_out_" + tag], rec["dust_out_" + tag] = g, d
+    np.savez_compressed(os.path.join(outdir, "drag_etdrk2.npz"),
+                        meta=json.dumps({"shapes": [list(s) for s in ETDRK2_SHAPES], "tg": TG, "td": TD,
+                                         "td_stiff": TD_STIFF, "dt": 0.05}), **rec)
+    print("wrote drag_etdrk2", flush=True)
+
+
+def main(outdir, only=None):
     os.makedirs(outdir, exist_ok=True)
+    if only == "etdrk2":
+        etdrk2_golden(outdir)
+        return
     index = {}
     for name, gen, shape, method, limiter, gamma, c_iso, bc, cfl, niter in FLUID_CASES:
         q0 = make_input(gen, shape, gamma)
@@ -135,8 +180,7 @@ def main(outdir):
     dust[1, :n] = 0.5 * dust[2, :n] ** 2 / rho_d + 1e-4 * rho_d
     drag = {"gas": gas, "dust": dust}
     tg = np.array(TG)
-    # ETDRK2 (method 3) is not run: it needs the finite-difference pressure gradient, which the
-    # library does not implement
+    # ETDRK2 (method 3) has its own states with a pressure gradient: etdrk2_golden
     for case, tdv in (("", TD), ("stiff_", TD_STIFF)):
         td = np.array(tdv)
         for method in (0, 1, 2, 4, 5):
@@ -152,9 +196,12 @@ def main(outdir):
                                                                           "td_stiff": TD_STIFF, "dt": 0.05}),
                         **drag)
     print("wrote drag", flush=True)
+    etdrk2_golden(outdir)
     with open(os.path.join(outdir, "index.json"), "w") as f:
         json.dump(index, f, indent=1)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__)))
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    main(args[0] if args else os.path.dirname(os.path.abspath(__file__)),
+         only="etdrk2" if "--etdrk2-only" in sys.argv else None)

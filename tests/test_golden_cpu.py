@@ -17,7 +17,7 @@ from helpers import bits_equal, first_diff, rel_l1
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 FLUID = sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-               if os.path.basename(p) not in ("cfl.npz", "drag.npz"))
+               if os.path.basename(p) not in ("cfl.npz", "drag.npz", "drag_etdrk2.npz"))
 
 
 def load(path):
@@ -97,4 +97,26 @@ def test_oracle_drag_matches_reference_gpu(po, method, case):
             assert np.array_equal(np.isnan(mine[:, :n]), bad), tag
             a, b = np.where(bad, 0.0, mine[:, :n]), np.where(bad, 0.0, ref[:, :n])
             err = rel_l1(a, b, n)
+            assert np.all(err <= 1e-12), (tag, err)
+
+
+ETDRK2_SHAPES = [(16, 8, 1), (8, 6, 5), (12, 1, 6), (32, 1, 1)]
+
+
+@pytest.mark.parametrize("case", ["", "stiff_"])
+@pytest.mark.parametrize("shape", ETDRK2_SHAPES, ids=lambda s: "%dx%dx%d" % s)
+def test_oracle_etdrk2_matches_reference_gpu(po, shape, case):
+    """ETDRK2 (exponential midpoint with the finite-difference pressure gradient) against the
+    reference's kernels, one state per gradient layout (x-y, 3-D, x-z, 1-D), weak and stiff drag."""
+    z = np.load(os.path.join(GOLDEN, "drag_etdrk2.npz"))
+    meta = json.loads(str(z["meta"]))
+    key = "%dx%dx%d" % shape
+    n = shape[0] * shape[1] * shape[2]
+    g, d = np.array(z["gas_" + key]), np.array(z["dust_" + key])
+    td = meta["td_stiff"] if case else meta["td"]
+    po.drag_2fluid(g, d, shape, meta["tg"], td, meta["dt"], 3, h=[1.0 / s for s in shape])
+    for tag in ("strict", "fast"):
+        for mine, ref in ((g, z["gas_out_%s%s_%s" % (case, key, tag)]), (d, z["dust_out_%s%s_%s" % (case, key, tag)])):
+            assert not np.any(np.isnan(ref[:, :n]))
+            err = rel_l1(mine[:, :n], ref[:, :n], n)
             assert np.all(err <= 1e-12), (tag, err)

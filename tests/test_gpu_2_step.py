@@ -178,16 +178,75 @@ def test_drag_logtrap_matches_oracle(cuda, ib, po, method):
     assert not np.array_equal(g_ref[2, :n], gas[2, :n])   # the drag did act
 
 
-def test_drag_etdrk2_not_implemented(cuda, ib):
+def _etdrk2_state(shape, seed):
+    n = shape[0] * shape[1] * shape[2]
+    rng = np.random.Generator(np.random.Philox(seed))
+    S = ib_slab_pitch(shape)
+    gas, dust = np.zeros((5, S)), np.zeros((5, S))
+    gas[0, :n] = 1.0 + 0.1 * rng.uniform(-1, 1, n)
+    dust[0, :n] = gas[0, :n] * 10 ** rng.uniform(-2, 0, n)
+    for k in (2, 3, 4):
+        gas[k, :n] = gas[0, :n] * rng.uniform(-1e-2, 1e-2, n)
+        dust[k, :n] = dust[0, :n] * rng.uniform(-2e-2, 2e-2, n)
+    P = 1.0 + 0.2 * rng.uniform(-1, 1, n)
+    gas[1, :n] = P / (5 / 3.0 - 1) + 0.5 * (gas[2, :n] ** 2 + gas[3, :n] ** 2 + gas[4, :n] ** 2) / gas[0, :n]
+    dust[1, :n] = 0.5 * (dust[2, :n] ** 2 + dust[3, :n] ** 2 + dust[4, :n] ** 2) / dust[0, :n] + 1e-4 * dust[0, :n]
+    return gas, dust
+
+
+def ib_slab_pitch(shape):
+    n = shape[0] * shape[1] * shape[2]
+    return (n + 31) // 32 * 32
+
+
+ETD_TG = [5 / 3.0, 3.3e-27, 8.4e-6, 0.7, 2.4e-19, 0.2, 1.381e-23, -1]
+ETD_TD = {"weak": [1.01, 3e-11, 0, 0, math.pi * 25e-12, 0, 1.381e-23, 0.1],
+          "stiff": [1.01, 3e-15, 0, 0, math.pi * 25e-12, 0, 1.381e-23, 0.1]}
+
+
+@pytest.mark.parametrize("stiff", ["weak", "stiff"])
+@pytest.mark.parametrize("shape", [(16, 8, 1), (8, 6, 5), (12, 1, 6), (32, 1, 1), (300, 5, 3), (40, 1, 70)],
+                         ids=lambda s: "%dx%dx%d" % s)
+def test_drag_etdrk2_matches_oracle(cuda, ib, po, shape, stiff):
+    """ETDRK2: pressure gradient by periodic central differences in every gradient layout (x-y,
+    3-D, x-z, 1-D; rows longer than one block), then the exponential midpoint update."""
+    n = shape[0] * shape[1] * shape[2]
+    gas, dust = _etdrk2_state(shape, 7 + shape[0])
+    h = [0.5 / shape[0], 0.25 / shape[1], 2.0 / shape[2]]
+    g_ref, d_ref = gas.copy(), dust.copy()
+    po.drag_2fluid(g_ref, d_ref, shape, ETD_TG, ETD_TD[stiff], 0.05, 3, h=h)
+    for variant in ("strict", "product"):
+        fg, fd = to_fluid(gas.copy(), shape), to_fluid(dust.copy(), shape)
+        ib.use_variant(variant)
+        try:
+            ib.cudaSource2FluidDrag(fg, fd, ETD_TG, ETD_TD[stiff], ib.Geometry(shape, h=h), [0.05, 3])
+        finally:
+            ib.use_variant("product")
+        # exp, expm1, pow and sqrt come from CUDA on the GPU and glibc on the CPU (see the LogTrap test)
+        ok, info = product_close(host(fg), g_ref, n, l1=1e-12, scale=1e-11)
+        assert ok, (variant, info)
+        ok, info = product_close(host(fd), d_ref, n, l1=1e-12, scale=1e-11)
+        assert ok, (variant, info)
+    assert not np.array_equal(g_ref[2, :n], gas[2, :n])
+
+
+def test_drag_etdrk2_zero_relative_velocity_cell_unchanged(cuda, ib, po):
+    """A cell whose gas and dust move together (|dv| < 1e-9, drag rate 0) keeps its state, where
+    the reference divides 0 by 0; its neighbours still feel their pressure gradient."""
     shape = (16, 8, 1)
-    q = np.zeros((5, ib.slab_pitch(*shape)))
-    q[0] = 1.0
-    q[1] = 1.0
-    fg, fd = to_fluid(q, shape), to_fluid(q.copy(), shape)
-    tg = [5 / 3.0, 3.3e-27, 8.4e-6, 0.7, 2.4e-19, 0.2, 1.381e-23, -1]
-    td = [1.01, 3e-11, 0, 0, math.pi * 25e-12, 0, 1.381e-23, 0.1]
-    with pytest.raises(ib.ImogenError):
-        ib.cudaSource2FluidDrag(fg, fd, tg, td, ib.Geometry(shape), [0.05, 3])
+    n = 128
+    gas, dust = _etdrk2_state(shape, 3)
+    j = 37
+    dust[2:5, j] = gas[2:5, j] * dust[0, j] / gas[0, j]
+    g_ref, d_ref = gas.copy(), dust.copy()
+    po.drag_2fluid(g_ref, d_ref, shape, ETD_TG, ETD_TD["weak"], 0.05, 3)
+    fg, fd = to_fluid(gas.copy(), shape), to_fluid(dust.copy(), shape)
+    ib.cudaSource2FluidDrag(fg, fd, ETD_TG, ETD_TD["weak"], ib.Geometry(shape), [0.05, 3])
+    G, D = host(fg), host(fd)
+    assert np.array_equal(G[:, j], gas[:, j]) and np.array_equal(D[:, j], dust[:, j])
+    assert np.array_equal(g_ref[:, j], gas[:, j])
+    ok, info = product_close(G, g_ref, n, l1=1e-12, scale=1e-11)
+    assert ok, info
 
 
 def test_sod_gpu_matches_oracle_and_exact(cuda, ib, po):
