@@ -93,23 +93,36 @@ class ClockSampler:
         self.proc = None
         self.lines = []
 
-    def start(self):
+    def start(self, wait_s=10.0):
+        """Starts nvidia-smi (20 ms interval) and waits for its first sample, so that the timed
+        region that follows is covered from its beginning."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "--query-gpu=" + ",".join(self.FIELDS), "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "20", "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
             self.proc = None
+            return
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < wait_s:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
 
-    def stop(self):
+    def mark(self):
+        """Host time stamp for the window of samples kept (begin and end of the timed region)."""
+        return time.time()
+
+    def stop(self, begin=None, end=None):
+        """Stops sampling; summarises the samples taken between begin and end (host times of the
+        timed region; the sample after end is kept too, as it covers the region's last interval)."""
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.05)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -117,7 +130,14 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons, power = [], None, set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
+        lines = list(self.lines)
+        if begin is not None and end is not None:
+            inside = [l for t, l in lines if begin <= t <= end]
+            after = [l for t, l in lines if t > end][:1]
+            lines = inside + after
+        else:
+            lines = [l for _, l in lines]
+        for l in lines:
             p = [x.strip() for x in l.split(",")]
             if len(p) < 9:
                 continue
@@ -239,17 +259,18 @@ def main():
     barrier()
     torch.cuda.synchronize()
     sampler.start()
-    time.sleep(0.3)
     l0 = ib.imogen.launch_count()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    t_begin = sampler.mark()
     e0.record(stream)
     for _ in range(args.steps):
         ib.run_iteration([fl], geo, tm, METHOD, num)
     e1.record(stream)
     torch.cuda.synchronize()
+    t_end = sampler.mark()
     launches = ib.imogen.launch_count() - l0
-    clocks = sampler.stop()
+    clocks = sampler.stop(t_begin, t_end)
     ms = e0.elapsed_time(e1)
     barrier()
     ms_max = max_over_ranks(ms, world, dev)

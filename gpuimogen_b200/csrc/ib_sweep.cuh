@@ -218,11 +218,17 @@ struct SweepArgs {
 
 // ------------------------------------------------------------------------------------------
 // Row kernel: one CTA per x row (nx <= CPT*blockDim.x), periodic in shared memory.
-// Dynamic shared memory: 2 planes x 5 components x nx elements of FT.
+// Dynamic shared memory: 2 planes x 5 components x nx elements of FT; with row_ssum, 5 x nx
+// doubles more hold u1 + u0 of the SSPRK average through the second stage, so that neither state
+// stays in registers there (fewer spills at 64 registers; slower for the 512-cell rows and two
+// cells per thread, which keep them in registers).
 // ------------------------------------------------------------------------------------------
 #ifndef IB_ROW_MINB
 #define IB_ROW_MINB 2
 #endif
+template <int CPT, int NFIX>
+__host__ __device__ constexpr bool row_ssum() { return CPT == 1 && NFIX != 512; }
+
 template <int METHOD, int SLOPE, typename FT, int CPT, int NFIX = 0>
 __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_kernel(SweepArgs a, FluidConsts<FT> c)
 {
@@ -230,6 +236,7 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
     const int n = NFIX ? NFIX : a.nx;  // NFIX: the row length fixed at compile time
     FT *SA = reinterpret_cast<FT *>(smem_raw);
     FT *SB = SA + 5 * n;
+    double *SS = reinterpret_cast<double *>(smem_raw + (size_t)10 * n * sizeof(FT));
     const int64_t row = blockIdx.x;
     double *q = a.q + row * n;
     const int64_t S = a.slab;
@@ -257,6 +264,10 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
                 V5<FT> w = stage_prims<METHOD, 1, FT>(u[m], c);
 #pragma unroll
                 for (int k = 0; k < 5; k++) SA[k * n + i] = w.a[k];
+                if (row_ssum<CPT, NFIX>() && stage == 1) {  // after the prims: HLL floors u1 in place
+#pragma unroll
+                    for (int k = 0; k < 5; k++) SS[k * n + i] = u1[m][k] + u0[m][k];
+                }
             }
         }
         __syncthreads();
@@ -304,6 +315,7 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
                 for (int k = 0; k < 5; k++) {
                     double df = (double)keep[m].a[k] - (double)SA[k * n + il];
                     if (stage == 0) u1[m][k] = u0[m][k] - lambda * df;
+                    else if (row_ssum<CPT, NFIX>()) u1[m][k] = .5 * (SS[k * n + i] - lambda * df);
                     else u1[m][k] = .5 * (u1[m][k] + u0[m][k] - lambda * df);
                 }
             }
@@ -378,6 +390,9 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
     FT *SA = reinterpret_cast<FT *>(smem_raw + 3 * tb);
     FT *SB = SA + 5 * NW;
     const uint32_t tile_tx = (uint32_t)(40 * NW);
+    // u1 + u0 through the second stage in the output tile rather than registers: fewer spills for
+    // the FP64 one-cell-per-thread blocks (64 registers); the others are faster without it
+    constexpr bool SSUM = (CPT == 1) && (sizeof(FT) == 8);
     constexpr int s0 = slot_of<METHOD, DIR>(0), s1 = slot_of<METHOD, DIR>(1), s2 = slot_of<METHOD, DIR>(2),
                   s3 = slot_of<METHOD, DIR>(3), s4 = slot_of<METHOD, DIR>(4);
     const int slots[5] = {s0, s1, s2, s3, s4};
@@ -452,6 +467,13 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
                     V5<FT> w = stage_prims<METHOD, DIR, FT>(u[m], c);
 #pragma unroll
                     for (int k = 0; k < 5; k++) SA[SI(k, ci[m])] = w.a[k];
+                    if (SSUM && stage == 1) {
+                        // u1 + u0 of the SSPRK average goes to this block's output tile, so
+                        // neither state stays in registers through the second stage (after the
+                        // prims: the HLL pressure pass floors u1 in place)
+#pragma unroll
+                        for (int k = 0; k < 5; k++) O[SI(slots[k], ci[m])] = u1[m][k] + u0[m][k];
+                    }
                 }
             }
             __syncthreads();
@@ -501,26 +523,184 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
                     for (int k = 0; k < 5; k++) {
                         double df = (double)keep[m].a[k] - (double)SA[SI(k, il[m])];
                         if (stage == 0) u1[m][k] = u0[m][k] - lambda * df;
-                        else u1[m][k] = .5 * (u1[m][k] + u0[m][k] - lambda * df);
+                        else if (SSUM) {
+                            double &o = O[SI(slots[k], ci[m])];
+                            o = .5 * (o - lambda * df);
+                        } else {
+                            O[SI(slots[k], ci[m])] = .5 * (u1[m][k] + u0[m][k] - lambda * df);
+                        }
                     }
                 }
             }
-            if (stage == 0) __syncthreads();
-        }
-        // the previous block's store must have read O before O is overwritten
-        if (leader) bulk_wait_read_all();
-        __syncthreads();
-#pragma unroll
-        for (int m = 0; m < CPT; m++) {
-            if (act[m]) {
-#pragma unroll
-                for (int k = 0; k < 5; k++) O[SI(slots[k], ci[m])] = u1[m][k];
+            if (stage == 0) {
+                // the previous block's store must have read O before stage 1 rewrites it
+                if (leader) bulk_wait_read_all();
+                __syncthreads();
             }
         }
         fence_proxy_async_smem();
         __syncthreads();
         if (leader) {
             pipe_store<DIR>(&tm, O, b, a, W);
+            bulk_commit();
+        }
+    }
+    if (leader) bulk_wait_all();
+}
+
+// Wide-block variant for z sweeps of large x-y planes.  A block is WL = G*W adjacent columns of
+// whole pencils (64-byte box rows for WL = 8: z rows sit a plane apart, megabytes, and narrow
+// rows there waste most of each memory access), computed in G groups of W columns through
+// shared-memory planes sized for one group.  Results overwrite the tile in place and leave by one
+// TMA store, so two tiles fit: the refill of a tile is issued after the store from it has read
+// it, one block ahead (block b + grid is requested while block b is computed).
+template <int METHOD, int SLOPE, typename FT, int DIR, int W, int G, int CPT, int NFIX = 0>
+__global__ void __launch_bounds__(512, 1)
+    sweep_pipe_wide_kernel(const __grid_constant__ CUtensorMap tm, PipeArgs a, FluidConsts<FT> c)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[2];
+    constexpr int WL = W * G;
+    const int n = NFIX ? NFIX : a.n;
+    const size_t tb = pipe_tile_bytes(n, WL);
+    double *U[2] = {reinterpret_cast<double *>(smem_raw), reinterpret_cast<double *>(smem_raw + tb)};
+    FT *SA = reinterpret_cast<FT *>(smem_raw + 2 * tb);
+    FT *SB = SA + 5 * n * W;
+    const uint32_t tile_tx = (uint32_t)(40 * n * WL);
+    constexpr int s0 = slot_of<METHOD, DIR>(0), s1 = slot_of<METHOD, DIR>(1), s2 = slot_of<METHOD, DIR>(2),
+                  s3 = slot_of<METHOD, DIR>(3), s4 = slot_of<METHOD, DIR>(4);
+    const int slots[5] = {s0, s1, s2, s3, s4};
+    const int col = (int)(threadIdx.x % W);
+    const int rows_per_pass = blockDim.x / W;
+    int ci[CPT], il[CPT], ir[CPT];
+    bool act[CPT];
+#pragma unroll
+    for (int m = 0; m < CPT; m++) {
+        ci[m] = (int)(threadIdx.x / W) + m * rows_per_pass;
+        act[m] = ci[m] < n;
+        il[m] = (ci[m] == 0) ? n - 1 : ci[m] - 1;
+        ir[m] = (ci[m] == n - 1) ? 0 : ci[m] + 1;
+    }
+    auto SI = [&](int k, int j) { return (k * n + j) * W + col; };
+    const double lambda = a.lambda;
+    const int64_t step = gridDim.x;
+    const bool leader = threadIdx.x == 0;
+
+    if (leader) {
+        prefetch_tmap(&tm);
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    bool issued[2] = {false, false};  // leader's bookkeeping of loads in flight
+    if (leader) {
+        for (int t = 0; t < 2; t++) {
+            const int64_t bt = blockIdx.x + t * step;
+            if (bt < a.nblocks) {
+                mbar_arrive_expect_tx(&full[t], tile_tx);
+                pipe_load<DIR>(U[t], &tm, bt, a, WL, &full[t]);
+                issued[t] = true;
+            }
+        }
+    }
+    uint32_t phase[2] = {0, 0};
+    int it = 0;
+    for (int64_t b = blockIdx.x; b < a.nblocks; b += step, it++) {
+        const int t = it & 1;
+        double *Ut = U[t];
+        const bool ok = mbar_wait_cta(&full[t], phase[t]);  // uniform across the CTA
+        if (!ok) {
+            if (leader) {
+                atomicOr(a.err, 1u);
+                mbar_wait(&full[t], phase[t]);  // one more bounded wait for the late tile
+                if (issued[t ^ 1]) mbar_wait(&full[t ^ 1], phase[t ^ 1]);
+                bulk_wait_all();
+            }
+            return;
+        }
+        phase[t] ^= 1;
+        issued[t] = false;
+#pragma unroll 1
+        for (int g = 0; g < G; g++) {
+            const int tc = g * W + col;  // column within the tile
+            auto TI = [&](int k, int j) { return (k * n + j) * WL + tc; };
+            double u0[CPT][5], u1[CPT][5];
+#pragma unroll
+            for (int m = 0; m < CPT; m++)
+#pragma unroll
+                for (int k = 0; k < 5; k++) u0[m][k] = act[m] ? Ut[TI(slots[k], ci[m])] : 1.0;
+            V5<FT> keep[CPT];
+#pragma unroll
+            for (int stage = 0; stage < 2; stage++) {
+                double (*u)[5] = (stage == 0) ? u0 : u1;
+#pragma unroll
+                for (int m = 0; m < CPT; m++) {
+                    if (act[m]) {
+                        V5<FT> w = stage_prims<METHOD, DIR, FT>(u[m], c);
+#pragma unroll
+                        for (int k = 0; k < 5; k++) SA[SI(k, ci[m])] = w.a[k];
+                    }
+                }
+                __syncthreads();
+                if (stage == 0 && g == 0 && it > 0 && leader) {
+                    // the other tile's block has been stored: once that store has read it,
+                    // request the next block into it
+                    bulk_wait_read_all();
+                    const int64_t bn = b + step;
+                    if (bn < a.nblocks) {
+                        mbar_arrive_expect_tx(&full[t ^ 1], tile_tx);
+                        pipe_load<DIR>(U[t ^ 1], &tm, bn, a, WL, &full[t ^ 1]);
+                        issued[t ^ 1] = true;
+                    }
+                }
+#pragma unroll
+                for (int m = 0; m < CPT; m++) {
+                    if (act[m]) {
+                        V5<FT> w, dl, dr, L;
+#pragma unroll
+                        for (int k = 0; k < 5; k++) {
+                            w.a[k] = SA[SI(k, ci[m])];
+                            dl.a[k] = w.a[k] - SA[SI(k, il[m])];
+                            dr.a[k] = SA[SI(k, ir[m])] - w.a[k];
+                        }
+                        stage_faces<METHOD, SLOPE, FT>(c, w, dl, dr, L, keep[m]);
+#pragma unroll
+                        for (int k = 0; k < 5; k++) SB[SI(k, ci[m])] = L.a[k];
+                    }
+                }
+                __syncthreads();
+#pragma unroll
+                for (int m = 0; m < CPT; m++) {
+                    if (act[m]) {
+                        V5<FT> Lr;
+#pragma unroll
+                        for (int k = 0; k < 5; k++) Lr.a[k] = SB[SI(k, ir[m])];
+                        keep[m] = stage_flux<METHOD, FT>(c, keep[m], Lr);
+#pragma unroll
+                        for (int k = 0; k < 5; k++) SA[SI(k, ci[m])] = keep[m].a[k];
+                    }
+                }
+                __syncthreads();
+#pragma unroll
+                for (int m = 0; m < CPT; m++) {
+                    if (act[m]) {
+#pragma unroll
+                        for (int k = 0; k < 5; k++) {
+                            double df = (double)keep[m].a[k] - (double)SA[SI(k, il[m])];
+                            if (stage == 0) u1[m][k] = u0[m][k] - lambda * df;
+                            // each thread rewrites only the cells it read
+                            else Ut[TI(slots[k], ci[m])] = .5 * (u1[m][k] + u0[m][k] - lambda * df);
+                        }
+                    }
+                }
+                __syncthreads();  // the planes are rewritten next (stage 1, or the next group)
+            }
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (leader) {
+            pipe_store<DIR>(&tm, Ut, b, a, WL);
             bulk_commit();
         }
     }

@@ -45,13 +45,18 @@ int launch_tile_dw(double *q, int64_t slab, const int grid[3], double lambda, co
 // block, W*n <= CPT*512 threads' cells.  Returns IB_ERROR_NOIMPLEMENT (caller falls back) when
 // the grid does not meet TMA's rules: x even (16-byte strides and box rows), W dividing nx,
 // pencils above 256 cells even (two box rows of n/2).
-template <int METHOD, int SLOPE, typename FT, int DIR, int W, int CPT, int NFIX = 0>
+//
+// G > 1 selects sweep_pipe_wide_kernel: blocks of W*G columns (one TMA box), computed W at a time,
+// results stored from the input tile; pencils up to 256 cells, y/z sweeps only.
+template <int METHOD, int SLOPE, typename FT, int DIR, int W, int CPT, int NFIX = 0, int G = 1>
 int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c, cudaStream_t st)
 {
     const int nx = grid[0], ny = grid[1], nz = grid[2];
     const int n = grid[DIR - 1];
-    if (n > 512 || (n > 256 && (n & 1)) || W * n > CPT * 512 || (nx & 1) || nx % W) return IB_ERROR_NOIMPLEMENT;
+    constexpr int WL = W * G;  // columns per block (and per TMA box)
+    if (n > 512 || (n > 256 && (n & 1)) || W * n > CPT * 512 || (nx & 1) || nx % WL) return IB_ERROR_NOIMPLEMENT;
     if (DIR == 1 && n > 256) return IB_ERROR_NOIMPLEMENT;
+    if (G > 1 && (DIR == 1 || n > 256)) return IB_ERROR_NOIMPLEMENT;
     if (((uintptr_t)q & 15) || (slab * 8) % 16) return IB_ERROR_NOIMPLEMENT;
     const int bh = (n > 256) ? n / 2 : n, nh = (n > 256) ? 2 : 1;
     CUtensorMap tm;
@@ -59,7 +64,7 @@ int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const
     uint32_t box[5];
     int rank;
     int64_t nblocks;
-    const int npw = (DIR == 1) ? 1 : nx / W;
+    const int npw = (DIR == 1) ? 1 : nx / WL;
     if (DIR == 1) {
         rank = 3;
         dims[0] = nx; dims[1] = (uint64_t)ny * nz; dims[2] = 5;
@@ -73,7 +78,7 @@ int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const
         const uint64_t os = (DIR == 2) ? (uint64_t)nx * ny * 8 : (uint64_t)nx * 8;   // across pencils
         dims[0] = nx; dims[1] = bh; dims[2] = nh; dims[3] = other; dims[4] = 5;
         strides[0] = rs; strides[1] = rs * bh; strides[2] = os; strides[3] = (uint64_t)slab * 8;
-        box[0] = W; box[1] = bh; box[2] = nh; box[3] = 1; box[4] = 5;
+        box[0] = WL; box[1] = bh; box[2] = nh; box[3] = 1; box[4] = 5;
         nblocks = (int64_t)npw * other;
     }
     if (nblocks >= (int64_t)1 << 31) return IB_ERROR_NOIMPLEMENT;
@@ -83,9 +88,14 @@ int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const
     if (!err) return IB_ERROR_NOMEM;
     const int nt = ((W * n + CPT - 1) / CPT + 31) / 32 * 32;  // a multiple of 32, hence of W
     if (nt > 512) return IB_ERROR_NOIMPLEMENT;
-    const size_t shm = 3 * pipe_tile_bytes(n, W) + (size_t)10 * W * n * sizeof(FT);
+    const size_t shm = (G == 1 ? 3 * pipe_tile_bytes(n, W) : 2 * pipe_tile_bytes(n, WL)) +
+                       (size_t)10 * W * n * sizeof(FT);
     if (NFIX && n != NFIX) return IB_ERROR_NOIMPLEMENT;
-    auto kern = sweep_pipe_kernel<METHOD, SLOPE, FT, DIR, W, CPT, NFIX>;
+    if (shm > 227 * 1024) return IB_ERROR_NOIMPLEMENT;
+    auto kern = [] {
+        if constexpr (G == 1) return &sweep_pipe_kernel<METHOD, SLOPE, FT, DIR, W, CPT, NFIX>;
+        else return &sweep_pipe_wide_kernel<METHOD, SLOPE, FT, DIR, W, G, CPT, NFIX>;
+    }();
     static int attr_bytes = 0;
     if ((int)shm > attr_bytes) {
         rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
@@ -136,6 +146,10 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
         // z pencils of large x-y planes: blocks 4 columns wide (32-byte rows), which the memory
         // system serves far better than 16-byte rows at megabyte strides
         const bool wide = (dir == 3) && ((int64_t)nx * ny * 8 > (1 << 20));
+        static const int wide8 = [] {
+            const char *e = getenv("IMOGEN_B200_WIDE8");  // 0 = 4-column blocks for wide z planes
+            return (e && e[0] == '0') ? 0 : 1;
+        }();
         if (dir == 1) {
             if (n <= 256) rc = launch_pipe<METHOD, SLOPE, FT, 1, 1, 1>(q, slab, grid, lambda, c, st);
         } else if (n == 256 && !wide) {
@@ -148,9 +162,18 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
             if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1>(q, slab, grid, lambda, c, st);
             else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1>(q, slab, grid, lambda, c, st);
         } else if (n == 256) {
-            rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2, 256>(q, slab, grid, lambda, c, st);
+            // FP32 flux: 8-column blocks (64-byte rows) computed 4 columns at a time (3.48 -> 2.52
+            // ms at 512 x 512 x 256).  FP64 is bound by its arithmetic there and keeps 4 columns:
+            // its planes leave room for only 2 columns per group, which is slower.
+            if constexpr (sizeof(FT) == 4) {
+                if (wide8 == 1) rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2, 256, 2>(q, slab, grid, lambda, c, st);
+            }
+            if (rc == IB_ERROR_NOIMPLEMENT) rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2, 256>(q, slab, grid, lambda, c, st);
         } else if (n <= 256) {
-            rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2>(q, slab, grid, lambda, c, st);
+            if constexpr (sizeof(FT) == 4) {
+                if (wide8 == 1) rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2, 0, 2>(q, slab, grid, lambda, c, st);
+            }
+            if (rc == IB_ERROR_NOIMPLEMENT) rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2>(q, slab, grid, lambda, c, st);
         } else if (n == 512) {
             if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 2, 512>(q, slab, grid, lambda, c, st);
             else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 2, 512>(q, slab, grid, lambda, c, st);
@@ -165,27 +188,38 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
         // one CTA per row, one or two cells per thread
         SweepArgs a{q, slab, nx, ny, nz, lambda};
         const int64_t rows = (int64_t)ny * nz;
-        const size_t shm = (size_t)10 * nx * sizeof(FT);
         static const int xcpt = [] {
             const char *e = getenv("IMOGEN_B200_XCPT");  // 2 = two cells per thread for all rows
             return (e && e[0] == '2') ? 2 : 1;
         }();
-        if (nx <= 512 && xcpt == 1) {
+        const int cpt = (nx <= 512 && xcpt == 1) ? 1 : 2;
+        // the planes, plus the SSPRK sum where row_ssum holds (one cell per thread, rows but 512)
+        const size_t shm = (size_t)10 * nx * sizeof(FT) + ((cpt == 1 && nx != 512) ? (size_t)40 * nx : 0);
+        // rows above 384 FP64 cells need more than the default 48 KB of shared memory
+        auto opt_in = [](auto kern, size_t bytes) {
+            return check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        };
+        if (cpt == 1) {
             int nt = ((nx + 31) / 32) * 32;
+            const size_t max1 = (size_t)10 * 512 * sizeof(FT) + (size_t)40 * 512;
             // common row lengths get the length at compile time (cheaper shared-memory indexing)
-            if (nx == 256) sweep_row_kernel<METHOD, SLOPE, FT, 1, 256><<<(unsigned)rows, nt, shm, st>>>(a, c);
-            else if (nx == 512) sweep_row_kernel<METHOD, SLOPE, FT, 1, 512><<<(unsigned)rows, nt, shm, st>>>(a, c);
-            else if (nx == 128) sweep_row_kernel<METHOD, SLOPE, FT, 1, 128><<<(unsigned)rows, nt, shm, st>>>(a, c);
-            else sweep_row_kernel<METHOD, SLOPE, FT, 1><<<(unsigned)rows, nt, shm, st>>>(a, c);
+            if (nx == 256) {
+                sweep_row_kernel<METHOD, SLOPE, FT, 1, 256><<<(unsigned)rows, nt, shm, st>>>(a, c);
+            } else if (nx == 512) {
+                static const int rc0 = opt_in(sweep_row_kernel<METHOD, SLOPE, FT, 1, 512>, max1);
+                if (rc0) return rc0;
+                sweep_row_kernel<METHOD, SLOPE, FT, 1, 512><<<(unsigned)rows, nt, shm, st>>>(a, c);
+            } else if (nx == 128) {
+                sweep_row_kernel<METHOD, SLOPE, FT, 1, 128><<<(unsigned)rows, nt, shm, st>>>(a, c);
+            } else {
+                static const int rc1 = opt_in(sweep_row_kernel<METHOD, SLOPE, FT, 1>, max1);
+                if (rc1) return rc1;
+                sweep_row_kernel<METHOD, SLOPE, FT, 1><<<(unsigned)rows, nt, shm, st>>>(a, c);
+            }
         } else {
             int nt = (((nx + 1) / 2 + 31) / 32) * 32;
-            static bool attr_set = false;  // rows above 512 cells need more than 48 KB
-            if (!attr_set) {
-                int rc = check_cuda(cudaFuncSetAttribute(sweep_row_kernel<METHOD, SLOPE, FT, 2>,
-                                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-                if (rc) return rc;
-                attr_set = true;
-            }
+            static const int rc2 = opt_in(sweep_row_kernel<METHOD, SLOPE, FT, 2>, (size_t)10 * 1024 * sizeof(FT));
+            if (rc2) return rc2;
             sweep_row_kernel<METHOD, SLOPE, FT, 2><<<(unsigned)rows, nt, shm, st>>>(a, c);
         }
         return check_launch();

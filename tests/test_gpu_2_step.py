@@ -358,10 +358,11 @@ def test_tile_path_long_pencils(cuda, ib, po, shape):
     assert bits_equal(out, ref, n), first_diff(out, ref, n)
 
 
-@pytest.mark.parametrize("shape", [(6, 300, 4), (8, 512, 3), (388, 340, 12)])
+@pytest.mark.parametrize("shape", [(6, 300, 4), (8, 512, 3), (388, 340, 12), (392, 336, 6)])
 def test_pipeline_long_pencils_and_wide_z_blocks(cuda, ib, po, shape):
     """TMA pipeline shapes beyond the basic one: y pencils of 257-512 cells (two box rows, two
-    cells per thread) and z sweeps of large x-y planes (blocks four columns wide)."""
+    cells per thread) and z sweeps of large x-y planes (blocks four columns wide; with the FP32
+    flux and nx a multiple of 8, eight columns computed in groups and stored in place)."""
     n = shape[0] * shape[1] * shape[2]
     q = problems.random_smooth(shape, gamma=1.4, seed=67, amp=0.3)
     h = [1.0 / s for s in shape]
@@ -381,3 +382,33 @@ def test_pipeline_long_pencils_and_wide_z_blocks(cuda, ib, po, shape):
     finally:
         ib.use_variant("product")
     assert bits_equal(out, ref, n), first_diff(out, ref, n)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32flux"])
+@pytest.mark.parametrize("nz", [256, 200])
+def test_wide_z_blocks_match_y_sweep_of_transposed_state(cuda, ib, nz, precision):
+    """Full-size z sweeps of a 256 x 520 plane (the 8-column wide-block kernel; nz = 256 with the
+    pencil length fixed at compile time) against the y sweep of the same state with y and z (and
+    p_y and p_z) exchanged, which runs through the ordinary pipeline kernel."""
+    shape = (256, 520, nz)
+    N = shape[0] * shape[1] * shape[2]
+    q = torch.from_numpy(problems.kelvin_helmholtz(shape, seed=3)).cuda()
+    h = [1.0 / 256, 1.0 / 520, 1.0 / nz]
+    num = ib.numerics(slope="mc", precision=precision)
+    dt = 0.2 / (2.0 * 520)
+    fl = ib.Fluid(shape, q=q.clone(), gamma=5 / 3.0)
+    ib.cudaFluidStep(fl, ib.Geometry(shape, h), [dt, 1, 5 / 3.0, 1e-5, 2, 3], num)
+    tshape = (256, nz, 520)
+    qt = torch.zeros_like(q)
+    qt[:, :N] = q[:, :N].view(5, nz, 520, 256).transpose(1, 2).reshape(5, N)
+    qt[[3, 4]] = qt[[4, 3]].clone()
+    ft = ib.Fluid(tshape, q=qt, gamma=5 / 3.0)
+    ib.cudaFluidStep(ft, ib.Geometry(tshape, [h[0], h[2], h[1]]), [dt, 1, 5 / 3.0, 1e-5, 2, 2], num)
+    back = ft.q[:, :N].view(5, 520, nz, 256).transpose(1, 2).reshape(5, N).clone()
+    back[[3, 4]] = back[[4, 3]].clone()
+    out = fl.q[:, :N]
+    assert ib.device_wait_status() == 0
+    assert not torch.equal(out, q[:, :N])  # the sweep did act
+    err = ((out - back).abs().sum(dim=1) / back.abs().sum(dim=1).clamp_min(1e-300)).cpu().numpy()
+    tol = 1e-13 if precision == "fp64" else 1e-7
+    assert np.all(err <= tol), err
