@@ -385,7 +385,8 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
     const int n = NFIX ? NFIX : a.n;  // NFIX: the pencil length fixed at compile time
     const int NW = n * W;
     const size_t tb = pipe_tile_bytes(n, W);
-    double *U[2] = {reinterpret_cast<double *>(smem_raw), reinterpret_cast<double *>(smem_raw + tb)};
+    // input tile t (computed, not an indexed array, which would live in local memory)
+    auto Ub = [&](int t) { return reinterpret_cast<double *>(smem_raw + t * tb); };
     double *O = reinterpret_cast<double *>(smem_raw + 2 * tb);
     FT *SA = reinterpret_cast<FT *>(smem_raw + 3 * tb);
     FT *SB = SA + 5 * NW;
@@ -424,12 +425,12 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
         const int64_t b0 = blockIdx.x, b1 = blockIdx.x + step;
         if (b0 < a.nblocks) {
             mbar_arrive_expect_tx(&full[0], tile_tx);
-            pipe_load<DIR>(U[0], &tm, b0, a, W, &full[0]);
+            pipe_load<DIR>(Ub(0), &tm, b0, a, W, &full[0]);
             issued0 = true;
         }
         if (b1 < a.nblocks) {
             mbar_arrive_expect_tx(&full[1], tile_tx);
-            pipe_load<DIR>(U[1], &tm, b1, a, W, &full[1]);
+            pipe_load<DIR>(Ub(1), &tm, b1, a, W, &full[1]);
             issued1 = true;
         }
     }
@@ -437,7 +438,7 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
     int it = 0;
     for (int64_t b = blockIdx.x; b < a.nblocks; b += step, it++) {
         const int t = it & 1;
-        double *Ut = U[t];
+        double *Ut = Ub(t);
         const uint32_t par = t ? phase1 : phase0;
         const bool ok = mbar_wait_cta(&full[t], par);  // uniform across the CTA
         if (t) phase1 ^= 1; else phase0 ^= 1;
@@ -563,7 +564,7 @@ __global__ void __launch_bounds__(512, 1)
     constexpr int WL = W * G;
     const int n = NFIX ? NFIX : a.n;
     const size_t tb = pipe_tile_bytes(n, WL);
-    double *U[2] = {reinterpret_cast<double *>(smem_raw), reinterpret_cast<double *>(smem_raw + tb)};
+    auto Ub = [&](int t) { return reinterpret_cast<double *>(smem_raw + t * tb); };
     FT *SA = reinterpret_cast<FT *>(smem_raw + 2 * tb);
     FT *SB = SA + 5 * n * W;
     const uint32_t tile_tx = (uint32_t)(40 * n * WL);
@@ -593,34 +594,34 @@ __global__ void __launch_bounds__(512, 1)
         fence_mbar_init();
     }
     __syncthreads();
-    bool issued[2] = {false, false};  // leader's bookkeeping of loads in flight
+    // bit t: a load into tile t is in flight (leader's bookkeeping) / parity to wait for on t
+    uint32_t issued = 0, phase = 0;
     if (leader) {
         for (int t = 0; t < 2; t++) {
             const int64_t bt = blockIdx.x + t * step;
             if (bt < a.nblocks) {
                 mbar_arrive_expect_tx(&full[t], tile_tx);
-                pipe_load<DIR>(U[t], &tm, bt, a, WL, &full[t]);
-                issued[t] = true;
+                pipe_load<DIR>(Ub(t), &tm, bt, a, WL, &full[t]);
+                issued |= 1u << t;
             }
         }
     }
-    uint32_t phase[2] = {0, 0};
     int it = 0;
     for (int64_t b = blockIdx.x; b < a.nblocks; b += step, it++) {
         const int t = it & 1;
-        double *Ut = U[t];
-        const bool ok = mbar_wait_cta(&full[t], phase[t]);  // uniform across the CTA
+        double *Ut = Ub(t);
+        const bool ok = mbar_wait_cta(&full[t], (phase >> t) & 1);  // uniform across the CTA
         if (!ok) {
             if (leader) {
                 atomicOr(a.err, 1u);
-                mbar_wait(&full[t], phase[t]);  // one more bounded wait for the late tile
-                if (issued[t ^ 1]) mbar_wait(&full[t ^ 1], phase[t ^ 1]);
+                mbar_wait(&full[t], (phase >> t) & 1);  // one more bounded wait for the late tile
+                if ((issued >> (t ^ 1)) & 1) mbar_wait(&full[t ^ 1], (phase >> (t ^ 1)) & 1);
                 bulk_wait_all();
             }
             return;
         }
-        phase[t] ^= 1;
-        issued[t] = false;
+        phase ^= 1u << t;
+        issued &= ~(1u << t);
 #pragma unroll 1
         for (int g = 0; g < G; g++) {
             const int tc = g * W + col;  // column within the tile
@@ -650,8 +651,8 @@ __global__ void __launch_bounds__(512, 1)
                     const int64_t bn = b + step;
                     if (bn < a.nblocks) {
                         mbar_arrive_expect_tx(&full[t ^ 1], tile_tx);
-                        pipe_load<DIR>(U[t ^ 1], &tm, bn, a, WL, &full[t ^ 1]);
-                        issued[t ^ 1] = true;
+                        pipe_load<DIR>(Ub(t ^ 1), &tm, bn, a, WL, &full[t ^ 1]);
+                        issued |= 1u << (t ^ 1);
                     }
                 }
 #pragma unroll
@@ -705,6 +706,225 @@ __global__ void __launch_bounds__(512, 1)
         }
     }
     if (leader) bulk_wait_all();
+}
+
+// ------------------------------------------------------------------------------------------
+// Chunked pipeline for pencils longer than 512 cells.  A job is one chunk of L = R - 8 output
+// cells of a block of W adjacent pencils; its tile is one TMA box of R rows, the chunk with 4 rows
+// of halo on each side (both SSPRK stages are recomputed on the halo).  x rows: W = 1, R = 256;
+// y/z pencils: W = 4, R = 128 (32-byte box rows: 16-byte rows at the large strides of long
+// pencils are served poorly).  A persistent CTA walks its pencil blocks one after the other and
+// each block chunk by chunk, with the loads of the next two jobs in flight (double-buffered tiles,
+// one mbarrier each).
+//   * Periodic ends: the box of the first chunk starts 4 rows before the pencil and the last
+//     one runs past its end; TMA fills those rows, and a 4-row halo box from the other end of the
+//     pencil (loaded with the same mbarrier) replaces them.
+//   * In-place update: a chunk's outputs overlap the halo of the next chunk's box, so before they
+//     are written the CTA waits for that load to have landed; the first chunk's first 4 outputs
+//     are the last chunk's halo, so they wait in shared memory until the last chunk is loaded.
+//   * Outputs are plain stores from registers (rows 4 .. Rr-5 of the tile).
+//   * The chunk length Lr and tile rows Rr = Lr + 8 <= R are launch arguments (threads past Rr
+//     idle); the launcher uses Lr = R - 8.
+// Dynamic shared memory: 2 tiles of 40*R*W bytes, 2 halo slots of 40*4*W, the deferred outputs
+// (40*4*W), the SSPRK sum u1 + u0 through the second stage (40*R*W: neither state stays in
+// registers there), then 2 planes of 5*R*W elements of FT.
+// ------------------------------------------------------------------------------------------
+struct ChunkArgs {
+    double *q;
+    int64_t slab;       // doubles between slabs
+    int64_t rs;         // doubles between consecutive cells of a pencil
+    int64_t os;         // doubles between consecutive pencils along the other axis (rows for x)
+    int n;              // pencil length (> 512)
+    int C;              // chunks per pencil
+    int Lr, Rr;         // output rows per chunk (n split evenly, even) and rows per tile, Lr + 8 <= R
+    int npw;            // pencil blocks per line of x (nx / W; 1 for x sweeps)
+    int64_t ngroups;    // pencil blocks in the grid
+    double lambda;
+    unsigned int *err;  // set to 1 when a TMA wait ran out
+};
+
+__host__ __device__ constexpr size_t chunk_smem_bytes(int W, int R, int ftsize)
+{
+    return 3 * (((size_t)40 * R * W + 127) / 128 * 128) + 3 * (((size_t)160 * W + 127) / 128 * 128) +
+           (size_t)10 * R * W * ftsize;
+}
+
+template <int DIR>
+__device__ __forceinline__ void chunk_load(double *dst, const CUtensorMap *tm, int64_t grp, int g0, const ChunkArgs &a,
+                                           int W, uint64_t *bar)
+{
+    if (DIR == 1) tma_load_3d(dst, tm, g0, (int)grp, 0, bar);
+    else tma_load_4d(dst, tm, (int)(grp % a.npw) * W, g0, (int)(grp / a.npw), 0, bar);
+}
+
+template <int METHOD, int SLOPE, typename FT, int DIR, int W, int R>
+__global__ void __launch_bounds__(512, 2)
+    sweep_chunk_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_constant__ CUtensorMap tmH, ChunkArgs a,
+                       FluidConsts<FT> c)
+{
+    const int L = a.Lr, Rr = a.Rr;  // rows of this launch's tiles: Rr <= R
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[2];
+    constexpr size_t tb = ((size_t)40 * R * W + 127) / 128 * 128;
+    constexpr size_t hb = ((size_t)160 * W + 127) / 128 * 128;
+    // tile and halo slot of buffer b (computed, not indexed arrays, which would live in local memory)
+    auto Ub = [&](int b) { return reinterpret_cast<double *>(smem_raw + b * tb); };
+    auto Hb = [&](int b) { return reinterpret_cast<double *>(smem_raw + 2 * tb + b * hb); };
+    double *DEF = reinterpret_cast<double *>(smem_raw + 2 * tb + 2 * hb);
+    double *SS = reinterpret_cast<double *>(smem_raw + 2 * tb + 3 * hb);
+    FT *SA = reinterpret_cast<FT *>(smem_raw + 3 * tb + 3 * hb);
+    FT *SB = SA + 5 * R * W;
+    const uint32_t tile_tx = 40u * Rr * W;
+    constexpr uint32_t halo_tx = 160u * W;
+    constexpr int s0 = slot_of<METHOD, DIR>(0), s1 = slot_of<METHOD, DIR>(1), s2 = slot_of<METHOD, DIR>(2),
+                  s3 = slot_of<METHOD, DIR>(3), s4 = slot_of<METHOD, DIR>(4);
+    const int slots[5] = {s0, s1, s2, s3, s4};
+    const int col = (W == 1) ? 0 : (int)(threadIdx.x % W);
+    const int r = (int)(threadIdx.x / W);  // tile row of this thread; blockDim.x = W * R
+    const int il = (r > 0) ? r - 1 : 0, ir = (r < Rr - 1) ? r + 1 : Rr - 1;  // edge rows: unused results
+    auto SI = [&](int k, int j) { return (k * R + j) * W + col; };
+    const int n = a.n, C = a.C;
+    const double lambda = a.lambda;
+    const bool leader = threadIdx.x == 0;
+    // jobs of this CTA: pencil blocks blockIdx.x, +gridDim.x, ..., each chunk 0 .. C-1
+    const int64_t mygroups = (a.ngroups > (int64_t)blockIdx.x) ? (a.ngroups - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const int64_t njobs = mygroups * C;
+    auto job_group = [&](int64_t j) { return (int64_t)blockIdx.x + (j / C) * (int64_t)gridDim.x; };
+
+    if (leader) {
+        prefetch_tmap(&tmM);
+        prefetch_tmap(&tmH);
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    auto issue = [&](int64_t j, int buf) {  // leader only
+        const int64_t grp = job_group(j);
+        const int cc = (int)(j % C);
+        const bool edge = (cc == 0) || (cc == C - 1);
+        mbar_arrive_expect_tx(&full[buf], tile_tx + (edge ? halo_tx : 0u));
+        chunk_load<DIR>(Ub(buf), &tmM, grp, cc * L - 4, a, W, &full[buf]);
+        if (cc == 0) chunk_load<DIR>(Hb(buf), &tmH, grp, n - 4, a, W, &full[buf]);
+        else if (cc == C - 1) chunk_load<DIR>(Hb(buf), &tmH, grp, 0, a, W, &full[buf]);
+    };
+    // bit b: a load into buffer b is in flight (leader's bookkeeping) / parity to wait for on b
+    uint32_t issued = 0, phase = 0;
+    if (leader) {
+        for (int t = 0; t < 2; t++)
+            if (t < njobs) { issue(t, t); issued |= 1u << t; }
+    }
+    for (int64_t j = 0; j < njobs; j++) {
+        const int buf = (int)(j & 1);
+        const int64_t grp = job_group(j);
+        const int cc = (int)(j % C);
+        bool ok = mbar_wait_cta(&full[buf], (phase >> buf) & 1);
+        if (!ok) {
+            if (leader) {
+                atomicOr(a.err, 1u);
+                mbar_wait(&full[buf], (phase >> buf) & 1);
+                if ((issued >> (buf ^ 1)) & 1) mbar_wait(&full[buf ^ 1], (phase >> (buf ^ 1)) & 1);
+            }
+            return;
+        }
+        phase ^= 1u << buf;
+        issued &= ~(1u << buf);
+        // this thread's cell: g = cc*L - 4 + r; rows before the pencil and past its end come from
+        // the halo slot, rows more than 4 past the end are idle
+        const int g = cc * L - 4 + r;
+        const bool act = r < Rr && g < n + 4;
+        const double *src;
+        int srow, srows;
+        if (g < 0) { src = Hb(buf); srow = g + 4; srows = 4; }
+        else if (g >= n) { src = Hb(buf); srow = g - n; srows = 4; }
+        else { src = Ub(buf); srow = r; srows = Rr; }
+        double u0[5], u1[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) u0[k] = act ? src[(slots[k] * srows + srow) * W + col] : 1.0;
+        V5<FT> keep;
+#pragma unroll
+        for (int stage = 0; stage < 2; stage++) {
+            double *u = (stage == 0) ? u0 : u1;
+            {
+                V5<FT> w = stage_prims<METHOD, DIR, FT>(u, c);
+#pragma unroll
+                for (int k = 0; k < 5; k++) SA[SI(k, r)] = w.a[k];
+                if (stage == 1) {  // after the prims: HLL floors u1 in place
+#pragma unroll
+                    for (int k = 0; k < 5; k++) SS[SI(k, r)] = u1[k] + u0[k];
+                }
+            }
+            __syncthreads();
+            if (stage == 0 && leader && j + 2 < njobs) {
+                // every thread has read tile buf: request the job after next into it
+                fence_proxy_async_smem();
+                issue(j + 2, buf);
+                issued |= 1u << buf;
+            }
+            {
+                V5<FT> w, dl, dr, Lf;
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    w.a[k] = SA[SI(k, r)];
+                    dl.a[k] = w.a[k] - SA[SI(k, il)];
+                    dr.a[k] = SA[SI(k, ir)] - w.a[k];
+                }
+                stage_faces<METHOD, SLOPE, FT>(c, w, dl, dr, Lf, keep);
+#pragma unroll
+                for (int k = 0; k < 5; k++) SB[SI(k, r)] = Lf.a[k];
+            }
+            __syncthreads();
+            {
+                V5<FT> Lr;
+#pragma unroll
+                for (int k = 0; k < 5; k++) Lr.a[k] = SB[SI(k, ir)];
+                keep = stage_flux<METHOD, FT>(c, keep, Lr);
+#pragma unroll
+                for (int k = 0; k < 5; k++) SA[SI(k, r)] = keep.a[k];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                double df = (double)keep.a[k] - (double)SA[SI(k, il)];
+                if (stage == 0) u1[k] = u0[k] - lambda * df;
+                else u1[k] = .5 * (SS[SI(k, r)] - lambda * df);
+            }
+            __syncthreads();  // the planes are rewritten next
+        }
+        // the next chunk of this block re-reads this chunk's last 4 outputs as its halo: its tile
+        // must have landed before they are written
+        if (cc < C - 1) {
+            ok = mbar_wait_cta(&full[buf ^ 1], (phase >> (buf ^ 1)) & 1);
+            if (!ok) {
+                if (leader) {
+                    atomicOr(a.err, 1u);
+                    mbar_wait(&full[buf ^ 1], (phase >> (buf ^ 1)) & 1);  // one more bounded wait for it
+                    if ((issued >> buf) & 1) mbar_wait(&full[buf], (phase >> buf) & 1);
+                }
+                return;
+            }
+        }
+        const bool out = act && r >= 4 && r < Rr - 4 && g < n;
+        double *base;
+        if (DIR == 1) base = a.q + grp * a.os;
+        else base = a.q + (grp % a.npw) * W + col + (grp / a.npw) * a.os;
+        if (out) {
+            if (cc == 0 && g < 4) {
+#pragma unroll
+                for (int k = 0; k < 5; k++) DEF[(k * 4 + g) * W + col] = u1[k];
+            } else {
+#pragma unroll
+                for (int k = 0; k < 5; k++) base[slots[k] * a.slab + (int64_t)g * a.rs] = u1[k];
+            }
+        }
+        if (cc == C - 1 && r >= 4 && r < 8) {
+            // the deferred first 4 outputs of this block (written by these same threads in chunk 0;
+            // this chunk's tile, which held them as its halo, has landed)
+            const int gd = r - 4;
+#pragma unroll
+            for (int k = 0; k < 5; k++) base[slots[k] * a.slab + (int64_t)gd * a.rs] = DEF[(k * 4 + gd) * W + col];
+        }
+    }
 }
 
 // The HLL corrector adds (fluid after the floors of the predictor's pressure pass) and

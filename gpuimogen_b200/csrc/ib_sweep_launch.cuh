@@ -113,6 +113,84 @@ int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const
     return check_launch();
 }
 
+// Chunked TMA pipeline (sweep_chunk_kernel) for pencils of more than 512 cells: W = 1, R = 256
+// (x rows) or W = 4, R = 128 (y/z pencils).  Returns IB_ERROR_NOIMPLEMENT (caller falls back)
+// when the grid does not meet TMA's rules: x rows of even length; y/z with W dividing nx.
+template <int METHOD, int SLOPE, typename FT, int DIR, int W, int R>
+int launch_chunk(double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c, cudaStream_t st)
+{
+    const int nx = grid[0], ny = grid[1], nz = grid[2];
+    const int n = grid[DIR - 1];
+    if (n <= 512) return IB_ERROR_NOIMPLEMENT;
+    if (DIR == 1 && (n & 1)) return IB_ERROR_NOIMPLEMENT;
+    if (DIR != 1 && ((nx & 1) || nx % W)) return IB_ERROR_NOIMPLEMENT;
+    if (((uintptr_t)q & 15) || (slab * 8) % 16) return IB_ERROR_NOIMPLEMENT;
+    CUtensorMap tmM, tmH;
+    uint64_t dims[4], strides[3];
+    uint32_t boxM[4], boxH[4];
+    int rank;
+    ChunkArgs a;
+    a.q = q;
+    a.slab = slab;
+    a.n = n;
+    a.C = (n + (R - 8) - 1) / (R - 8);
+    // full-length chunks: a job costs its tile's rows whatever its outputs, and an even split
+    // (shorter tiles, box rows not a multiple of 128 bytes) measured slower
+    a.Lr = R - 8;
+    a.Rr = R;
+    a.lambda = lambda;
+    if (DIR == 1) {
+        rank = 3;
+        dims[0] = nx; dims[1] = (uint64_t)ny * nz; dims[2] = 5;
+        strides[0] = (uint64_t)nx * 8; strides[1] = (uint64_t)slab * 8;
+        boxM[0] = a.Rr; boxM[1] = 1; boxM[2] = 5;
+        boxH[0] = 4; boxH[1] = 1; boxH[2] = 5;
+        a.rs = 1; a.os = nx; a.npw = 1;
+        a.ngroups = (int64_t)ny * nz;
+    } else {
+        rank = 4;
+        const uint64_t other = (DIR == 2) ? nz : ny;
+        a.rs = (DIR == 2) ? (int64_t)nx : (int64_t)nx * ny;
+        a.os = (DIR == 2) ? (int64_t)nx * ny : (int64_t)nx;
+        dims[0] = nx; dims[1] = n; dims[2] = other; dims[3] = 5;
+        strides[0] = (uint64_t)a.rs * 8; strides[1] = (uint64_t)a.os * 8; strides[2] = (uint64_t)slab * 8;
+        boxM[0] = W; boxM[1] = a.Rr; boxM[2] = 1; boxM[3] = 5;
+        boxH[0] = W; boxH[1] = 4; boxH[2] = 1; boxH[3] = 5;
+        a.npw = nx / W;
+        a.ngroups = (int64_t)a.npw * other;
+    }
+    if (a.ngroups >= ((int64_t)1 << 31) / a.C) return IB_ERROR_NOIMPLEMENT;
+    int rc = encode_tmap_f64(&tmM, q, rank, dims, strides, boxM);
+    if (rc) return rc;
+    rc = encode_tmap_f64(&tmH, q, rank, dims, strides, boxH);
+    if (rc) return rc;
+    a.err = scratch().wait_flag();
+    if (!a.err) return IB_ERROR_NOMEM;
+    const int nt = W * R;
+    const size_t shm = chunk_smem_bytes(W, R, (int)sizeof(FT));
+    auto kern = sweep_chunk_kernel<METHOD, SLOPE, FT, DIR, W, R>;
+    static int attr_bytes = 0;
+    if ((int)shm > attr_bytes) {
+        rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        if (rc) return rc;
+        attr_bytes = (int)shm;
+    }
+    int per_sm = 0;
+    rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, shm));
+    if (rc) return rc;
+    if (per_sm < 1) return IB_ERROR_NOIMPLEMENT;
+    // as many resident CTAs as fit: a CTA's pencil blocks are latency-bound chains of chunks
+    int k = per_sm;
+    static const int force_k = [] {
+        const char *e = getenv("IMOGEN_B200_CHUNK_CTAS");  // resident CTAs per SM, overriding the choice
+        return (e && e[0] >= '1' && e[0] <= '8') ? e[0] - '0' : 0;
+    }();
+    if (force_k) k = std::min(force_k, per_sm);
+    const unsigned nblk = (unsigned)std::min<int64_t>((int64_t)k * num_sms(), a.ngroups);
+    kern<<<nblk, nt, shm, st>>>(tmM, tmH, a, c);
+    return check_launch();
+}
+
 template <int METHOD, int SLOPE, typename FT>
 int launch_tile_t(int dir, double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c,
                   cudaStream_t st)
@@ -181,6 +259,19 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
             if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 2>(q, slab, grid, lambda, c, st);
             else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 2>(q, slab, grid, lambda, c, st);
         }
+        if (rc != IB_ERROR_NOIMPLEMENT) return rc;
+    }
+
+    // pencils above 512 cells: chunked TMA pipeline (x rows above 1024 cells; y and z above 512)
+    static const int use_chunk = [] {
+        const char *e = getenv("IMOGEN_B200_CHUNK");  // 0 = the tile kernel for long pencils
+        return (e && e[0] == '0') ? 0 : 1;
+    }();
+    if (use_pipe && use_chunk && n > 512 && (dir > 1 || nx > 1024)) {
+        int rc;
+        if (dir == 1) rc = launch_chunk<METHOD, SLOPE, FT, 1, 1, 256>(q, slab, grid, lambda, c, st);
+        else if (dir == 2) rc = launch_chunk<METHOD, SLOPE, FT, 2, 4, 128>(q, slab, grid, lambda, c, st);
+        else rc = launch_chunk<METHOD, SLOPE, FT, 3, 4, 128>(q, slab, grid, lambda, c, st);
         if (rc != IB_ERROR_NOIMPLEMENT) return rc;
     }
 

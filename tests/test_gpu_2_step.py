@@ -358,6 +358,39 @@ def test_tile_path_long_pencils(cuda, ib, po, shape):
     assert bits_equal(out, ref, n), first_diff(out, ref, n)
 
 
+@pytest.mark.parametrize("shape,method,slope", [((1100, 3, 2), 2, "mc"), ((1240, 2, 1), 2, "mc"),
+                                                ((4, 700, 3), 2, "mc"), ((8, 4, 1030), 2, "mc"),
+                                                ((4, 720, 2), 1, "ospre"), ((1028, 520, 1), 2, "mc"),
+                                                ((1028, 520, 1), 1, "vanleer"), ((1101, 2, 2), 2, "mc"),
+                                                ((6, 4, 600), 2, "mc")])
+def test_chunk_pipeline_long_pencils(cuda, ib, po, shape, method, slope):
+    """Pencils above 512 cells (x rows above 1024) through the chunked TMA pipeline: chunks of
+    248 (x) or 120 (y/z) cells with 4-cell halos, periodic ends from halo boxes, the first chunk's
+    first outputs deferred; pencil lengths with a partial and with a whole last chunk (1240 = 5 x
+    248, 720 = 6 x 120), HLLC and HLL.  Odd x rows (1101) and nx not a multiple of 4 (6) fall back
+    to the tile kernel.  Strict build bit-exact."""
+    n = shape[0] * shape[1] * shape[2]
+    q = problems.random_smooth(shape, gamma=1.4, seed=71, amp=0.3)
+    h = [1.0 / s for s in shape]
+    sp = po.step_params(0.0, h, 1.4, rho_min=1e-5, method=method, slope=slope)
+    ref = q.copy()
+    ib.use_variant("strict")
+    try:
+        ib.device_wait_status(clear=True)
+        fl = to_fluid(q, shape, bc="circular", gamma=1.4)
+        geo = ib.Geometry(shape, h)
+        for it in range(2):
+            sp.dt = 0.4 * po.cfl_timestep(ref, shape, 1.4, h, method)
+            for sd in (1, -1):
+                po.fluid_step_3d(ref, shape, sp, ["circular"] * 6, sd, it)
+                ib.fluidstep([fl], geo, [sp.dt, 1, sd, it, method], ib.numerics(slope=slope))
+        out = host(fl)
+        assert ib.device_wait_status() == 0
+    finally:
+        ib.use_variant("product")
+    assert bits_equal(out, ref, n), first_diff(out, ref, n)
+
+
 @pytest.mark.parametrize("shape", [(6, 300, 4), (8, 512, 3), (388, 340, 12), (392, 336, 6)])
 def test_pipeline_long_pencils_and_wide_z_blocks(cuda, ib, po, shape):
     """TMA pipeline shapes beyond the basic one: y pencils of 257-512 cells (two box rows, two
