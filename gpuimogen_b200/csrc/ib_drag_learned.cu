@@ -334,11 +334,23 @@ static int launch_mlp_tc(const LearnedArgs &a, cudaStream_t st)
             return rc;
         attr = true;
     }
-    int per_sm = 0;
-    if ((rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, LT, shm)))) return rc;
-    // 4 CTAs of 128 threads fit by registers and shared memory; 8 x 64 tensor-memory columns are
-    // all 512 of an SM.  CTAs never wait on each other, so a grid above residency only queues.
-    per_sm = std::max(4, std::min(per_sm, 8));
+    // A CTA walks its tiles to the end, so the grid is what fits at once: counted here from the
+    // registers and shared memory (the occupancy query reports 1 for this kernel), at most 8
+    // (8 x 64 tensor-memory columns are all 512 of an SM).
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        cudaFuncAttributes fa;
+        int dev = 0, smem_sm = 0, resv = 0;
+        if ((rc = check_cuda(cudaFuncGetAttributes(&fa, kern)))) return rc;
+        if ((rc = check_cuda(cudaGetDevice(&dev)))) return rc;
+        if ((rc = check_cuda(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev))))
+            return rc;
+        if ((rc = check_cuda(cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev)))) return rc;
+        const int regs = (fa.numRegs + 7) / 8 * 8;
+        const int by_regs = 65536 / std::max(1, regs * LT);
+        const int by_smem = smem_sm / (int)(shm + fa.sharedSizeBytes + resv);
+        per_sm = std::max(1, std::min(std::min(by_regs, by_smem), 8));
+    }
     const int64_t ntiles = (a.n + LT - 1) / LT;
     const unsigned grid = (unsigned)std::min<int64_t>(ntiles, (int64_t)per_sm * num_sms());
     kern<<<grid, LT, shm, st>>>(a);
