@@ -36,11 +36,11 @@ CFL = 0.4
 METHOD = 2  # HLLC
 METRIC = "Mcell-updates/s"
 # DRAM bytes per cell of one sweep launch (dram__bytes_read.sum + dram__bytes_write.sum / cells),
-# from the ncu capture summarised in profiles/sweep_pipe_kernels_kh192_fp64.md (KH 192^3, state
-# larger than L2; the traffic scales with the cells swept, so it is applied per cell here).
-TRAFFIC_B_PER_CELL = {"x_row": (283.22 + 236.16) * 1e6 / 192 ** 3,
-                      "y_pipe": (284.39 + 241.22) * 1e6 / 192 ** 3,
-                      "z_pipe": (284.54 + 241.27) * 1e6 / 192 ** 3}
+# from the ncu capture of this workload's three sweep kernels summarised in
+# profiles/sweep_kernels_kh256_fp64.md (KH 256^3, state larger than L2).
+TRAFFIC_B_PER_CELL = {"x_row": (671.12 + 612.90) * 1e6 / 256 ** 3,
+                      "y_pipe": (697.60 + 639.29) * 1e6 / 256 ** 3,
+                      "z_pipe": (699.63 + 644.84) * 1e6 / 256 ** 3}
 
 
 def parse():

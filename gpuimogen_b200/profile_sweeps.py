@@ -1,9 +1,10 @@
 """Small-case driver for profiling the sweep kernels with Nsight Compute.
 
 Runs one warm-up iteration of the Kelvin-Helmholtz problem, then one launch of each sweep
-kernel (x row, y march, z march) and one CFL reduction on a grid whose state (5 FP64 slabs)
-exceeds the 126 MB L2.  Usage:
-  python -m gpuimogen_b200.profile_sweeps [--n 192] [--precision fp64|fp32flux] [--method 2]
+kernel (x, y, z; a sweep along an axis of extent 1 launches nothing) and one CFL reduction on a
+grid whose state (5 FP64 slabs) exceeds the 126 MB L2: n^3, or --shape nx,ny,nz.  Usage:
+  python -m gpuimogen_b200.profile_sweeps [--n 192 | --shape 2048,2048,1] [--precision fp64|fp32flux]
+                                         [--method 2]
 """
 import argparse
 
@@ -16,11 +17,12 @@ from gpuimogen_b200 import problems
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=192)
+    ap.add_argument("--shape", default=None, help="nx,ny,nz instead of n^3")
     ap.add_argument("--precision", default="fp64")
     ap.add_argument("--method", type=int, default=2)
     ap.add_argument("--slope", default="mc")
     a = ap.parse_args()
-    shape = (a.n, a.n, a.n)
+    shape = tuple(int(v) for v in a.shape.split(",")) if a.shape else (a.n, a.n, a.n)
     q = problems.kelvin_helmholtz(shape, seed=1)
     fl = ib.Fluid(shape, q=torch.from_numpy(q).cuda(), gamma=5 / 3.0)
     geo = ib.Geometry(shape)
