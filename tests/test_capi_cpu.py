@@ -96,6 +96,12 @@ def test_invalid_calls_rejected_without_device():
     pd2 = (ctypes.c_double * 2)(1e-3, 6)
     assert L.ib_cudaSource2FluidDrag(ctypes.byref(f), ctypes.byref(f), ctypes.byref(tg), ctypes.byref(tg),
                                      ctypes.byref(geo), pd2, 2, None) == -100
+    # ETDRK2 differentiates the pressure: it needs the geometry, and square cells
+    pe = (ctypes.c_double * 2)(1e-3, 3)
+    assert L.ib_cudaSource2FluidDrag(ctypes.byref(f), ctypes.byref(f), ctypes.byref(tg), ctypes.byref(tg),
+                                     None, pe, 2, None) == -102
+    assert L.ib_cudaSource2FluidDrag(ctypes.byref(f), ctypes.byref(f), ctypes.byref(tg), ctypes.byref(tg),
+                                     ctypes.byref(geo2), pe, 2, None) == -105
     # cudaStatics direction and vector component
     grid = imogen.IbGrid(16, 8, 4, 0, 512)
     bc = (ctypes.c_int32 * 6)(0, 0, 0, 0, 0, 0)
