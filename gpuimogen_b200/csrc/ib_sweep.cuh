@@ -709,44 +709,66 @@ __global__ void __launch_bounds__(512, 1)
 }
 
 // ------------------------------------------------------------------------------------------
-// Chunked pipeline for pencils longer than 512 cells.  A job is one chunk of L = R - 8 output
-// cells of a block of W adjacent pencils; its tile is one TMA box of R rows, the chunk with 4 rows
-// of halo on each side (both SSPRK stages are recomputed on the halo).  x rows: W = 1, R = 256;
-// y/z pencils: W = 4, R = 128 (32-byte box rows: 16-byte rows at the large strides of long
-// pencils are served poorly).  A persistent CTA walks its pencil blocks one after the other and
-// each block chunk by chunk, with the loads of the next two jobs in flight (double-buffered tiles,
-// one mbarrier each).
-//   * Periodic ends: the box of the first chunk starts 4 rows before the pencil and the last
-//     one runs past its end; TMA fills those rows, and a 4-row halo box from the other end of the
-//     pencil (loaded with the same mbarrier) replaces them.
-//   * In-place update: a chunk's outputs overlap the halo of the next chunk's box, so before they
-//     are written the CTA waits for that load to have landed; the first chunk's first 4 outputs
-//     are the last chunk's halo, so they wait in shared memory until the last chunk is loaded.
-//   * Outputs are plain stores from registers (rows 4 .. Rr-5 of the tile).
-//   * The chunk length Lr and tile rows Rr = Lr + 8 <= R are launch arguments (threads past Rr
-//     idle); the launcher uses Lr = R - 8.
-// Dynamic shared memory: 2 tiles of 40*R*W bytes, 2 halo slots of 40*4*W, the deferred outputs
-// (40*4*W), the SSPRK sum u1 + u0 through the second stage (40*R*W: neither state stays in
-// registers there), then 2 planes of 5*R*W elements of FT.
+// Chunked pipeline for pencils longer than 512 cells.  A pencil is cut into C chunks of L cells
+// (the last one shorter); a job is one chunk of a block of W adjacent pencils, computed on R = L + 8
+// rows: the chunk plus 4 rows of halo on each side (both SSPRK stages are recomputed on the halo).
+// x rows: W = 1, L = 248; y/z pencils: W = 4, L = 120 (32-byte box rows: 16-byte rows at the large
+// strides of long pencils are served poorly).
+//   * Independent jobs: before the sweep, chunk_halo_kernel copies the 8 rows around every chunk
+//     boundary (periodic: boundary 0 is rows n-4 .. 3) to a side buffer, and a job takes its halo
+//     rows from there.  No job reads what another writes, so the jobs of one pencil run on any
+//     CTAs in any order and the persistent grid deals them out evenly.
+//   * A job's L chunk rows arrive as one TMA box (rows past the pencil's end are filled and idle);
+//     the loads of the next two jobs are in flight while one is computed (double-buffered tiles,
+//     one mbarrier each, bounded waits).  Outputs are plain stores from registers.
+// Dynamic shared memory: 2 tiles of 40*L*W bytes (rounded to 128), the SSPRK sum u1 + u0 through
+// the second stage (40*R*W bytes: neither state stays in registers there), then 2 planes of
+// 5*R*W elements of FT.
 // ------------------------------------------------------------------------------------------
 struct ChunkArgs {
     double *q;
-    int64_t slab;       // doubles between slabs
-    int64_t rs;         // doubles between consecutive cells of a pencil
-    int64_t os;         // doubles between consecutive pencils along the other axis (rows for x)
-    int n;              // pencil length (> 512)
-    int C;              // chunks per pencil
-    int Lr, Rr;         // output rows per chunk (n split evenly, even) and rows per tile, Lr + 8 <= R
-    int npw;            // pencil blocks per line of x (nx / W; 1 for x sweeps)
-    int64_t ngroups;    // pencil blocks in the grid
+    const double *side;  // halo rows: [group][boundary][slab][8 rows][W]
+    int64_t slab;        // doubles between slabs
+    int64_t rs;          // doubles between consecutive cells of a pencil
+    int64_t os;          // doubles between consecutive pencils along the other axis (rows for x)
+    int n;               // pencil length (> 512)
+    int C;               // chunks per pencil: ceil(n / L)
+    int npw;             // pencil blocks per line of x (nx / W; 1 for x sweeps)
+    int64_t ngroups;     // pencil blocks in the grid
     double lambda;
-    unsigned int *err;  // set to 1 when a TMA wait ran out
+    unsigned int *err;   // set to 1 when a TMA wait ran out
 };
 
 __host__ __device__ constexpr size_t chunk_smem_bytes(int W, int R, int ftsize)
 {
-    return 3 * (((size_t)40 * R * W + 127) / 128 * 128) + 3 * (((size_t)160 * W + 127) / 128 * 128) +
-           (size_t)10 * R * W * ftsize;
+    return 2 * (((size_t)40 * (R - 8) * W + 127) / 128 * 128) + (size_t)40 * R * W + (size_t)10 * R * W * ftsize;
+}
+
+// First cell of pencil block grp, column col.
+__device__ __forceinline__ int64_t chunk_base(const ChunkArgs &a, int DIR, int W, int64_t grp, int col)
+{
+    if (DIR == 1) return grp * a.os;
+    return (grp % a.npw) * W + col + (grp / a.npw) * a.os;
+}
+
+// Side buffer: for every pencil block and chunk boundary b, rows (b*L - 4 .. b*L + 3) mod n of the
+// 5 slabs.  One thread per value.
+template <int DIR, int W>
+__global__ void __launch_bounds__(256) chunk_halo_kernel(ChunkArgs a, int L, double *side)
+{
+    const int64_t total = a.ngroups * a.C * 5 * 8 * W;
+    for (int64_t t = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; t < total; t += (int64_t)blockDim.x * gridDim.x) {
+        const int col = (int)(t % W);
+        const int rr = (int)((t / W) % 8);
+        const int k = (int)((t / (8 * W)) % 5);
+        const int64_t gb = t / (40 * W);  // grp * C + b
+        const int b = (int)(gb % a.C);
+        const int64_t grp = gb / a.C;
+        int row = b * L - 4 + rr;
+        if (row < 0) row += a.n;
+        else if (row >= a.n) row -= a.n;
+        side[t] = a.q[chunk_base(a, DIR, W, grp, col) + k * a.slab + (int64_t)row * a.rs];
+    }
 }
 
 template <int DIR>
@@ -759,88 +781,87 @@ __device__ __forceinline__ void chunk_load(double *dst, const CUtensorMap *tm, i
 
 template <int METHOD, int SLOPE, typename FT, int DIR, int W, int R>
 __global__ void __launch_bounds__(512, 2)
-    sweep_chunk_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_constant__ CUtensorMap tmH, ChunkArgs a,
-                       FluidConsts<FT> c)
+    sweep_chunk_kernel(const __grid_constant__ CUtensorMap tm, ChunkArgs a, FluidConsts<FT> c)
 {
-    const int L = a.Lr, Rr = a.Rr;  // rows of this launch's tiles: Rr <= R
+    constexpr int L = R - 8;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full[2];
-    constexpr size_t tb = ((size_t)40 * R * W + 127) / 128 * 128;
-    constexpr size_t hb = ((size_t)160 * W + 127) / 128 * 128;
-    // tile and halo slot of buffer b (computed, not indexed arrays, which would live in local memory)
+    constexpr size_t tb = ((size_t)40 * L * W + 127) / 128 * 128;
+    // tile of buffer b (computed, not an indexed array, which would live in local memory)
     auto Ub = [&](int b) { return reinterpret_cast<double *>(smem_raw + b * tb); };
-    auto Hb = [&](int b) { return reinterpret_cast<double *>(smem_raw + 2 * tb + b * hb); };
-    double *DEF = reinterpret_cast<double *>(smem_raw + 2 * tb + 2 * hb);
-    double *SS = reinterpret_cast<double *>(smem_raw + 2 * tb + 3 * hb);
-    FT *SA = reinterpret_cast<FT *>(smem_raw + 3 * tb + 3 * hb);
+    double *SS = reinterpret_cast<double *>(smem_raw + 2 * tb);
+    FT *SA = reinterpret_cast<FT *>(smem_raw + 2 * tb + (size_t)40 * R * W);
     FT *SB = SA + 5 * R * W;
-    const uint32_t tile_tx = 40u * Rr * W;
-    constexpr uint32_t halo_tx = 160u * W;
+    constexpr uint32_t tile_tx = 40u * L * W;
     constexpr int s0 = slot_of<METHOD, DIR>(0), s1 = slot_of<METHOD, DIR>(1), s2 = slot_of<METHOD, DIR>(2),
                   s3 = slot_of<METHOD, DIR>(3), s4 = slot_of<METHOD, DIR>(4);
     const int slots[5] = {s0, s1, s2, s3, s4};
     const int col = (W == 1) ? 0 : (int)(threadIdx.x % W);
-    const int r = (int)(threadIdx.x / W);  // tile row of this thread; blockDim.x = W * R
-    const int il = (r > 0) ? r - 1 : 0, ir = (r < Rr - 1) ? r + 1 : Rr - 1;  // edge rows: unused results
+    const int r = (int)(threadIdx.x / W);  // row of this thread in the job; blockDim.x = W * R
+    const int il = (r > 0) ? r - 1 : 0, ir = (r < R - 1) ? r + 1 : R - 1;  // edge rows: unused results
     auto SI = [&](int k, int j) { return (k * R + j) * W + col; };
     const int n = a.n, C = a.C;
     const double lambda = a.lambda;
     const bool leader = threadIdx.x == 0;
-    // jobs of this CTA: pencil blocks blockIdx.x, +gridDim.x, ..., each chunk 0 .. C-1
-    const int64_t mygroups = (a.ngroups > (int64_t)blockIdx.x) ? (a.ngroups - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-    const int64_t njobs = mygroups * C;
-    auto job_group = [&](int64_t j) { return (int64_t)blockIdx.x + (j / C) * (int64_t)gridDim.x; };
+    const int64_t njobs_all = a.ngroups * C;
+    const int64_t step = gridDim.x;
 
     if (leader) {
-        prefetch_tmap(&tmM);
-        prefetch_tmap(&tmH);
+        prefetch_tmap(&tm);
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
         fence_mbar_init();
     }
     __syncthreads();
     auto issue = [&](int64_t j, int buf) {  // leader only
-        const int64_t grp = job_group(j);
-        const int cc = (int)(j % C);
-        const bool edge = (cc == 0) || (cc == C - 1);
-        mbar_arrive_expect_tx(&full[buf], tile_tx + (edge ? halo_tx : 0u));
-        chunk_load<DIR>(Ub(buf), &tmM, grp, cc * L - 4, a, W, &full[buf]);
-        if (cc == 0) chunk_load<DIR>(Hb(buf), &tmH, grp, n - 4, a, W, &full[buf]);
-        else if (cc == C - 1) chunk_load<DIR>(Hb(buf), &tmH, grp, 0, a, W, &full[buf]);
+        mbar_arrive_expect_tx(&full[buf], tile_tx);
+        chunk_load<DIR>(Ub(buf), &tm, j / C, (int)(j % C) * L, a, W, &full[buf]);
     };
     // bit b: a load into buffer b is in flight (leader's bookkeeping) / parity to wait for on b
     uint32_t issued = 0, phase = 0;
     if (leader) {
-        for (int t = 0; t < 2; t++)
-            if (t < njobs) { issue(t, t); issued |= 1u << t; }
+        for (int t = 0; t < 2; t++) {
+            const int64_t jt = blockIdx.x + t * step;
+            if (jt < njobs_all) { issue(jt, t); issued |= 1u << t; }
+        }
     }
-    for (int64_t j = 0; j < njobs; j++) {
-        const int buf = (int)(j & 1);
-        const int64_t grp = job_group(j);
+    int it = 0;
+    for (int64_t j = blockIdx.x; j < njobs_all; j += step, it++) {
+        const int buf = it & 1;
+        const int64_t grp = j / C;
         const int cc = (int)(j % C);
-        bool ok = mbar_wait_cta(&full[buf], (phase >> buf) & 1);
+        const int c0 = cc * L;                    // first cell of the chunk
+        const int cend = (c0 + L < n) ? c0 + L : n;
+        const bool ok = mbar_wait_cta(&full[buf], (phase >> buf) & 1);
         if (!ok) {
             if (leader) {
                 atomicOr(a.err, 1u);
-                mbar_wait(&full[buf], (phase >> buf) & 1);
+                mbar_wait(&full[buf], (phase >> buf) & 1);  // one more bounded wait for the late tile
                 if ((issued >> (buf ^ 1)) & 1) mbar_wait(&full[buf ^ 1], (phase >> (buf ^ 1)) & 1);
             }
             return;
         }
         phase ^= 1u << buf;
         issued &= ~(1u << buf);
-        // this thread's cell: g = cc*L - 4 + r; rows before the pencil and past its end come from
-        // the halo slot, rows more than 4 past the end are idle
-        const int g = cc * L - 4 + r;
-        const bool act = r < Rr && g < n + 4;
-        const double *src;
-        int srow, srows;
-        if (g < 0) { src = Hb(buf); srow = g + 4; srows = 4; }
-        else if (g >= n) { src = Hb(buf); srow = g - n; srows = 4; }
-        else { src = Ub(buf); srow = r; srows = Rr; }
+        // this thread's cell g = c0 - 4 + r: left halo (side buffer, boundary cc), chunk (tile),
+        // right halo (side buffer, boundary cc + 1 mod C), or idle
+        const int g = c0 - 4 + r;
+        const bool act = g < cend + 4;
         double u0[5], u1[5];
+        if (g >= c0 && g < cend) {
+            const double *Ut = Ub(buf);
 #pragma unroll
-        for (int k = 0; k < 5; k++) u0[k] = act ? src[(slots[k] * srows + srow) * W + col] : 1.0;
+            for (int k = 0; k < 5; k++) u0[k] = Ut[(slots[k] * L + (g - c0)) * W + col];
+        } else if (act) {
+            const int b = (g < c0) ? cc : ((cc + 1 == C) ? 0 : cc + 1);
+            const int rr = (g < c0) ? r : 4 + (g - cend);
+            const double *sd = a.side + ((grp * C + b) * 5) * 8 * W;
+#pragma unroll
+            for (int k = 0; k < 5; k++) u0[k] = sd[(slots[k] * 8 + rr) * W + col];
+        } else {
+#pragma unroll
+            for (int k = 0; k < 5; k++) u0[k] = 1.0;
+        }
         V5<FT> keep;
 #pragma unroll
         for (int stage = 0; stage < 2; stage++) {
@@ -855,11 +876,14 @@ __global__ void __launch_bounds__(512, 2)
                 }
             }
             __syncthreads();
-            if (stage == 0 && leader && j + 2 < njobs) {
+            if (stage == 0 && leader) {
                 // every thread has read tile buf: request the job after next into it
-                fence_proxy_async_smem();
-                issue(j + 2, buf);
-                issued |= 1u << buf;
+                const int64_t jn = j + 2 * step;
+                if (jn < njobs_all) {
+                    fence_proxy_async_smem();
+                    issue(jn, buf);
+                    issued |= 1u << buf;
+                }
             }
             {
                 V5<FT> w, dl, dr, Lf;
@@ -891,38 +915,10 @@ __global__ void __launch_bounds__(512, 2)
             }
             __syncthreads();  // the planes are rewritten next
         }
-        // the next chunk of this block re-reads this chunk's last 4 outputs as its halo: its tile
-        // must have landed before they are written
-        if (cc < C - 1) {
-            ok = mbar_wait_cta(&full[buf ^ 1], (phase >> (buf ^ 1)) & 1);
-            if (!ok) {
-                if (leader) {
-                    atomicOr(a.err, 1u);
-                    mbar_wait(&full[buf ^ 1], (phase >> (buf ^ 1)) & 1);  // one more bounded wait for it
-                    if ((issued >> buf) & 1) mbar_wait(&full[buf], (phase >> buf) & 1);
-                }
-                return;
-            }
-        }
-        const bool out = act && r >= 4 && r < Rr - 4 && g < n;
-        double *base;
-        if (DIR == 1) base = a.q + grp * a.os;
-        else base = a.q + (grp % a.npw) * W + col + (grp / a.npw) * a.os;
-        if (out) {
-            if (cc == 0 && g < 4) {
+        if (g >= c0 && g < cend) {
+            double *base = a.q + chunk_base(a, DIR, W, grp, col);
 #pragma unroll
-                for (int k = 0; k < 5; k++) DEF[(k * 4 + g) * W + col] = u1[k];
-            } else {
-#pragma unroll
-                for (int k = 0; k < 5; k++) base[slots[k] * a.slab + (int64_t)g * a.rs] = u1[k];
-            }
-        }
-        if (cc == C - 1 && r >= 4 && r < 8) {
-            // the deferred first 4 outputs of this block (written by these same threads in chunk 0;
-            // this chunk's tile, which held them as its halo, has landed)
-            const int gd = r - 4;
-#pragma unroll
-            for (int k = 0; k < 5; k++) base[slots[k] * a.slab + (int64_t)gd * a.rs] = DEF[(k * 4 + gd) * W + col];
+            for (int k = 0; k < 5; k++) base[slots[k] * a.slab + (int64_t)g * a.rs] = u1[k];
         }
     }
 }

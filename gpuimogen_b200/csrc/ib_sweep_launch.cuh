@@ -114,37 +114,34 @@ int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const
 }
 
 // Chunked TMA pipeline (sweep_chunk_kernel) for pencils of more than 512 cells: W = 1, R = 256
-// (x rows) or W = 4, R = 128 (y/z pencils).  Returns IB_ERROR_NOIMPLEMENT (caller falls back)
-// when the grid does not meet TMA's rules: x rows of even length; y/z with W dividing nx.
+// (x rows) or W = 4, R = 128 (y/z pencils), after chunk_halo_kernel has copied the rows around the
+// chunk boundaries to scratch memory.  Returns IB_ERROR_NOIMPLEMENT (caller falls back) when the
+// grid does not meet TMA's rules: x rows of even length; y/z with W dividing nx.
 template <int METHOD, int SLOPE, typename FT, int DIR, int W, int R>
 int launch_chunk(double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c, cudaStream_t st)
 {
+    constexpr int L = R - 8;
     const int nx = grid[0], ny = grid[1], nz = grid[2];
     const int n = grid[DIR - 1];
     if (n <= 512) return IB_ERROR_NOIMPLEMENT;
     if (DIR == 1 && (n & 1)) return IB_ERROR_NOIMPLEMENT;
     if (DIR != 1 && ((nx & 1) || nx % W)) return IB_ERROR_NOIMPLEMENT;
     if (((uintptr_t)q & 15) || (slab * 8) % 16) return IB_ERROR_NOIMPLEMENT;
-    CUtensorMap tmM, tmH;
+    CUtensorMap tm;
     uint64_t dims[4], strides[3];
-    uint32_t boxM[4], boxH[4];
+    uint32_t box[4];
     int rank;
     ChunkArgs a;
     a.q = q;
     a.slab = slab;
     a.n = n;
-    a.C = (n + (R - 8) - 1) / (R - 8);
-    // full-length chunks: a job costs its tile's rows whatever its outputs, and an even split
-    // (shorter tiles, box rows not a multiple of 128 bytes) measured slower
-    a.Lr = R - 8;
-    a.Rr = R;
+    a.C = (n + L - 1) / L;
     a.lambda = lambda;
     if (DIR == 1) {
         rank = 3;
         dims[0] = nx; dims[1] = (uint64_t)ny * nz; dims[2] = 5;
         strides[0] = (uint64_t)nx * 8; strides[1] = (uint64_t)slab * 8;
-        boxM[0] = a.Rr; boxM[1] = 1; boxM[2] = 5;
-        boxH[0] = 4; boxH[1] = 1; boxH[2] = 5;
+        box[0] = L; box[1] = 1; box[2] = 5;
         a.rs = 1; a.os = nx; a.npw = 1;
         a.ngroups = (int64_t)ny * nz;
     } else {
@@ -154,18 +151,26 @@ int launch_chunk(double *q, int64_t slab, const int grid[3], double lambda, cons
         a.os = (DIR == 2) ? (int64_t)nx * ny : (int64_t)nx;
         dims[0] = nx; dims[1] = n; dims[2] = other; dims[3] = 5;
         strides[0] = (uint64_t)a.rs * 8; strides[1] = (uint64_t)a.os * 8; strides[2] = (uint64_t)slab * 8;
-        boxM[0] = W; boxM[1] = a.Rr; boxM[2] = 1; boxM[3] = 5;
-        boxH[0] = W; boxH[1] = 4; boxH[2] = 1; boxH[3] = 5;
+        box[0] = W; box[1] = L; box[2] = 1; box[3] = 5;
         a.npw = nx / W;
         a.ngroups = (int64_t)a.npw * other;
     }
     if (a.ngroups >= ((int64_t)1 << 31) / a.C) return IB_ERROR_NOIMPLEMENT;
-    int rc = encode_tmap_f64(&tmM, q, rank, dims, strides, boxM);
-    if (rc) return rc;
-    rc = encode_tmap_f64(&tmH, q, rank, dims, strides, boxH);
+    int rc = encode_tmap_f64(&tm, q, rank, dims, strides, box);
     if (rc) return rc;
     a.err = scratch().wait_flag();
     if (!a.err) return IB_ERROR_NOMEM;
+    // halo rows of every chunk boundary, copied before the sweep overwrites them
+    const int64_t nside = a.ngroups * a.C * 40 * W;
+    double *side = scratch().bytes((size_t)nside * sizeof(double));
+    if (!side) return IB_ERROR_NOMEM;
+    a.side = side;
+    {
+        const int hb = (int)std::min<int64_t>((nside + 255) / 256, (int64_t)8 * num_sms());
+        chunk_halo_kernel<DIR, W><<<hb, 256, 0, st>>>(a, L, side);
+        rc = check_launch();
+        if (rc) return rc;
+    }
     const int nt = W * R;
     const size_t shm = chunk_smem_bytes(W, R, (int)sizeof(FT));
     auto kern = sweep_chunk_kernel<METHOD, SLOPE, FT, DIR, W, R>;
@@ -179,15 +184,9 @@ int launch_chunk(double *q, int64_t slab, const int grid[3], double lambda, cons
     rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, shm));
     if (rc) return rc;
     if (per_sm < 1) return IB_ERROR_NOIMPLEMENT;
-    // as many resident CTAs as fit: a CTA's pencil blocks are latency-bound chains of chunks
-    int k = per_sm;
-    static const int force_k = [] {
-        const char *e = getenv("IMOGEN_B200_CHUNK_CTAS");  // resident CTAs per SM, overriding the choice
-        return (e && e[0] >= '1' && e[0] <= '8') ? e[0] - '0' : 0;
-    }();
-    if (force_k) k = std::min(force_k, per_sm);
-    const unsigned nblk = (unsigned)std::min<int64_t>((int64_t)k * num_sms(), a.ngroups);
-    kern<<<nblk, nt, shm, st>>>(tmM, tmH, a, c);
+    const int64_t njobs = a.ngroups * a.C;
+    const unsigned nblk = (unsigned)std::min<int64_t>((int64_t)per_sm * num_sms(), njobs);
+    kern<<<nblk, nt, shm, st>>>(tm, a, c);
     return check_launch();
 }
 
