@@ -714,20 +714,21 @@ __global__ void __launch_bounds__(512, 1)
 // rows: the chunk plus 4 rows of halo on each side (both SSPRK stages are recomputed on the halo).
 // x rows: W = 1, L = 248; y/z pencils: W = 4, L = 120 (32-byte box rows: 16-byte rows at the large
 // strides of long pencils are served poorly).
-//   * Independent jobs: before the sweep, chunk_halo_kernel copies the 8 rows around every chunk
-//     boundary (periodic: boundary 0 is rows n-4 .. 3) to a side buffer, and a job takes its halo
-//     rows from there.  No job reads what another writes, so the jobs of one pencil run on any
-//     CTAs in any order and the persistent grid deals them out evenly.
-//   * A job's L chunk rows arrive as one TMA box (rows past the pencil's end are filled and idle);
-//     the loads of the next two jobs are in flight while one is computed (double-buffered tiles,
-//     one mbarrier each, bounded waits).  Outputs are plain stores from registers.
-// Dynamic shared memory: 2 tiles of 40*L*W bytes (rounded to 128), the SSPRK sum u1 + u0 through
-// the second stage (40*R*W bytes: neither state stays in registers there), then 2 planes of
-// 5*R*W elements of FT.
+//   * Independent jobs: before the sweep, chunk_halo_kernel copies every job's 8 halo rows (the
+//     4 before its chunk and the 4 after, periodic) to a side buffer, contiguous per job, and a job
+//     takes its halo from there.  No job reads what another writes, so the jobs of one pencil run
+//     on any CTAs in any order and the persistent grid deals them out evenly.
+//   * A job's L chunk rows arrive as one TMA box (rows past the pencil's end are filled and idle)
+//     and its halo block as one untiled bulk copy, on the same mbarrier; the loads of the next two
+//     jobs are in flight while one is computed (double-buffered, bounded waits).  Outputs are
+//     plain stores from registers.
+// Dynamic shared memory: 2 tiles of 40*L*W bytes and 2 halo blocks of 320*W bytes (each rounded to
+// 128), the SSPRK sum u1 + u0 through the second stage (40*R*W bytes: neither state stays in
+// registers there), then 2 planes of 5*R*W elements of FT.
 // ------------------------------------------------------------------------------------------
 struct ChunkArgs {
     double *q;
-    const double *side;  // halo rows: [group][boundary][slab][8 rows][W]
+    const double *side;  // halo rows of every job: [group * C + chunk][slab][8 rows][W]
     int64_t slab;        // doubles between slabs
     int64_t rs;          // doubles between consecutive cells of a pencil
     int64_t os;          // doubles between consecutive pencils along the other axis (rows for x)
@@ -741,7 +742,8 @@ struct ChunkArgs {
 
 __host__ __device__ constexpr size_t chunk_smem_bytes(int W, int R, int ftsize)
 {
-    return 2 * (((size_t)40 * (R - 8) * W + 127) / 128 * 128) + (size_t)40 * R * W + (size_t)10 * R * W * ftsize;
+    return 2 * (((size_t)40 * (R - 8) * W + 127) / 128 * 128) + 2 * (((size_t)320 * W + 127) / 128 * 128) +
+           (size_t)40 * R * W + (size_t)10 * R * W * ftsize;
 }
 
 // First cell of pencil block grp, column col.
@@ -751,8 +753,8 @@ __device__ __forceinline__ int64_t chunk_base(const ChunkArgs &a, int DIR, int W
     return (grp % a.npw) * W + col + (grp / a.npw) * a.os;
 }
 
-// Side buffer: for every pencil block and chunk boundary b, rows (b*L - 4 .. b*L + 3) mod n of the
-// 5 slabs.  One thread per value.
+// Side buffer: for every job (pencil block grp, chunk cc), rows c0-4 .. c0-1 and cend .. cend+3
+// (mod n) of the 5 slabs, c0 = cc*L, cend = min(c0 + L, n).  One thread per value.
 template <int DIR, int W>
 __global__ void __launch_bounds__(256) chunk_halo_kernel(ChunkArgs a, int L, double *side)
 {
@@ -761,10 +763,11 @@ __global__ void __launch_bounds__(256) chunk_halo_kernel(ChunkArgs a, int L, dou
         const int col = (int)(t % W);
         const int rr = (int)((t / W) % 8);
         const int k = (int)((t / (8 * W)) % 5);
-        const int64_t gb = t / (40 * W);  // grp * C + b
-        const int b = (int)(gb % a.C);
-        const int64_t grp = gb / a.C;
-        int row = b * L - 4 + rr;
+        const int64_t job = t / (40 * W);  // grp * C + cc
+        const int cc = (int)(job % a.C);
+        const int64_t grp = job / a.C;
+        const int c0 = cc * L, cend = (c0 + L < a.n) ? c0 + L : a.n;
+        int row = (rr < 4) ? c0 - 4 + rr : cend + (rr - 4);
         if (row < 0) row += a.n;
         else if (row >= a.n) row -= a.n;
         side[t] = a.q[chunk_base(a, DIR, W, grp, col) + k * a.slab + (int64_t)row * a.rs];
@@ -787,12 +790,14 @@ __global__ void __launch_bounds__(512, 2)
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full[2];
     constexpr size_t tb = ((size_t)40 * L * W + 127) / 128 * 128;
-    // tile of buffer b (computed, not an indexed array, which would live in local memory)
+    constexpr size_t hb = ((size_t)320 * W + 127) / 128 * 128;
+    // tile and halo block of buffer b (computed, not indexed arrays, which would live in local memory)
     auto Ub = [&](int b) { return reinterpret_cast<double *>(smem_raw + b * tb); };
-    double *SS = reinterpret_cast<double *>(smem_raw + 2 * tb);
-    FT *SA = reinterpret_cast<FT *>(smem_raw + 2 * tb + (size_t)40 * R * W);
+    auto Hb = [&](int b) { return reinterpret_cast<double *>(smem_raw + 2 * tb + b * hb); };
+    double *SS = reinterpret_cast<double *>(smem_raw + 2 * tb + 2 * hb);
+    FT *SA = reinterpret_cast<FT *>(smem_raw + 2 * tb + 2 * hb + (size_t)40 * R * W);
     FT *SB = SA + 5 * R * W;
-    constexpr uint32_t tile_tx = 40u * L * W;
+    constexpr uint32_t tile_tx = 40u * L * W + 320u * W;
     constexpr int s0 = slot_of<METHOD, DIR>(0), s1 = slot_of<METHOD, DIR>(1), s2 = slot_of<METHOD, DIR>(2),
                   s3 = slot_of<METHOD, DIR>(3), s4 = slot_of<METHOD, DIR>(4);
     const int slots[5] = {s0, s1, s2, s3, s4};
@@ -816,6 +821,7 @@ __global__ void __launch_bounds__(512, 2)
     auto issue = [&](int64_t j, int buf) {  // leader only
         mbar_arrive_expect_tx(&full[buf], tile_tx);
         chunk_load<DIR>(Ub(buf), &tm, j / C, (int)(j % C) * L, a, W, &full[buf]);
+        bulk_load(Hb(buf), a.side + j * 40 * W, 320u * W, &full[buf]);
     };
     // bit b: a load into buffer b is in flight (leader's bookkeeping) / parity to wait for on b
     uint32_t issued = 0, phase = 0;
@@ -853,11 +859,10 @@ __global__ void __launch_bounds__(512, 2)
 #pragma unroll
             for (int k = 0; k < 5; k++) u0[k] = Ut[(slots[k] * L + (g - c0)) * W + col];
         } else if (act) {
-            const int b = (g < c0) ? cc : ((cc + 1 == C) ? 0 : cc + 1);
             const int rr = (g < c0) ? r : 4 + (g - cend);
-            const double *sd = a.side + ((grp * C + b) * 5) * 8 * W;
+            const double *H = Hb(buf);
 #pragma unroll
-            for (int k = 0; k < 5; k++) u0[k] = sd[(slots[k] * 8 + rr) * W + col];
+            for (int k = 0; k < 5; k++) u0[k] = H[(slots[k] * 8 + rr) * W + col];
         } else {
 #pragma unroll
             for (int k = 0; k < 5; k++) u0[k] = 1.0;

@@ -108,6 +108,16 @@ __device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, i
         : "memory");
 }
 
+// Untiled bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned) from global
+// memory into this CTA's shared memory, completing on `bar`.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"((uint64_t)src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
 // Tiled TMA stores from this CTA's shared memory (bulk-group completion).
 __device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, const void *src, int c0, int c1, int c2)
 {
