@@ -8,6 +8,8 @@ Produces, next to this file:
                             product build instead contracts multiply-adds and replaces a few
                             divisions by reciprocals or comparisons (same mathematics, last-bit
                             differences), checked against the oracle within a tolerance.
+  imogen_run                the standalone driver (driver/imogen_run.cpp), host code linked
+                            against the product library through its C ABI only.
 
 Usage: python -m gpuimogen_b200.build [--force] [--only product|strict]
 """
@@ -94,9 +96,33 @@ def build_variant(name, force=False, jobs=None):
     return out
 
 
+DRIVER_SRC = os.path.join(HERE, "driver", "imogen_run.cpp")
+
+
+def build_driver(force=False):
+    """The standalone driver: host C++ against the product library (runtime path $ORIGIN)."""
+    lib = build_variant("product")
+    out = os.path.join(HERE, "imogen_run")
+    newest = max(os.path.getmtime(DRIVER_SRC), os.path.getmtime(lib),
+                 os.path.getmtime(os.path.join(ROOT, "include", "imogen_b200.h")))
+    if not force and os.path.exists(out) and os.path.getmtime(out) >= newest:
+        return out
+    tmp = out + ".tmp"
+    cmd = [NVCC, "-std=c++17", "-O2", "-I" + os.path.join(ROOT, "include"), DRIVER_SRC, "-o", tmp,
+           "-L" + HERE, "-limogen_b200", "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("driver build failed:\n%s\n%s" % (" ".join(cmd), r.stderr))
+    os.replace(tmp, out)
+    return out
+
+
 def build(force=False, only=None):
     names = [only] if only else list(VARIANTS)
-    return [build_variant(n, force=force) for n in names]
+    out = [build_variant(n, force=force) for n in names]
+    if only in (None, "product"):
+        out.append(build_driver(force=force))
+    return out
 
 
 if __name__ == "__main__":
