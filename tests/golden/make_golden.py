@@ -14,7 +14,7 @@ Boundary conditions are limited to circular, const and mirror: the reference's o
 extrapolation kernels write outside their rows (cudaStatics.cu / boundaryConds.cu), so they are not
 run here.
 
-Usage: python tests/golden/make_golden.py OUTDIR [--etdrk2-only]
+Usage: python tests/golden/make_golden.py OUTDIR [--etdrk2-only | --cases=name1,name2]
 """
 import ctypes
 import json
@@ -65,6 +65,9 @@ FLUID_CASES = [
     ("sod_hll_const", "sod", (256, 1, 1), 1, "ospre", 1.4, -1.0, ["const"] * 6, 0.4, 25),
     ("sod_hllc_const", "sod", (256, 1, 1), 2, "mc", 1.4, -1.0, ["const"] * 6, 0.4, 25),
     ("sod_xj_const", "sod", (256, 1, 1), 3, "ospre", 1.4, -1.0, ["const"] * 6, 0.4, 25),
+    # 100 iterations: the FP64 drop-in's parity bound is stated after 100 steps
+    ("kh_hllc_mc_100", "kh", (20, 16, 12), 2, "mc", 5 / 3.0, -1.0, ["circular"] * 6, 0.4, 100),
+    ("jumpy_hll_ospre_100", "jumpy", (16, 12, 10), 1, "ospre", 1.4, -1.0, ["circular"] * 6, 0.3, 100),
 ]
 # No multi-dimensional Xin-Jin case: on a 32x32x1 periodic grid the reference's Xin-Jin prediction
 # kernel (cukern_XinJinHydro_step, cudaFluidStep.cu:421, launched with a 32x4 block) made an illegal
@@ -125,13 +128,22 @@ def etdrk2_golden(outdir):
     print("wrote drag_etdrk2", flush=True)
 
 
-def main(outdir, only=None):
+def main(outdir, only=None, cases=None):
+    """only="etdrk2": the ETDRK2 drag vectors alone; cases: run only these fluid cases (their
+    entries are merged into an existing index.json) and nothing else."""
     os.makedirs(outdir, exist_ok=True)
     if only == "etdrk2":
         etdrk2_golden(outdir)
         return
     index = {}
+    if cases:
+        ipath = os.path.join(outdir, "index.json")
+        if os.path.exists(ipath):
+            with open(ipath) as f:
+                index = json.load(f)
     for name, gen, shape, method, limiter, gamma, c_iso, bc, cfl, niter in FLUID_CASES:
+        if cases and name not in cases:
+            continue
         q0 = make_input(gen, shape, gamma)
         h = np.array([1.0 / s for s in shape])
         bca = (ctypes.c_int * 6)(*[BC[b] for b in bc])
@@ -150,6 +162,10 @@ def main(outdir, only=None):
         np.savez_compressed(os.path.join(outdir, name + ".npz"), meta=json.dumps(meta), **rec)
         index[name] = meta
         print("wrote", name, flush=True)
+    if cases:
+        with open(os.path.join(outdir, "index.json"), "w") as f:
+            json.dump(index, f, indent=1)
+        return
 
     # CFL timesteps
     cfl_rec = {}
@@ -203,5 +219,6 @@ def main(outdir, only=None):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    sel = [a.split("=", 1)[1].split(",") for a in sys.argv[1:] if a.startswith("--cases=")]
     main(args[0] if args else os.path.dirname(os.path.abspath(__file__)),
-         only="etdrk2" if "--etdrk2-only" in sys.argv else None)
+         only="etdrk2" if "--etdrk2-only" in sys.argv else None, cases=sel[0] if sel else None)
