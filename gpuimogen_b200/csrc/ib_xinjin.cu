@@ -3,61 +3,70 @@
 //
 // The reference needs the maximum of |v|+c_s over the whole swept row before each stage, so it
 // runs freeze / predictor / freeze / corrector as four kernels with a host reduction in
-// between (MGA_globalReduceDimension, cudaCommon.cu:919-1004).  Here one CTA owns one pencil:
-// it stages the pencil in shared memory, reduces the freezing speed in-block, and runs both
-// stages, so a sweep is one launch with one read and one write of the state.
+// between (MGA_globalReduceDimension, cudaCommon.cu:919-1004).  Here one CTA owns one pencil (or
+// 2 to 4 adjacent y/z pencils): it keeps them in registers, reduces each freezing speed in-block,
+// and runs both stages, so a sweep is one launch with one read and one write of the state.
 #include "ib_internal.cuh"
 
 namespace ib {
 
-__device__ __forceinline__ double block_max_keep(double v, double *red)
+// Maximum over the pencil of column `col` (W interleaved pencils per block), ignoring NaN
+// candidates as the reference's `(a > b) ? a : b` tree does.
+template <int W>
+__device__ __forceinline__ double block_max_keep(double v, double *red, int col)
 {
-    // maximum ignoring NaN candidates, as the reference's `(a > b) ? a : b` tree
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
+    for (int o = 16; o >= W; o >>= 1) {
         double w = __shfl_xor_sync(0xffffffffu, v, o);
         v = (w > v) ? w : v;
     }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     __syncthreads();
-    if (lane == 0) red[wid] = v;
+    if (lane < W) red[wid * W + lane] = v;
     __syncthreads();
     double m = 0.0;
-    for (int w = 0; w < nw; w++) m = (red[w] > m) ? red[w] : m;
+    for (int w = 0; w < nw; w++) m = (red[w * W + col] > m) ? red[w * W + col] : m;
     return m;
 }
 
-// Uses memory slab 2 (px) as the transported momentum whatever the sweep direction, as the
-// reference's freeze kernel does.
-__device__ __forceinline__ double freeze_cell(const double *U, int n, int i, double gamma, double gm1)
+// Freezing speed |v| + c_s of one cell.  Uses memory slab 2 (px) as the transported momentum
+// whatever the sweep direction, as the reference's freeze kernel does.
+__device__ __forceinline__ double freeze_cell(const double (&X)[5], double gamma, double gm1)
 {
-    double invrho = 1.0 / U[i];
-    double psq = U[3 * n + i];
-    double px = U[4 * n + i];
+    double invrho = 1.0 / X[0];
+    double psq = X[3];
+    double px = X[4];
     psq = psq * psq + px * px;
-    px = U[2 * n + i];
+    px = X[2];
     psq += px * px;
-    double P = (U[n + i] - .5 * psq * invrho) * gm1;
+    double P = (X[1] - .5 * psq * invrho) * gm1;
     return fabs(px) * invrho + sqrt(gamma * P * invrho);
 }
 
-template <int FLIM>
-__global__ void __launch_bounds__(256) xj_pencil_kernel(double *q, int64_t slab, int nx, int ny, int nz, int dir,
-                                                        double lambda, double gamma, double minmass, double mintemp)
+// W adjacent pencils per block (W = 1 for x rows; y/z pencils take W = 2 or 4 when nx allows it,
+// so that the loads of a warp cover 16- or 32-byte runs of x instead of single doubles a row or a
+// plane apart).  Thread t works on column t % W and cells t / W + m * S (m < CPT,
+// S = blockDim / W); a cell's five conserved variables stay in registers through both stages and
+// only the relaxation fluxes L = C q - F, R = C q + F pass through shared memory ([5][n][W]
+// each), so a stage costs the freezing-speed reduction and one (predictor) or three (corrector)
+// barriers.  RELOAD (x rows): the corrector re-reads its base state from memory, coalesced and
+// L2-resident, rather than keep it in registers; fewer spills made x 0.85 -> 0.82 ms at 256^3 and
+// 0.30 -> 0.27 ms at 2048^2, while the strided y/z loads measured slower that way.
+template <int FLIM, int W, int CPT, bool RELOAD>
+__global__ void __launch_bounds__(1024) xj_pencil_kernel(double *q, int64_t slab, int nx, int ny, int nz, int dir,
+                                                         double lambda, double gamma, double minmass, double mintemp)
 {
     extern __shared__ __align__(16) double sm[];
+    __shared__ double red[32 * W];
     const int n = (dir == 1) ? nx : (dir == 2 ? ny : nz);
-    double *U0 = sm;            // [5][n] fluid
-    double *U1 = U0 + 5 * n;    // [5][n] prediction, then corrected output
-    double *Lb = U1 + 5 * n;    // [n] left-going flux of the current component
-    double *Rb = Lb + n;        // [n] right-going
-    double *dLb = Rb + n;       // [n]
-    double *dRb = dLb + n;      // [n]
-    double *Pv = dRb + n;       // [n] pressure
-    double *Vx = Pv + n;        // [n] normal velocity
-    __shared__ double red[32];
+    const int NW = n * W;
+    double *Lb = sm;            // [5][n][W]
+    double *Rb = Lb + 5 * NW;   // [5][n][W]
 
-    const int64_t p = blockIdx.x;
+    const int col = (W == 1) ? 0 : (int)(threadIdx.x % W);
+    const int r0 = (int)(threadIdx.x / W), S = (int)(blockDim.x / W);
+    auto IX = [&](int k, int i) { return (k * n + i) * W + col; };
+    const int64_t p = (int64_t)blockIdx.x * W + col;  // this column's pencil
     int64_t base, stride;
     if (dir == 1) { base = p * nx; stride = 1; }
     else if (dir == 2) { base = (p % nx) + (int64_t)nx * ny * (p / nx); stride = nx; }
@@ -65,79 +74,116 @@ __global__ void __launch_bounds__(256) xj_pencil_kernel(double *q, int64_t slab,
     const int nslot = 1 + dir;
     const double gm1 = gamma - 1.0;
 
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
-        for (int k = 0; k < 5; k++) U0[k * n + i] = q[k * slab + base + i * stride];
-    __syncthreads();
-
-    for (int stage = 0; stage < 2; stage++) {
-        const double *Qin = (stage == 0) ? U0 : U1;
-        const double lam = (stage == 0) ? 0.25 * lambda : 0.5 * lambda;
-        // freezing speed of the row
-        double cm = 0.0;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            double v = freeze_cell(Qin, n, i, gamma, gm1);
-            cm = (v > cm) ? v : cm;
-        }
-        const double Cf = block_max_keep(cm, red);
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            double q0 = Qin[i], q1 = Qin[n + i], q2 = Qin[2 * n + i], q3 = Qin[3 * n + i], q4 = Qin[4 * n + i];
-            Pv[i] = gm1 * (q1 - .5 * (q4 * q4 + q3 * q3 + q2 * q2) / q0);
-            Vx[i] = Qin[nslot * n + i] / q0;
-        }
-        // proposed values, one component at a time; kept in registers per thread (<= 8 cells)
-        double prop[5][8];
-        __syncthreads();
-        for (int k = 0; k < 5; k++) {
-            for (int i = threadIdx.x; i < n; i += blockDim.x) {
-                double qk = Qin[k * n + i], w;
-                if (k == 0) w = Qin[nslot * n + i];
-                else if (k == 1) w = Vx[i] * (qk + Pv[i]);
-                else if (k == nslot) w = Vx[i] * qk + Pv[i];
-                else w = Vx[i] * qk;
-                Lb[i] = (Cf * qk - w);
-                Rb[i] = (Cf * qk + w);
-            }
-            __syncthreads();
-            if (stage == 1) {
-                for (int i = threadIdx.x; i < n; i += blockDim.x) {
-                    int il = (i == 0) ? n - 1 : i - 1;
-                    dLb[i] = 0.5 * (Lb[i] - Lb[il]);
-                    dRb[i] = 0.5 * (Rb[i] - Rb[il]);
-                }
-                __syncthreads();
-                double nl[8], nr[8];
-                int m = 0;
-                for (int i = threadIdx.x; i < n; i += blockDim.x, m++) {
-                    int ir = (i == n - 1) ? 0 : i + 1;
-                    nl[m] = Lb[i] - flux_limit<FLIM>(dLb[i], dLb[ir]);
-                    nr[m] = Rb[i] + flux_limit<FLIM>(dRb[i], dRb[ir]);
-                }
-                __syncthreads();
-                m = 0;
-                for (int i = threadIdx.x; i < n; i += blockDim.x, m++) { Lb[i] = nl[m]; Rb[i] = nr[m]; }
-                __syncthreads();
-            }
-            int m = 0;
-            for (int i = threadIdx.x; i < n; i += blockDim.x, m++) {
-                int il = (i == 0) ? n - 1 : i - 1, ir = (i == n - 1) ? 0 : i + 1;
-                double b = (stage == 0) ? Qin[k * n + i] : U0[k * n + i];
-                prop[k][m] = b - lam * (Rb[i] - Rb[il] - Lb[ir] + Lb[i]);
-            }
-            __syncthreads();
-        }
-        // floors (cudaFluidStep.cu:2620-2629) and store
-        int m = 0;
-        for (int i = threadIdx.x; i < n; i += blockDim.x, m++) {
-            double p0 = prop[0][m], p1 = prop[1][m], p2 = prop[2][m], p3 = prop[3][m], p4 = prop[4][m];
-            p0 = (p0 < minmass) ? minmass : p0;
-            double w = .5 * (p2 * p2 + p3 * p3 + p4 * p4) / p0;
-            if ((p1 - w) < p0 * mintemp) p1 = w + p0 * mintemp;
-            U1[i] = p0; U1[n + i] = p1; U1[2 * n + i] = p2; U1[3 * n + i] = p3; U1[4 * n + i] = p4;
-        }
-        __syncthreads();
+    double u0[CPT][5], u1[CPT][5];
+#pragma unroll
+    for (int m = 0; m < CPT; m++) {
+        const int i = r0 + m * S;
+#pragma unroll
+        for (int k = 0; k < 5; k++) u0[m][k] = (i < n) ? q[k * slab + base + i * stride] : 1.0;
     }
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
-        for (int k = 0; k < 5; k++) q[k * slab + base + i * stride] = U1[k * n + i];
+
+#pragma unroll
+    for (int stage = 0; stage < 2; stage++) {
+        const double lam = (stage == 0) ? 0.25 * lambda : 0.5 * lambda;
+        // freezing speed of the pencil (cudaFluidStep.cu:2867-2941 + the global max)
+        double cm = 0.0;
+#pragma unroll
+        for (int m = 0; m < CPT; m++) {
+            if (r0 + m * S < n) {
+                double v = freeze_cell((stage == 0) ? u0[m] : u1[m], gamma, gm1);
+                cm = (v > cm) ? v : cm;
+            }
+        }
+        const double Cf = block_max_keep<W>(cm, red, col);
+        // relaxation fluxes of every component (cudaFluidStep.cu:2470-2520)
+#pragma unroll
+        for (int m = 0; m < CPT; m++) {
+            const int i = r0 + m * S;
+            if (i < n) {
+                const double *Q = (stage == 0) ? u0[m] : u1[m];
+                const double q0 = Q[0], q1 = Q[1], q2 = Q[2], q3 = Q[3], q4 = Q[4];
+#ifdef IB_STRICT_ARITH
+                const double Pv = gm1 * (q1 - .5 * (q4 * q4 + q3 * q3 + q2 * q2) / q0);
+                const double Vx = Q[nslot] / q0;
+#else  // one reciprocal of the density for pressure and velocity
+                const double ir = 1.0 / q0;
+                const double Pv = gm1 * (q1 - .5 * (q4 * q4 + q3 * q3 + q2 * q2) * ir);
+                const double Vx = Q[nslot] * ir;
+#endif
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    const double qk = Q[k];
+                    double w;
+                    if (k == 0) w = Q[nslot];
+                    else if (k == 1) w = Vx * (qk + Pv);
+                    else if (k == nslot) w = Vx * qk + Pv;
+                    else w = Vx * qk;
+                    Lb[IX(k, i)] = (Cf * qk - w);
+                    Rb[IX(k, i)] = (Cf * qk + w);
+                }
+            }
+        }
+        __syncthreads();
+        if (stage == 1) {
+            // limited second-order fluxes (cudaFluidStep.cu:2560-2600), written back in place
+            double nl[CPT][5], nr[CPT][5];
+#pragma unroll
+            for (int m = 0; m < CPT; m++) {
+                const int i = r0 + m * S;
+                if (i < n) {
+                    const int il = (i == 0) ? n - 1 : i - 1, ir = (i == n - 1) ? 0 : i + 1;
+#pragma unroll
+                    for (int k = 0; k < 5; k++) {
+                        const double Lm = Lb[IX(k, il)], L0 = Lb[IX(k, i)], Lp = Lb[IX(k, ir)];
+                        const double Rm = Rb[IX(k, il)], R0 = Rb[IX(k, i)], Rp = Rb[IX(k, ir)];
+                        const double dL0 = 0.5 * (L0 - Lm), dLp = 0.5 * (Lp - L0);
+                        const double dR0 = 0.5 * (R0 - Rm), dRp = 0.5 * (Rp - R0);
+                        nl[m][k] = L0 - flux_limit<FLIM>(dL0, dLp);
+                        nr[m][k] = R0 + flux_limit<FLIM>(dR0, dRp);
+                    }
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < CPT; m++) {
+                const int i = r0 + m * S;
+                if (i < n) {
+#pragma unroll
+                    for (int k = 0; k < 5; k++) { Lb[IX(k, i)] = nl[m][k]; Rb[IX(k, i)] = nr[m][k]; }
+                }
+            }
+            __syncthreads();
+        }
+        // update and floors (cudaFluidStep.cu:2610-2629)
+#pragma unroll
+        for (int m = 0; m < CPT; m++) {
+            const int i = r0 + m * S;
+            if (i < n) {
+                const int il = (i == 0) ? n - 1 : i - 1, ir = (i == n - 1) ? 0 : i + 1;
+                double pr[5];
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    // the block's own pencils are unchanged in memory until the final store
+                    const double b = (RELOAD && stage == 1) ? q[k * slab + base + i * stride] : u0[m][k];
+                    pr[k] = b - lam * (Rb[IX(k, i)] - Rb[IX(k, il)] - Lb[IX(k, ir)] + Lb[IX(k, i)]);
+                }
+                double p0 = pr[0], p1 = pr[1];
+                const double p2 = pr[2], p3 = pr[3], p4 = pr[4];
+                p0 = (p0 < minmass) ? minmass : p0;
+                double w = .5 * (p2 * p2 + p3 * p3 + p4 * p4) / p0;
+                if ((p1 - w) < p0 * mintemp) p1 = w + p0 * mintemp;
+                u1[m][0] = p0; u1[m][1] = p1; u1[m][2] = p2; u1[m][3] = p3; u1[m][4] = p4;
+            }
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < CPT; m++) {
+        const int i = r0 + m * S;
+        if (i < n) {
+#pragma unroll
+            for (int k = 0; k < 5; k++) q[k * slab + base + i * stride] = u1[m][k];
+        }
+    }
 }
 
 int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
@@ -145,33 +191,59 @@ int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3
 {
     const int n = grid[dir - 1];
     const int64_t N = (int64_t)grid[0] * grid[1] * grid[2];
-    if (n > 2048) return IB_ERROR_NOIMPLEMENT;  // per-thread proposal registers cover 8 cells x 256 threads
-    const size_t shm = (size_t)16 * n * sizeof(double);
-    const size_t shm_cap = 227 * 1024 - 1024;  // opt-in limit minus the kernel's static shared memory
-    if (shm > shm_cap) return IB_ERROR_NOIMPLEMENT;
+    if (n > 2048) return IB_ERROR_NOIMPLEMENT;  // 1024 threads x 2 cells per pencil block
     const int64_t np = N / n;
     const double mintemp = 1e-5 / (gamma - 1);
-    int nt = std::min(256, ((n + 31) / 32) * 32);
-    if ((n + nt - 1) / nt > 8) nt = 256;
-#define IB_XJ(F)                                                                                              \
+    // y/z pencils: W adjacent pencils per block when nx allows it (IMOGEN_B200_XJW caps W)
+    static const int xjw = [] {
+        const char *e = getenv("IMOGEN_B200_XJW");
+        return (e && e[0] >= '1' && e[0] <= '4') ? e[0] - '0' : 4;
+    }();
+    // Blocks of at most 512 threads run two or more per SM and measured faster than 1024-thread
+    // blocks of wider runs (256^3: y 1.33 ms at W = 2 against 1.39 at W = 4; 128^3: W = 4 0.146 ms,
+    // W = 8 0.171); W = 2 in a 1024-thread block still beats W = 1 (512 x 512 x 64, y: 1.55 / 1.78).
+    int W = 1;
+    if (dir > 1) {
+        for (int w = 4; w >= 2; w >>= 1)
+            if (w <= xjw && grid[0] % w == 0 && n * w <= 512) { W = w; break; }
+        if (W == 1 && xjw >= 2 && grid[0] % 2 == 0 && n * 2 <= 1024) W = 2;
+    }
+    const int CPT = (n * W > 1024) ? 2 : 1;
+    const int rows = (n + CPT - 1) / CPT;
+    const int nt = ((rows * W + 31) / 32) * 32;
+    const size_t shm = (size_t)10 * n * W * sizeof(double);
+    const size_t shm_cap = 227 * 1024 - 2048;  // opt-in limit minus the kernel's static shared memory
+    if (shm > shm_cap) return IB_ERROR_NOIMPLEMENT;
+    const unsigned nblk = (unsigned)(np / W);
+#define IB_XJ(F, WW, CC, RR)                                                                                  \
     do {                                                                                                      \
         static bool attr_set = false;                                                                         \
         if (!attr_set) {                                                                                      \
-            int rc_ = check_cuda(cudaFuncSetAttribute(xj_pencil_kernel<F>,                                    \
+            int rc_ = check_cuda(cudaFuncSetAttribute(xj_pencil_kernel<F, WW, CC, RR>,                        \
                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm_cap)); \
             if (rc_) return rc_;                                                                              \
             attr_set = true;                                                                                  \
         }                                                                                                     \
-        xj_pencil_kernel<F><<<(unsigned)np, nt, shm, st>>>(q, slab, grid[0], grid[1], grid[2], dir, lambda, gamma, \
-                                                           rho_min, mintemp);                                 \
+        xj_pencil_kernel<F, WW, CC, RR><<<nblk, nt, shm, st>>>(q, slab, grid[0], grid[1], grid[2], dir,       \
+                                                               lambda, gamma, rho_min, mintemp);              \
+    } while (0)
+#define IB_XJ_W(F)                                            \
+    do {                                                      \
+        if (W == 4) IB_XJ(F, 4, 1, false);                    \
+        else if (W == 2) IB_XJ(F, 2, 1, false);               \
+        else if (CPT == 2 && dir == 1) IB_XJ(F, 1, 2, true);  \
+        else if (CPT == 2) IB_XJ(F, 1, 2, false);             \
+        else if (dir == 1) IB_XJ(F, 1, 1, true);              \
+        else IB_XJ(F, 1, 1, false);                           \
     } while (0)
     switch (flim) {
-    case IB_FLUX_OSPRE: IB_XJ(IB_FLUX_OSPRE); break;
-    case IB_FLUX_VANLEER: IB_XJ(IB_FLUX_VANLEER); break;
-    case IB_FLUX_MINMOD: IB_XJ(IB_FLUX_MINMOD); break;
-    case IB_FLUX_SUPERBEE: IB_XJ(IB_FLUX_SUPERBEE); break;
-    default: IB_XJ(IB_FLUX_ZERO); break;
+    case IB_FLUX_OSPRE: IB_XJ_W(IB_FLUX_OSPRE); break;
+    case IB_FLUX_VANLEER: IB_XJ_W(IB_FLUX_VANLEER); break;
+    case IB_FLUX_MINMOD: IB_XJ_W(IB_FLUX_MINMOD); break;
+    case IB_FLUX_SUPERBEE: IB_XJ_W(IB_FLUX_SUPERBEE); break;
+    default: IB_XJ_W(IB_FLUX_ZERO); break;
     }
+#undef IB_XJ_W
 #undef IB_XJ
     return check_launch();
 }
