@@ -35,6 +35,9 @@ GAMMA = 5.0 / 3.0
 CFL = 0.4
 METHOD = 2  # HLLC
 METRIC = "Mcell-updates/s"
+# device copies of the state in the end-to-end leg: a buffer holds a step's upload, compute and
+# download in turn, so with three the upload of step i+1 never waits for step i-1's download
+E2E_BUFFERS = int(os.environ.get("IMOGEN_BENCH_E2E_BUFFERS", "3"))
 # DRAM bytes per cell of one sweep launch (dram__bytes_read.sum + dram__bytes_write.sum / cells),
 # from the ncu capture of this workload's three sweep kernels summarised in
 # profiles/sweep_kernels_kh256_fp64.md (KH 256^3, state larger than L2).
@@ -317,17 +320,20 @@ def main():
     # Every step is one job: its input state is copied in from pinned host memory, the step runs
     # through the public API (run_iteration: CFL timestep read to the host, six sweeps), and its
     # result state is copied back out.  Uploads and downloads have their own streams and the
-    # device state is double-buffered, so step i's compute overlaps step i+1's upload and step
-    # i-1's download (the copy engines and the SMs work at once).  Timed from the first upload's
+    # device state has E2E_BUFFERS copies, so step i's compute overlaps step i+1's upload and
+    # step i-1's download (the copy engines and the SMs work at once).  Timed from the first upload's
     # start to the last download's end (CUDA events; all streams of this device).
-    e2e_steps = max(2, min(args.steps, 10))
+    # at least 20 steps, so that the first upload and the last download (not overlapped with
+    # anything) weigh as little as in a long run of the same pipeline
+    e2e_steps = max(20, min(args.steps, 40))
+    NB = E2E_BUFFERS
     pinned_in = torch.from_numpy(q0).pin_memory()
-    pinned_out = [torch.empty_like(pinned_in).pin_memory() for _ in range(2)]
-    bufs = [fl, ib.Fluid(shape, q=torch.empty_like(fl.q), gamma=GAMMA)]
+    pinned_out = [torch.empty_like(pinned_in).pin_memory() for _ in range(NB)]
+    bufs = [fl] + [ib.Fluid(shape, q=torch.empty_like(fl.q), gamma=GAMMA) for _ in range(NB - 1)]
     s_up, s_down = torch.cuda.Stream(), torch.cuda.Stream()
-    up_done = [torch.cuda.Event() for _ in range(2)]
-    comp_done = [torch.cuda.Event() for _ in range(2)]
-    down_done = [torch.cuda.Event() for _ in range(2)]
+    up_done = [torch.cuda.Event() for _ in range(NB)]
+    comp_done = [torch.cuda.Event() for _ in range(NB)]
+    down_done = [torch.cuda.Event() for _ in range(NB)]
     tm2 = ib.TimeManager(cfl=CFL)
     torch.cuda.synchronize()
     barrier()
@@ -335,9 +341,9 @@ def main():
     b = torch.cuda.Event(enable_timing=True)
 
     def upload(i):
-        k = i % 2
+        k = i % NB
         with torch.cuda.stream(s_up):
-            if i >= 2:
+            if i >= NB:
                 s_up.wait_event(down_done[k])   # buffer k's previous result has been read out
             bufs[k].q.copy_(pinned_in, non_blocking=True)
             up_done[k].record(s_up)
@@ -345,7 +351,7 @@ def main():
     a.record(s_up)
     upload(0)
     for i in range(e2e_steps):
-        k = i % 2
+        k = i % NB
         if i + 1 < e2e_steps:
             upload(i + 1)                       # queued before this step's compute blocks the host
         stream.wait_event(up_done[k])
@@ -382,8 +388,8 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": "Mcell-updates/s", "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes + 8, "steps": e2e_steps,
-                    "copies": "own streams, double-buffered device state (upload i+1 and download i-1 "
-                              "overlap step i)"},
+                    "copies": "own streams, %d device copies of the state (upload i+1 and download i-1 "
+                              "overlap step i)" % NB},
             "gpu_launches": launches,
             "clocks": clocks,
         }

@@ -85,14 +85,28 @@ unsigned int *Scratch::cfl_counter()
     return counter_;
 }
 
+// The CFL kernel's last block writes the timestep straight into pinned, mapped host memory, so
+// reading it back needs no copy-engine transfer: a device-to-host copy would queue behind any
+// large download the caller has running on another stream (a 671 MB state read-out held each
+// timestep read for ~13 ms) while the kernel's store does not.
 double *Scratch::cfl_tau()
 {
     std::lock_guard<std::mutex> g(g_scratch_mu);
     if (!tau_) {
-        if (cudaMalloc(&tau_, sizeof(double)) != cudaSuccess) { tau_ = nullptr; return nullptr; }
+        void *h = nullptr, *d = nullptr;
+        if (cudaHostAlloc(&h, sizeof(double), cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess)
+            return nullptr;
+        if (cudaHostGetDevicePointer(&d, h, 0) != cudaSuccess) {
+            cudaFreeHost(h);
+            return nullptr;
+        }
+        tau_host_ = static_cast<double *>(h);
+        tau_ = static_cast<double *>(d);
     }
     return tau_;
 }
+
+volatile double *Scratch::cfl_tau_host() { return tau_host_; }
 
 unsigned int *Scratch::wait_flag()
 {
@@ -358,9 +372,12 @@ static int cfl_common(const ib_fluid *fluid, const double *cs, double gamma, con
     if (!tau) return IB_ERROR_NOMEM;
     const int grid[3] = {fluid->grid.nx, fluid->grid.ny, fluid->grid.nz};
     if ((rc = launch_cfl(fluid->q, cs, fluid->grid.slab_pitch, grid, geo, method, gamma, tau, st))) return rc;
-    if (tau_host) {
+    if (tau_host && tau_device) {
         if ((rc = check_cuda(cudaMemcpyAsync(tau_host, tau, sizeof(double), cudaMemcpyDeviceToHost, st)))) return rc;
         if ((rc = check_cuda(cudaStreamSynchronize(st)))) return rc;
+    } else if (tau_host) {  // host-mapped slot: the kernel's store is visible once the stream is done
+        if ((rc = check_cuda(cudaStreamSynchronize(st)))) return rc;
+        *tau_host = *scratch().cfl_tau_host();
     }
     return IB_SUCCESSFUL;
 }

@@ -21,7 +21,8 @@ class Scratch {
 public:
     double *cfl_partial(int nblocks);
     unsigned int *cfl_counter();
-    double *cfl_tau();
+    double *cfl_tau();        // device address of the host-mapped timestep slot
+    volatile double *cfl_tau_host();  // the same slot as the host sees it (after cfl_tau())
     double *bytes(size_t nbytes);  // general scratch (reused between calls on the device)
     unsigned int *wait_flag();     // set by a kernel whose bounded wait ran out (zeroed once)
     unsigned int *ensemble_counter();  // work counter of the ensemble kernel
@@ -30,7 +31,8 @@ private:
     double *partial_ = nullptr;
     int partial_n_ = 0;
     unsigned int *counter_ = nullptr;
-    double *tau_ = nullptr;
+    double *tau_ = nullptr;       // device pointer into tau_host_
+    double *tau_host_ = nullptr;  // pinned, mapped host memory
     double *gen_ = nullptr;
     size_t gen_n_ = 0;
     unsigned int *wait_flag_ = nullptr;
