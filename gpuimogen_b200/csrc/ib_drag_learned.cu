@@ -6,8 +6,8 @@
 // the no-swizzle K-major core-matrix layout (ib_tcgen05.cuh); each thread writes its cell's
 // feature row, thread 0 issues the MMAs of a layer (K = 16 for the first, 4 x K = 16 for the
 // others) into 64 tensor-memory columns and commits them to an mbarrier, and every thread reads
-// its own accumulator row back (tcgen05.ld 32x32b), adds the bias, applies ReLU and writes the
-// BF16 row of the next layer's A operand.  The 64 -> 1 output layer is a dot product in FP32.
+// its own accumulator row back (tcgen05.ld 32x32b), adds the bias in FP32, applies ReLU and
+// writes the BF16 row of the next layer's A operand.  The 64 -> 1 output layer is a dot product in FP32.
 // The update of the cell then runs in FP64 exactly as the exact integrator's (ib_drag.cuh), with
 // the predicted decay exponent in place of the integrated one.
 #include "ib_drag.cuh"
@@ -18,17 +18,21 @@ namespace ib {
 
 constexpr int LT = 128;  // cells per tile, threads per CTA, MMA M
 constexpr int NH = IB_MLP_HID;
-constexpr int KH = NH + 16;  // hidden-layer K: 64 activations + a 16-column block holding the bias
+constexpr int KH = NH;  // hidden-layer K: the 64 activations (4 MMAs of K = 16)
 
-// Shared memory of one CTA.  Biases ride inside the MMAs: input columns 14 and 15 of A0, and
-// columns 64 and 65 of A1, hold the constant 1, and the matching weight columns hold the bias
-// split into a BF16 high part and a BF16 remainder (about 16 significant bits together).
+// Shared memory of one CTA.  The first layer's bias rides inside its MMA: input columns 14 and 15
+// of A0 hold the constant 1 and the matching weight columns the bias split into a BF16 high part
+// and a BF16 remainder (about 16 significant bits together; K = 16 is the smallest MMA anyway).
+// The hidden layers' biases are added in FP32 when the accumulators are read back (a bias block
+// in K would cost a fifth MMA per layer).
 struct LearnedSmem {
     alignas(128) unsigned char W1[NH * 16 * 2];
     alignas(128) unsigned char W2[NH * KH * 2];
     alignas(128) unsigned char W3[NH * KH * 2];
     alignas(128) unsigned char A0[LT * 16 * 2];
     alignas(128) unsigned char A1[LT * KH * 2];
+    float b2[NH], b3[NH];
+    double stage[9][LT];  // drag mode: the next tile's gas and dust values, fetched behind the MMAs
     float w4[NH];
     float b4;
     uint32_t tmem;
@@ -78,14 +82,15 @@ __device__ __forceinline__ void put_bf16(unsigned char *base, uint32_t off, floa
     *reinterpret_cast<__nv_bfloat16 *>(base + off) = __float2bfloat16_rn(v);
 }
 
-// Weight matrix [64 out][K] -> BF16 core-matrix layout, bias split into columns bcol, bcol + 1
+// Weight matrix [64 out][K] -> BF16 core-matrix layout; with a bias, split into columns bcol and
+// bcol + 1
 __device__ void load_weights(unsigned char *W, const float *src, int kin, int K, int bcol, const float *bias)
 {
     for (int i = threadIdx.x; i < NH * K; i += blockDim.x) {
         const int j = i / K, k = i % K;
         float v = 0.f;
         if (k < kin) v = src[j * kin + k];
-        if (k == bcol || k == bcol + 1) {
+        if (bias && (k == bcol || k == bcol + 1)) {
             const float b = bias[j];
             const float hi = __bfloat162float(__float2bfloat16_rn(b));
             v = (k == bcol) ? hi : b - hi;
@@ -94,14 +99,19 @@ __device__ void load_weights(unsigned char *W, const float *src, int kin, int K,
     }
 }
 
-// this thread's accumulator row (16 columns at a time) -> ReLU -> BF16 row r of A1
-__device__ __forceinline__ void hidden_to_a1(unsigned char *A1, int r, uint32_t taddr)
+// this thread's accumulator row (16 columns at a time) + bias (none for the first layer, whose
+// bias is inside its MMA) -> ReLU -> BF16 row r of A1
+__device__ __forceinline__ void hidden_to_a1(unsigned char *A1, int r, uint32_t taddr, const float *bias)
 {
 #pragma unroll
     for (int c = 0; c < NH; c += 16) {
         float h[16];
         tmem_ld16(taddr + c, h);
         tmem_wait_ld();
+        if (bias) {
+#pragma unroll
+            for (int j = 0; j < 16; j++) h[j] += bias[c + j];
+        }
         uint4 u0, u1;
         u0.x = relu_bf16x2(h[0], h[1]);
         u0.y = relu_bf16x2(h[2], h[3]);
@@ -148,6 +158,24 @@ __device__ __forceinline__ void drag_apply_learned(double *g, double *ds, int64_
     g[S] = gE - .5 * pd * rdi;
 }
 
+// Drag mode: start copying the nine gas/dust values of cell i into this thread's column of the
+// stage (asynchronous copies, waited for by the same thread before it reads them).
+__device__ __forceinline__ void stage_cell(LearnedSmem &s, const LearnedArgs &a, int64_t i)
+{
+    const int tid = threadIdx.x;
+    const double *src[9] = {a.gas + i, a.gas + i + a.S, a.gas + i + 2 * a.S, a.gas + i + 3 * a.S,
+                            a.gas + i + 4 * a.S, a.dust + i, a.dust + i + 2 * a.S, a.dust + i + 3 * a.S,
+                            a.dust + i + 4 * a.S};
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&s.stage[k][tid]);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src[k]) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void stage_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 template <int MODE>
 __global__ void __launch_bounds__(LT, 4) mlp_tc_kernel(LearnedArgs a)
 {
@@ -156,13 +184,12 @@ __global__ void __launch_bounds__(LT, 4) mlp_tc_kernel(LearnedArgs a)
     const int tid = threadIdx.x, warp = tid >> 5;
     const float *p = a.params;
     load_weights(s.W1, p + IB_MLP_OFF_W1, 16, 16, 14, p + IB_MLP_OFF_B1);
-    load_weights(s.W2, p + IB_MLP_OFF_W2, NH, KH, NH, p + IB_MLP_OFF_B2);
-    load_weights(s.W3, p + IB_MLP_OFF_W3, NH, KH, NH, p + IB_MLP_OFF_B3);
-    for (int i = tid; i < NH; i += LT) s.w4[i] = p[IB_MLP_OFF_W4 + i];
-    {   // constant columns of A1: [1, 1, 0 x 14] after the 64 activations
-        const float one8[8] = {1.f, 1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, zero8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        store_bf16x8(s.A1 + core_offset(tid, NH, KH), one8);
-        store_bf16x8(s.A1 + core_offset(tid, NH + 8, KH), zero8);
+    load_weights(s.W2, p + IB_MLP_OFF_W2, NH, KH, -1, nullptr);
+    load_weights(s.W3, p + IB_MLP_OFF_W3, NH, KH, -1, nullptr);
+    for (int i = tid; i < NH; i += LT) {
+        s.w4[i] = p[IB_MLP_OFF_W4 + i];
+        s.b2[i] = p[IB_MLP_OFF_B2 + i];
+        s.b3[i] = p[IB_MLP_OFF_B3 + i];
     }
     if (tid == 0) {
         s.b4 = p[IB_MLP_OFF_B4];
@@ -178,6 +205,7 @@ __global__ void __launch_bounds__(LT, 4) mlp_tc_kernel(LearnedArgs a)
     uint32_t phase = 0;
     bool ok = true;
     const int64_t ntiles = (a.n + LT - 1) / LT;
+    if (MODE == 1 && (int64_t)blockIdx.x * LT + tid < a.n) stage_cell(s, a, (int64_t)blockIdx.x * LT + tid);
 
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int64_t i = tile * LT + tid;
@@ -192,11 +220,14 @@ __global__ void __launch_bounds__(LT, 4) mlp_tc_kernel(LearnedArgs a)
             if (live)
                 for (int k = 0; k < 14; k++) f[k] = a.xin[i * IB_MLP_IN + k];
         } else if (live) {
-            const double *g = a.gas + i, *ds = a.dust + i;
-            g0 = g[0]; gE = g[a.S];
-            d0 = ds[0];
+            stage_wait();
+            g0 = s.stage[0][tid]; gE = s.stage[1][tid];
+            d0 = s.stage[5][tid];
 #pragma unroll
-            for (int k = 0; k < 3; k++) { gm[k] = g[(2 + k) * a.S]; dm[k] = ds[(2 + k) * a.S]; }
+            for (int k = 0; k < 3; k++) { gm[k] = s.stage[2 + k][tid]; dm[k] = s.stage[6 + k][tid]; }
+            // the next tile's values stream in behind this tile's MMAs and update
+            const int64_t inext = i + (int64_t)gridDim.x * LT;
+            if (inext < a.n) stage_cell(s, a, inext);
             const double rgi = 1.0 / g0;
             rdi = 1.0 / d0;
             double dvsq = 0, momsq = 0;
@@ -234,10 +265,10 @@ __global__ void __launch_bounds__(LT, 4) mlp_tc_kernel(LearnedArgs a)
         ok = mbar_wait(&s.bar, phase);
         phase ^= 1;
         tc_fence_after();
-        hidden_to_a1(s.A1, tid, my_row);
+        hidden_to_a1(s.A1, tid, my_row, nullptr);
         ok = tc_sync(ok);
         if (!ok) break;
-        // ---- layers 2 and 3: [128 x 80] x [80 -> 64] as 5 MMAs of K = 16 ----
+        // ---- layers 2 and 3: [128 x 64] x [64 -> 64] as 4 MMAs of K = 16 ----
         for (int layer = 0; layer < 2; layer++) {
             const unsigned char *W = layer ? s.W3 : s.W2;
             if (tid == 0) {
@@ -251,7 +282,7 @@ __global__ void __launch_bounds__(LT, 4) mlp_tc_kernel(LearnedArgs a)
             phase ^= 1;
             tc_fence_after();
             if (layer == 0) {
-                hidden_to_a1(s.A1, tid, my_row);
+                hidden_to_a1(s.A1, tid, my_row, s.b2);
                 ok = tc_sync(ok);
                 if (!ok) break;
             }
@@ -265,7 +296,7 @@ __global__ void __launch_bounds__(LT, 4) mlp_tc_kernel(LearnedArgs a)
             tmem_ld16(my_row + c, h);
             tmem_wait_ld();
 #pragma unroll
-            for (int j = 0; j < 16; j++) y = fmaf(s.w4[c + j], fmaxf(h[j], 0.f), y);
+            for (int j = 0; j < 16; j++) y = fmaf(s.w4[c + j], fmaxf(h[j] + s.b3[c + j], 0.f), y);
         }
         if (MODE == 0) {
             if (live) a.yout[i] = y;
@@ -276,8 +307,9 @@ __global__ void __launch_bounds__(LT, 4) mlp_tc_kernel(LearnedArgs a)
                 if (magdv < 1e-9) {
                     fb = true;  // the exact integrator's no-drag cut: let it handle the cell
                 } else if (indom) {
+                    // FP32 exponentials: their 1e-7 relative error is far below the network's
                     const float sp = expf(a.oshift + a.oscale * y);
-                    if (isfinite(sp)) decay = exp(-(double)sp);
+                    if (isfinite(sp)) decay = (double)expf(-sp);
                     else fb = true;
                 } else {
                     fb = true;
@@ -299,6 +331,7 @@ __global__ void __launch_bounds__(LT, 4) mlp_tc_kernel(LearnedArgs a)
         // every thread's tensor-memory reads are done before the next tile's MMAs overwrite them
         tc_fence_before();
     }
+    if (MODE == 1) stage_wait();  // no copy into shared memory outlives the CTA (early exit)
     if (!ok && tid == 0) {
         atomicOr(a.err, 2u);
         mbar_wait(&s.bar, phase ^ 1);  // one more bounded wait for a late MMA before freeing its columns
