@@ -59,6 +59,22 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi)
     return *reinterpret_cast<uint32_t *>(&h);
 }
 
+// two FP32 lanes at once (packed f32x2 arithmetic of sm_100)
+__device__ __forceinline__ float2 add2(float2 a, float2 b)
+{
+    unsigned long long x = *reinterpret_cast<unsigned long long *>(&a), y = *reinterpret_cast<unsigned long long *>(&b), z;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(z) : "l"(x), "l"(y));
+    return *reinterpret_cast<float2 *>(&z);
+}
+
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c)
+{
+    unsigned long long x = *reinterpret_cast<unsigned long long *>(&a), y = *reinterpret_cast<unsigned long long *>(&b),
+                       z = *reinterpret_cast<unsigned long long *>(&c);
+    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(z) : "l"(x), "l"(y));
+    return *reinterpret_cast<float2 *>(&z);
+}
+
 // relu(lo), relu(hi) -> BF16x2 in one conversion (lo in the low half)
 __device__ __forceinline__ uint32_t relu_bf16x2(float lo, float hi)
 {
@@ -110,7 +126,11 @@ __device__ __forceinline__ void hidden_to_a1(unsigned char *A1, int r, uint32_t 
         tmem_wait_ld();
         if (bias) {
 #pragma unroll
-            for (int j = 0; j < 16; j++) h[j] += bias[c + j];
+            for (int j = 0; j < 16; j += 2) {
+                const float2 r = add2(make_float2(h[j], h[j + 1]), *reinterpret_cast<const float2 *>(bias + c + j));
+                h[j] = r.x;
+                h[j + 1] = r.y;
+            }
         }
         uint4 u0, u1;
         u0.x = relu_bf16x2(h[0], h[1]);
@@ -289,15 +309,21 @@ __global__ void __launch_bounds__(LT, 4) mlp_tc_kernel(LearnedArgs a)
         }
         if (!ok) break;
         // ---- output: y = b4 + w4 . relu(h3) (FP32, straight from tensor memory) ----
-        float y = s.b4;
+        float2 y2 = make_float2(0.f, 0.f);  // even and odd hidden units
 #pragma unroll
         for (int c = 0; c < NH; c += 16) {
             float h[16];
             tmem_ld16(my_row + c, h);
             tmem_wait_ld();
 #pragma unroll
-            for (int j = 0; j < 16; j++) y = fmaf(s.w4[c + j], fmaxf(h[j] + s.b3[c + j], 0.f), y);
+            for (int j = 0; j < 16; j += 2) {
+                float2 z = add2(make_float2(h[j], h[j + 1]), *reinterpret_cast<const float2 *>(s.b3 + c + j));
+                z.x = fmaxf(z.x, 0.f);
+                z.y = fmaxf(z.y, 0.f);
+                y2 = fma2(*reinterpret_cast<const float2 *>(s.w4 + c + j), z, y2);
+            }
         }
+        const float y = s.b4 + (y2.x + y2.y);
         if (MODE == 0) {
             if (live) a.yout[i] = y;
         } else {
