@@ -206,7 +206,11 @@ int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3
     if (dir > 1) {
         for (int w = 4; w >= 2; w >>= 1)
             if (w <= xjw && grid[0] % w == 0 && n * w <= 512) { W = w; break; }
-        if (W == 1 && xjw >= 2 && grid[0] % 2 == 0 && n * 2 <= 1024) W = 2;
+        // pencils of 257-512 cells: 4 pencils of 2 cells a thread (full 32-byte runs) rather than 2
+        // of one cell, both 1024 threads (512 x 512 x 64, y: 1.53 -> 1.32 ms; at 256 or fewer cells
+        // the 2-cell form measured slower: 256^3 y 1.31 -> 1.37)
+        if (W == 1 && xjw >= 4 && grid[0] % 4 == 0 && n * 4 <= 2048) W = 4;
+        else if (W == 1 && xjw >= 2 && grid[0] % 2 == 0 && n * 2 <= 1024) W = 2;
     }
     const int CPT = (n * W > 1024) ? 2 : 1;
     const int rows = (n + CPT - 1) / CPT;
@@ -229,7 +233,8 @@ int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3
     } while (0)
 #define IB_XJ_W(F)                                            \
     do {                                                      \
-        if (W == 4) IB_XJ(F, 4, 1, false);                    \
+        if (W == 4 && CPT == 2) IB_XJ(F, 4, 2, true);         \
+        else if (W == 4) IB_XJ(F, 4, 1, false);               \
         else if (W == 2) IB_XJ(F, 2, 1, false);               \
         else if (CPT == 2 && dir == 1) IB_XJ(F, 1, 2, true);  \
         else if (CPT == 2) IB_XJ(F, 1, 2, false);             \
