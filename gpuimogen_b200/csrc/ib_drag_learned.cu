@@ -29,7 +29,9 @@ struct LearnedSmem {
     alignas(128) unsigned char W1[NH * 16 * 2];
     alignas(128) unsigned char W2[NH * KH * 2];
     alignas(128) unsigned char W3[NH * KH * 2];
-    alignas(128) unsigned char A0[LT * 16 * 2];
+    // A0 (the first layer's [128 x 16] input) lives in the first 4 KB of A1: it is written at the
+    // start of a tile, after the previous tile's last MMA has read A1, and dead once the first
+    // layer's MMA has completed, before A1 is written
     alignas(128) unsigned char A1[LT * KH * 2];
     float b2[NH], b3[NH];
     double stage[9][LT];  // drag mode: the next tile's gas and dust values, fetched behind the MMAs
@@ -197,7 +199,7 @@ __device__ __forceinline__ void stage_cell(LearnedSmem &s, const LearnedArgs &a,
 __device__ __forceinline__ void stage_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 template <int MODE>
-__global__ void __launch_bounds__(LT, 4) mlp_tc_kernel(LearnedArgs a)
+__global__ void __launch_bounds__(LT, 5) mlp_tc_kernel(LearnedArgs a)
 {
     extern __shared__ __align__(1024) unsigned char learned_smem_raw[];
     LearnedSmem &s = *reinterpret_cast<LearnedSmem *>(learned_smem_raw);
@@ -221,7 +223,8 @@ __global__ void __launch_bounds__(LT, 4) mlp_tc_kernel(LearnedArgs a)
     const uint32_t tmem = s.tmem;
     const uint32_t my_row = tmem + ((uint32_t)(warp * 32) << 16);
     const uint32_t id = idesc_bf16_f32(LT, NH);
-    const uint64_t dA0 = smem_desc(s.A0, 128, 256), dW1 = smem_desc(s.W1, 128, 256);
+    unsigned char *const A0 = s.A1;
+    const uint64_t dA0 = smem_desc(A0, 128, 256), dW1 = smem_desc(s.W1, 128, 256);
     uint32_t phase = 0;
     bool ok = true;
     const int64_t ntiles = (a.n + LT - 1) / LT;
@@ -273,8 +276,8 @@ __global__ void __launch_bounds__(LT, 4) mlp_tc_kernel(LearnedArgs a)
         }
         f[14] = 1.f;
         f[15] = 1.f;
-        store_bf16x8(s.A0 + core_offset(tid, 0, 16), f);
-        store_bf16x8(s.A0 + core_offset(tid, 8, 16), f + 8);
+        store_bf16x8(A0 + core_offset(tid, 0, 16), f);
+        store_bf16x8(A0 + core_offset(tid, 8, 16), f + 8);
         ok = tc_sync(ok);
         if (!ok) break;
         // ---- layer 1: [128 x 16] x [16 -> 64], bias in columns 14-15 ----
