@@ -185,7 +185,9 @@ IB_API int ib_cudaSoundspeed(const ib_fluid *fluid, double gamma, double *cs_out
 
 /* Replaces the cflTimestep mex (gpuclass/cflTimestep.cu:64-103 -> computeLocalCFLTimestep
  * :107-252): *tau_host = min over cells of the signal-crossing time, halved for HLL/HLLC.
- * cs is the soundspeed array from ib_cudaSoundspeed.  Synchronises the stream. */
+ * cs is the soundspeed array from ib_cudaSoundspeed.  Synchronises the stream.  The kernel
+ * stores tau into pinned, mapped host memory (allocated once per device), so the read-back is
+ * not queued behind device-to-host copies the caller has running on other streams. */
 IB_API int ib_cflTimestep(const ib_fluid *fluid, const double *cs, const ib_geometry *geo, int method,
                    double *tau_host, void *stream);
 
