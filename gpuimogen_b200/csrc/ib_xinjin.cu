@@ -31,9 +31,8 @@ __device__ __forceinline__ double block_max_keep(double v, double *red, int col)
 
 // Freezing speed |v| + c_s of one cell.  Uses memory slab 2 (px) as the transported momentum
 // whatever the sweep direction, as the reference's freeze kernel does.
-__device__ __forceinline__ double freeze_cell(const double (&X)[5], double gamma, double gm1)
+__device__ __forceinline__ double freeze_cell(const double (&X)[5], double invrho, double gamma, double gm1)
 {
-    double invrho = 1.0 / X[0];
     double psq = X[3];
     double px = X[4];
     psq = psq * psq + px * px;
@@ -75,6 +74,10 @@ __global__ void __launch_bounds__(1024) xj_pencil_kernel(double *q, int64_t slab
     const double gm1 = gamma - 1.0;
 
     double u0[CPT][5], u1[CPT][5];
+    // 1 / density of each cell's current stage input: the product build computes it once per stage
+    // (for the freezing speed, the pressure and the velocity) and takes the corrector's from the
+    // predictor's floor; the strict build divides where the reference does
+    double rinv[CPT];
 #pragma unroll
     for (int m = 0; m < CPT; m++) {
         const int i = r0 + m * S;
@@ -90,7 +93,13 @@ __global__ void __launch_bounds__(1024) xj_pencil_kernel(double *q, int64_t slab
 #pragma unroll
         for (int m = 0; m < CPT; m++) {
             if (r0 + m * S < n) {
-                double v = freeze_cell((stage == 0) ? u0[m] : u1[m], gamma, gm1);
+                const double(&X)[5] = (stage == 0) ? u0[m] : u1[m];
+#ifdef IB_STRICT_ARITH
+                const double v = freeze_cell(X, 1.0 / X[0], gamma, gm1);
+#else
+                if (stage == 0) rinv[m] = 1.0 / X[0];
+                const double v = freeze_cell(X, rinv[m], gamma, gm1);
+#endif
                 cm = (v > cm) ? v : cm;
             }
         }
@@ -105,8 +114,8 @@ __global__ void __launch_bounds__(1024) xj_pencil_kernel(double *q, int64_t slab
 #ifdef IB_STRICT_ARITH
                 const double Pv = gm1 * (q1 - .5 * (q4 * q4 + q3 * q3 + q2 * q2) / q0);
                 const double Vx = Q[nslot] / q0;
-#else  // one reciprocal of the density for pressure and velocity
-                const double ir = 1.0 / q0;
+#else
+                const double ir = rinv[m];
                 const double Pv = gm1 * (q1 - .5 * (q4 * q4 + q3 * q3 + q2 * q2) * ir);
                 const double Vx = Q[nslot] * ir;
 #endif
@@ -170,7 +179,12 @@ __global__ void __launch_bounds__(1024) xj_pencil_kernel(double *q, int64_t slab
                 double p0 = pr[0], p1 = pr[1];
                 const double p2 = pr[2], p3 = pr[3], p4 = pr[4];
                 p0 = (p0 < minmass) ? minmass : p0;
+#ifdef IB_STRICT_ARITH
                 double w = .5 * (p2 * p2 + p3 * p3 + p4 * p4) / p0;
+#else
+                rinv[m] = 1.0 / p0;
+                double w = .5 * (p2 * p2 + p3 * p3 + p4 * p4) * rinv[m];
+#endif
                 if ((p1 - w) < p0 * mintemp) p1 = w + p0 * mintemp;
                 u1[m][0] = p0; u1[m][1] = p1; u1[m][2] = p2; u1[m][3] = p3; u1[m][4] = p4;
             }
