@@ -77,7 +77,9 @@ __global__ void __launch_bounds__(1024) xj_pencil_kernel(double *q, int64_t slab
     // 1 / density of each cell's current stage input: the product build computes it once per stage
     // (for the freezing speed, the pressure and the velocity) and takes the corrector's from the
     // predictor's floor; the strict build divides where the reference does
+#ifndef IB_STRICT_ARITH
     double rinv[CPT];
+#endif
 #pragma unroll
     for (int m = 0; m < CPT; m++) {
         const int i = r0 + m * S;
@@ -110,10 +112,10 @@ __global__ void __launch_bounds__(1024) xj_pencil_kernel(double *q, int64_t slab
             const int i = r0 + m * S;
             if (i < n) {
                 const double *Q = (stage == 0) ? u0[m] : u1[m];
-                const double q0 = Q[0], q1 = Q[1], q2 = Q[2], q3 = Q[3], q4 = Q[4];
+                const double q1 = Q[1], q2 = Q[2], q3 = Q[3], q4 = Q[4];
 #ifdef IB_STRICT_ARITH
-                const double Pv = gm1 * (q1 - .5 * (q4 * q4 + q3 * q3 + q2 * q2) / q0);
-                const double Vx = Q[nslot] / q0;
+                const double Pv = gm1 * (q1 - .5 * (q4 * q4 + q3 * q3 + q2 * q2) / Q[0]);
+                const double Vx = Q[nslot] / Q[0];
 #else
                 const double ir = rinv[m];
                 const double Pv = gm1 * (q1 - .5 * (q4 * q4 + q3 * q3 + q2 * q2) * ir);

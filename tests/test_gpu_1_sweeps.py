@@ -19,6 +19,8 @@ SHAPES = [
     (8, 300, 6),     # y: march with several chunks per pencil
     (6, 7, 130),     # z: march with several chunks per pencil
     (5, 4, 3),       # tiny pencils
+    (8, 140, 3),     # Xin-Jin y: pencil pairs of 129-256 cells with nx a multiple of 4
+    (4, 3, 200),     # Xin-Jin z: the same
 ]
 
 
