@@ -16,7 +16,9 @@ int num_sms();
 
 // Reusable per-device scratch: grown on demand, never shrunk, freed at process exit.  The
 // reference allocates and frees a 6-slab temporary per call (cudaFluidStep.cu:508-513); the
-// fused sweeps here need none, only the reductions and the Xin-Jin pencils use this.
+// fused sweeps here need none beyond the chunked pipeline's halo side buffer; the others
+// are the reductions, the ETDRK2 drag's internal-energy slab, the wait flags and the ensemble's
+// work counter.
 class Scratch {
 public:
     double *cfl_partial(int nblocks);
