@@ -283,7 +283,8 @@ IB_API int ib_riemannEnsemble(const ib_ensemble *e, const ib_fluid_thermo *therm
 
 /* ---------------------------------------------------------------------------------------------
  * Learned drag (no reference counterpart: it stands in for the LogTrap2 integrator of
- * cudaSource2FluidDrag.cu:709-795 and keeps that integrator as fallback and judge).
+ * cudaSource2FluidDrag.cu:709-795 and keeps that integrator as fallback and as the measure of
+ * its error).
  *
  * The LogTrap2 update of a cell is fixed by one number, the decay exponent s = dt * k_eff of
  * the gas-dust relative velocity (dv -> dv * exp(-s) about the centre-of-mass velocity, the gas
