@@ -10,8 +10,8 @@ Metric: Mcell-updates/s = cells x iterations / seconds / 1e6 (whole job over all
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Multi-GPU: each rank runs an independent replica of the workload (the problem does not shard
-across GPUs in this build), scaling "weak"; the time is the maximum over ranks.
+Multi-GPU: each rank runs an independent replica of the workload (the single-GPU fluid step has
+no inter-GPU exchange), scaling "weak"; the time is the maximum over ranks.
 --impl reference times the reference's CPU path, which for this hot path is the oracle's C
 restatement of the reference kernels (the reference itself has no CPU implementation), on all
 host cores, on a bounded sample of the same workload.
