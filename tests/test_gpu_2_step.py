@@ -445,3 +445,31 @@ def test_wide_z_blocks_match_y_sweep_of_transposed_state(cuda, ib, nz, precision
     err = ((out - back).abs().sum(dim=1) / back.abs().sum(dim=1).clamp_min(1e-300)).cpu().numpy()
     tol = 1e-13 if precision == "fp64" else 1e-7
     assert np.all(err <= tol), err
+
+
+def test_cfl_host_read_while_a_download_runs(cuda, ib, po):
+    """The CFL timestep reaches the host through mapped memory written by the kernel, not a
+    device-to-host copy: it must be correct, and bit-identical to the oracle in the strict build,
+    while a large state download is in flight on another stream."""
+    shape = (48, 40, 36)
+    q = problems.random_jumpy(shape, seed=21)
+    h = (0.02, 0.025, 0.03)
+    big = torch.empty(64 << 20, dtype=torch.float64, device="cuda")  # 512 MB read out meanwhile
+    big.fill_(1.0)
+    pinned = torch.empty(big.numel(), dtype=torch.float64).pin_memory()
+    side = torch.cuda.Stream()
+    ib.use_variant("strict")
+    try:
+        fl = to_fluid(q, shape)
+        geo = ib.Geometry(shape, h)
+        for method in (1, 2, 3):
+            ref = po.cfl_timestep(q, shape, 1.4, h, method)
+            torch.cuda.synchronize()
+            with torch.cuda.stream(side):
+                pinned.copy_(big, non_blocking=True)
+            tau = ib.cflTimestepFused(fl, 1.4, geo, method)
+            assert tau == ref, (method, tau, ref)
+            torch.cuda.synchronize()
+    finally:
+        ib.use_variant("product")
+    assert pinned[-1].item() == 1.0
