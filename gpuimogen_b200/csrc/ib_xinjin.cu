@@ -42,6 +42,54 @@ __device__ __forceinline__ double freeze_cell(const double (&X)[5], double invrh
     return fabs(px) * invrho + sqrt(gamma * P * invrho);
 }
 
+// The left- and right-going limited fluxes of one component, flux_limit<FLIM>(A1, B1) and
+// flux_limit<FLIM>(A2, B2).  Product build, Ospre and van Leer: their two divisions share one
+// (1/(d1 d2) times d2 and d1) when d1 d2 is a normal number; the strict build divides twice.
+template <int FLIM>
+__device__ __forceinline__ void flux_limit_pair(double A1, double B1, double A2, double B2, double &o1, double &o2)
+{
+#ifndef IB_STRICT_ARITH
+    if constexpr (FLIM == IB_FLUX_OSPRE || FLIM == IB_FLUX_VANLEER) {
+        double n1, d1, n2, d2;
+        bool p1, p2;
+        if constexpr (FLIM == IB_FLUX_OSPRE) {  // 1.5 r (A + B) / (A^2 + r + B^2), 0 where r <= 0
+            const double r1 = A1 * B1, r2 = A2 * B2;
+            p1 = !(r1 <= 0.0);
+            p2 = !(r2 <= 0.0);
+            n1 = 1.5 * r1 * (A1 + B1);
+            d1 = A1 * A1 + r1 + B1 * B1;
+            n2 = 1.5 * r2 * (A2 + B2);
+            d2 = A2 * A2 + r2 + B2 * B2;
+        } else {  // 2AB / (A + B) where 2AB > 0
+            const double r1 = 2.0 * A1 * B1, r2 = 2.0 * A2 * B2;
+            p1 = r1 > 0.0;
+            p2 = r2 > 0.0;
+            n1 = r1;
+            d1 = A1 + B1;
+            n2 = r2;
+            d2 = A2 + B2;
+        }
+        d1 = p1 ? d1 : 1.0;
+        d2 = p2 ? d2 : 1.0;
+        const double pd = d1 * d2;
+        double i1, i2;
+        if (fabs(pd) >= 2.2250738585072014e-308 && fabs(pd) <= 1.7976931348623157e308) {
+            const double rr = 1.0 / pd;
+            i1 = d2 * rr;
+            i2 = d1 * rr;
+        } else {
+            i1 = 1.0 / d1;
+            i2 = 1.0 / d2;
+        }
+        o1 = p1 ? n1 * i1 : 0.0;
+        o2 = p2 ? n2 * i2 : 0.0;
+        return;
+    }
+#endif
+    o1 = flux_limit<FLIM>(A1, B1);
+    o2 = flux_limit<FLIM>(A2, B2);
+}
+
 // W adjacent pencils per block (W = 1 for x rows; y/z pencils take W = 2 or 4 when nx allows it,
 // so that the loads of a warp cover 16- or 32-byte runs of x instead of single doubles a row or a
 // plane apart).  Thread t works on column t % W and cells t / W + m * S (m < CPT,
@@ -149,8 +197,10 @@ __global__ void __launch_bounds__(1024) xj_pencil_kernel(double *q, int64_t slab
                         const double Rm = Rb[IX(k, il)], R0 = Rb[IX(k, i)], Rp = Rb[IX(k, ir)];
                         const double dL0 = 0.5 * (L0 - Lm), dLp = 0.5 * (Lp - L0);
                         const double dR0 = 0.5 * (R0 - Rm), dRp = 0.5 * (Rp - R0);
-                        nl[m][k] = L0 - flux_limit<FLIM>(dL0, dLp);
-                        nr[m][k] = R0 + flux_limit<FLIM>(dR0, dRp);
+                        double limL, limR;
+                        flux_limit_pair<FLIM>(dL0, dLp, dR0, dRp, limL, limR);
+                        nl[m][k] = L0 - limL;
+                        nr[m][k] = R0 + limR;
                     }
                 }
             }
