@@ -97,6 +97,7 @@ __device__ __forceinline__ void drag_features(double g0, double gE, double g2, d
                                               double d3, double d4, double &magdv, double &u)
 {
     double dv, dvsq, press;
+#ifdef IB_STRICT_ARITH
     dv = (g2) / g0 - d2 / d0;
     dvsq = dv * dv;
     dv = (g3) / g0 - d3 / d0;
@@ -106,6 +107,18 @@ __device__ __forceinline__ void drag_features(double g0, double gE, double g2, d
     press = (gE - .5 * (g2 * g2 + g3 * g3 + g4 * g4) / g0);
     magdv = sqrt(dvsq);
     u = press / g0;
+#else  // the two density reciprocals once instead of eight divisions
+    const double ig = 1.0 / g0, id = 1.0 / d0;
+    dv = g2 * ig - d2 * id;
+    dvsq = dv * dv;
+    dv = g3 * ig - d3 * id;
+    dvsq += dv * dv;
+    dv = g4 * ig - d4 * id;
+    dvsq += dv * dv;
+    press = (gE - .5 * (g2 * g2 + g3 * g3 + g4 * g4) * ig);
+    magdv = sqrt(dvsq);
+    u = press * ig;
+#endif
 }
 
 // Momentum exchange about the centre-of-mass velocity with dv -> dv exp(-t k), gas energy
@@ -116,35 +129,50 @@ __device__ __forceinline__ void drag_apply(double *g, double *ds, int64_t S, dou
     double mu, rhoginv, pdustsq, vstick, dv_i, dv_t, qq;
     // the reference evaluates exp(-t k) once per axis with the same argument; once is the same value
     const double decay = exp(-t * k);
+#ifdef IB_STRICT_ARITH
     mu = d0 / (g0 + d0);
     mu = mu * g0;
     rhoginv = 1.0 / g0;
+    auto over_sum = [&](double x) { return x / (g0 + d0); };
+    auto over_d0 = [&](double x) { return x / d0; };
+#else  // three reciprocals instead of nine divisions
+    const double isum = 1.0 / (g0 + d0), rhodinv = 1.0 / d0;
+    mu = d0 * isum;
+    mu = mu * g0;
+    rhoginv = 1.0 / g0;
+    auto over_sum = [&](double x) { return x * isum; };
+    auto over_d0 = [&](double x) { return x * rhodinv; };
+#endif
 
     pdustsq = -d2 * d2;
-    vstick = (g2 + d2) / (g0 + d0);
-    dv_i = (g2) * rhoginv - d2 / d0;
+    vstick = over_sum(g2 + d2);
+    dv_i = (g2) * rhoginv - over_d0(d2);
     dv_t = dv_i * decay;
     g[2 * S] = g0 * vstick + dv_t * mu;
     ds[2 * S] = qq = d0 * vstick - dv_t * mu;
     pdustsq += qq * qq;
 
     pdustsq -= d3 * d3;
-    vstick = (g3 + d3) / (g0 + d0);
-    dv_i = (g3) * rhoginv - d3 / d0;
+    vstick = over_sum(g3 + d3);
+    dv_i = (g3) * rhoginv - over_d0(d3);
     dv_t = dv_i * decay;
     g[3 * S] = g0 * vstick + dv_t * mu;
     ds[3 * S] = qq = d0 * vstick - dv_t * mu;
     pdustsq += qq * qq;
 
     pdustsq -= d4 * d4;
-    vstick = (g4 + d4) / (g0 + d0);
-    dv_i = (g4) * rhoginv - d4 / d0;
+    vstick = over_sum(g4 + d4);
+    dv_i = (g4) * rhoginv - over_d0(d4);
     dv_t = dv_i * decay;
     g[4 * S] = g0 * vstick + dv_t * mu;
     ds[4 * S] = qq = d0 * vstick - dv_t * mu;
     pdustsq += qq * qq;
 
+#ifdef IB_STRICT_ARITH
     g[S] = gE - .5 * pdustsq / d0;
+#else
+    g[S] = gE - .5 * pdustsq * rhodinv;
+#endif
 }
 
 // cukern_GasDustDrag_GeneralAccel (cudaSource2FluidDrag.cu:898-931): -d|dv|/dt at |dv| = w; the
