@@ -53,7 +53,184 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--shape", default=None, help="override grid, e.g. 128,128,128 (not the benchmark config)")
+    ap.add_argument("--case", default="bench", choices=["bench"] + sorted(CASES),
+                    help="bench (default): the benchmark line; the others are small cases for ncu "
+                         "captures and per-kernel timings (one GPU, no JSON bench line)")
+    ap.add_argument("--n", type=int, default=None, help="cases: cube edge (sweeps, all) or 2-D edge (drag)")
+    ap.add_argument("--m", type=int, default=1024, help="case all: 2-D gas-dust edge")
+    ap.add_argument("--method", type=int, default=2, help="cases: 1 HLL, 2 HLLC, 3 Xin-Jin")
+    ap.add_argument("--slope", default="mc")
+    ap.add_argument("--fluxlim", default="vanleer")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32flux"])
+    ap.add_argument("--reps", type=int, default=5)
     return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------------
+# Small cases for Nsight Compute captures and per-kernel timings (one GPU).  Each launches the
+# kernels it names a few times on a state larger than the 126 MB L2 and prints one line.
+# ------------------------------------------------------------------------------------------------
+def _case_shape(args, default_n):
+    if args.shape:
+        return tuple(int(v) for v in args.shape.split(","))
+    n = args.n or default_n
+    return (n, n, n)
+
+
+def case_sweeps(args):
+    """One warm-up iteration of Kelvin-Helmholtz, then one launch of each sweep kernel (x, y, z;
+    an axis of extent 1 launches nothing) and one CFL reduction: n^3 (default 192) or --shape."""
+    import torch
+    import gpuimogen_b200 as ib
+    from gpuimogen_b200 import problems
+    shape = _case_shape(args, 192)
+    q = problems.kelvin_helmholtz(shape, seed=1)
+    fl = ib.Fluid(shape, q=torch.from_numpy(q).cuda(), gamma=GAMMA)
+    geo = ib.Geometry(shape)
+    num = ib.numerics(slope=args.slope, fluxlim=args.fluxlim, precision=args.precision)
+    tm = ib.TimeManager(cfl=CFL)
+    ib.run_iteration([fl], geo, tm, args.method, num)
+    for d in (1, 2, 3):
+        ib.cudaFluidStep(fl, geo, [tm.dTime, 1, GAMMA, 1e-5, args.method, d], num)
+    ib.cflTimestepFused(fl, GAMMA, geo, args.method)
+    torch.cuda.synchronize()
+    print("case sweeps done", shape, args.precision, "method", args.method)
+
+
+def case_time_sweeps(args):
+    """Per-direction sweep time (CUDA events, mean of --reps launches after one untimed launch)
+    of cudaFluidStep on the Kelvin-Helmholtz state: n^3 (default 256) or --shape."""
+    import torch
+    import gpuimogen_b200 as ib
+    from gpuimogen_b200 import problems
+    shape = _case_shape(args, 256)
+    num = ib.numerics(slope=args.slope, fluxlim=args.fluxlim, precision=args.precision)
+    fl = ib.Fluid(shape, q=torch.from_numpy(problems.kelvin_helmholtz(shape, seed=1)).cuda(), gamma=GAMMA)
+    geo = ib.Geometry(shape)
+    out = []
+    for d in (1, 2, 3):
+        if shape[d - 1] < 3:
+            out.append(None)
+            continue
+        params = [1e-5, 1, GAMMA, 1e-5, args.method, d]
+        ib.cudaFluidStep(fl, geo, params, num)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.reps):
+            ib.cudaFluidStep(fl, geo, params, num)
+        b.record()
+        torch.cuda.synchronize()
+        out.append(round(a.elapsed_time(b) / args.reps, 4))
+    print(json.dumps({"case": "time-sweeps", "shape": list(shape), "method": args.method, "slope": args.slope,
+                      "fluxlim": args.fluxlim, "precision": args.precision, "ms_x_y_z": out}))
+
+
+def case_cfl(args):
+    """CUDA-event time of the two device-result CFL entry points (ib_cflTimestepFused with its
+    allocated scratch, ib_cflTimestepNoAlloc with the built-in array) on 512^2 and 256^3."""
+    import ctypes
+    import torch
+    import gpuimogen_b200 as ib
+    from gpuimogen_b200 import imogen, problems
+    L = imogen.load("product")
+    res = {}
+    for shape in ((512, 512, 1), (256, 256, 256)):
+        fl = ib.Fluid(shape, q=torch.from_numpy(problems.kelvin_helmholtz(shape, seed=1)).cuda(), gamma=GAMMA)
+        geo = ib.Geometry(shape)
+        tau = torch.zeros(2, dtype=torch.float64, device="cuda")
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        f, g = fl.c_struct(), geo.c_struct()
+        times = {}
+        for name in ("fused", "noalloc"):
+            def call():
+                if name == "fused":
+                    return L.ib_cflTimestepFused(ctypes.byref(f), GAMMA, ctypes.byref(g), 2, None,
+                                                 ctypes.c_void_p(tau.data_ptr()), st)
+                return L.ib_cflTimestepNoAlloc(ctypes.byref(f), GAMMA, ctypes.byref(g), 2,
+                                               ctypes.c_void_p(tau.data_ptr() + 8), st)
+            assert call() == 0
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(args.reps):
+                assert call() == 0
+            b.record()
+            torch.cuda.synchronize()
+            times[name] = round(a.elapsed_time(b) / args.reps, 4)
+        assert tau[0].item() == tau[1].item()
+        res["x".join(str(v) for v in shape)] = times
+    print(json.dumps({"case": "cfl", "ms": res}))
+
+
+def case_drag(args):
+    """The 2-D gas-dust state on n x n (default 1024): one exact LogTrap2 drag call
+    (logtrap_kernel) and one learned call (mlp_tc_kernel<1>) after training a small model
+    (200k exact labels, 2 epochs)."""
+    import torch
+    import gpuimogen_b200 as ib
+    from gpuimogen_b200 import dusty
+    from gpuimogen_b200 import learned_drag as ld
+    n = args.n or 1024
+    model, _ = ld.train(n_samples=200_000, epochs=2, seed=3, batch=8192)
+    exact = dusty.DustyRun(n)
+    learned = dusty.DustyRun(n, model=model)
+    exact.drag([exact.gas, exact.dust], 4e-5)
+    learned.drag([learned.gas, learned.dust], 4e-5)
+    torch.cuda.synchronize()
+    print("case drag done", n, "fallbacks", int(learned.fallbacks.item()))
+
+
+def case_all(args):
+    """Every kind of kernel of the library once: KH at n^3 (default 160^3, 164 MB of state) for
+    the sweeps of every method and precision, CFL, freezeAndPtot and the outflow fill; KH on
+    512 x 512 x 8 (z sweeps of 2 MB planes: the wide-block kernels) and 2048 x 2048 x 1 (the
+    chunked pipeline and its halo copy); the 2-D gas-dust state at --m^2 for the drag kernels
+    (ETDRK2 included) and the learned drag; a 592-problem Riemann ensemble (4 iterations); the
+    MLP training kernels on a 65536-sample batch."""
+    import torch
+    import gpuimogen_b200 as ib
+    from gpuimogen_b200 import dusty, ensemble, problems
+    from gpuimogen_b200 import learned_drag as ld
+    shape = _case_shape(args, 160)
+    q = problems.kelvin_helmholtz(shape, seed=1)
+    geo = ib.Geometry(shape)
+    dt = 1e-5
+    for method, prec in ((2, "fp64"), (2, "fp32flux"), (1, "fp64"), (3, "fp64")):
+        fl = ib.Fluid(shape, q=torch.from_numpy(q).cuda(), gamma=GAMMA)
+        num = ib.numerics(slope="mc", precision=prec)
+        for d in (1, 2, 3):
+            ib.cudaFluidStep(fl, geo, [dt, 1, GAMMA, 1e-5, method, d], num)
+    shp = (512, 512, 8)
+    qw = problems.kelvin_helmholtz(shp, seed=2)
+    for prec in ("fp64", "fp32flux"):
+        fw = ib.Fluid(shp, q=torch.from_numpy(qw).cuda(), gamma=GAMMA)
+        ib.cudaFluidStep(fw, ib.Geometry(shp), [dt, 1, GAMMA, 1e-5, 2, 3], ib.numerics(slope="mc", precision=prec))
+    del fw
+    shp = (2048, 2048, 1)
+    fc = ib.Fluid(shp, q=torch.from_numpy(problems.kelvin_helmholtz(shp, seed=3)).cuda(), gamma=GAMMA)
+    for d in (1, 2):
+        ib.cudaFluidStep(fc, ib.Geometry(shp), [dt, 1, GAMMA, 1e-5, 2, d], ib.numerics(slope="mc"))
+    del fc
+    fl = ib.Fluid(shape, q=torch.from_numpy(q).cuda(), gamma=GAMMA, bc="outflow")
+    ib.cflTimestepFused(fl, GAMMA, geo, 2)
+    ib.freezeAndPtot(fl, GAMMA, 1, 0.0)
+    ib.setFluidBoundary(fl, 1)
+    run = dusty.DustyRun(args.m)
+    for method in ("logtrap2", "rk4", "etdrk1", "etdrk2"):
+        run.reset()
+        ib.cudaSource2FluidDrag(run.gas, run.dust, run.tg, run.td, run.geo, [4e-5, ib.DRAG[method]])
+    model, _ = ld.train(n_samples=65536 * 4, epochs=1, seed=3, batch=65536)
+    run.reset()
+    ld.drag_step(run.gas, run.dust, model, 4e-5)
+    ens = ensemble.RiemannEnsemble.random(592, seed=2)
+    ens.run(t_end=0.1, itermax=4, tuning={"threads": 512, "chunk": 504})
+    torch.cuda.synchronize()
+    print("case all done")
+
+
+CASES = {"sweeps": case_sweeps, "time-sweeps": case_time_sweeps, "cfl": case_cfl, "drag": case_drag,
+         "all": case_all}
 
 
 def dist_init(n_gpus):
@@ -222,6 +399,13 @@ def run_reference(args, world, rank):
 
 def main():
     args = parse()
+    if args.case != "bench":
+        import torch
+        import gpuimogen_b200 as ib
+        torch.cuda.set_device(0)
+        ib.load("product")
+        CASES[args.case](args)
+        return 0
     world, rank, local = dist_init(args.gpus)
     if args.impl == "reference":
         rc = run_reference(args, world, rank)

@@ -13,12 +13,12 @@ from helpers import bits_equal, first_diff, host, product_close, to_fluid
 pytestmark = pytest.mark.gpu
 
 SHAPES = [
-    (37, 11, 9),     # x: row kernel, 1 cell/thread; y,z: march, single chunk
-    (600, 5, 4),     # x: row kernel, 2 cells/thread
-    (1100, 3, 4),    # x: march fallback (rows > 1024); y: 3-cell pencils
-    (8, 300, 6),     # y: march with several chunks per pencil
-    (6, 7, 130),     # z: march with several chunks per pencil
-    (5, 4, 3),       # tiny pencils
+    (37, 11, 9),     # x: row kernel, 1 cell/thread; y,z: tile kernel (odd nx), single chunk
+    (600, 5, 4),     # x: row kernel, 2 cells/thread; y,z: TMA pipeline with 5- and 4-cell pencils
+    (1100, 3, 4),    # x: chunked TMA pipeline (rows > 1024); y: 3-cell pencils
+    (8, 300, 6),     # y: TMA pipeline, pencils of 257-512 cells (two box rows, 2 cells/thread)
+    (6, 7, 130),     # z: TMA pipeline, 130-cell pencils
+    (5, 4, 3),       # tiny pencils; y,z: tile kernel
     (8, 140, 3),     # Xin-Jin y: pencil pairs of 129-256 cells with nx a multiple of 4
     (4, 3, 200),     # Xin-Jin z: the same
 ]
