@@ -9,6 +9,8 @@
 #include <cstdio>
 #include <mutex>
 
+#include <cuda.h>
+
 #include "ib_cfl.cuh"
 #include "ib_internal.cuh"
 
@@ -195,18 +197,42 @@ int launch_freeze_ptot(double *q, int64_t slab, const int grid[3], double gamma,
 // ------------------------------------------------------------------------------------------
 namespace ib {
 
-constexpr int kNoAllocMaxBlocks = 8192;        // one partial minimum per reduction block
-constexpr int kNoAllocCellsPerBlock = 256 * 64;  // 256 threads x 64 cells each
-// largest grid the fixed scratch covers: 8192 blocks x 16384 cells = 134,217,728 cells
-constexpr int64_t kNoAllocMaxCells = (int64_t)kNoAllocMaxBlocks * kNoAllocCellsPerBlock;
+constexpr int kNoAllocMaxBlocks = 8192;  // one partial minimum per reduction block
+// largest grid this entry point accepts (the documented limit; the kernel itself strides over
+// any number of cells with at most kNoAllocMaxBlocks blocks)
+constexpr int64_t kNoAllocMaxCells = (int64_t)134217728;
 
 // [0, 256): completion counter (first 4 bytes); [256, 256 + 8*8192): partial minima
 static __device__ __align__(256) unsigned char g_cfl_noalloc_scratch[256 + sizeof(double) * kNoAllocMaxBlocks];
 
-// Device address of the array per device, looked up once with that device current.  Host code
-// must not hand the symbol itself to a kernel: in host code it names a host-side stand-in.
-static unsigned char *g_noalloc_addr[64] = {nullptr};
+// Device address of the array, looked up with the device current and cached per device and
+// context: after a cudaDeviceReset, or under a context the caller made current through the
+// driver API, the module may be loaded at another address, so a new context looks it up again.
+// Host code must not hand the symbol itself to a kernel: in host code it names a host-side
+// stand-in.
+typedef CUresult (*PFN_ctx_get_current)(CUcontext *);
+struct NoAllocSlot {
+    CUcontext ctx = nullptr;
+    unsigned char *addr = nullptr;
+};
+static NoAllocSlot g_noalloc_slot[64];
 static std::mutex g_noalloc_mu;
+
+static CUcontext current_context()
+{
+    static PFN_ctx_get_current fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            return reinterpret_cast<PFN_ctx_get_current>(p);
+        cudaGetLastError();
+        return (PFN_ctx_get_current) nullptr;
+    }();
+    CUcontext c = nullptr;
+    if (fn && fn(&c) != CUDA_SUCCESS) c = nullptr;
+    return c;
+}
 
 static int noalloc_scratch(unsigned char **out)
 {
@@ -214,14 +240,19 @@ static int noalloc_scratch(unsigned char **out)
     int rc = check_cuda(cudaGetDevice(&dev));
     if (rc) return rc;
     if (dev < 0 || dev >= 64) return IB_ERROR_INVALID_ARGS;
+    // no context current yet on this thread (a first call): cudaGetSymbolAddress makes the
+    // device's primary context current, and the slot records that context afterwards
     std::lock_guard<std::mutex> g(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
+    NoAllocSlot &s = g_noalloc_slot[dev];
+    CUcontext ctx = current_context();
+    if (!s.addr || !ctx || ctx != s.ctx) {
         void *p = nullptr;
         rc = check_cuda(cudaGetSymbolAddress(&p, g_cfl_noalloc_scratch));
         if (rc) return rc;
-        g_noalloc_addr[dev] = static_cast<unsigned char *>(p);
+        s.addr = static_cast<unsigned char *>(p);
+        s.ctx = current_context();
     }
-    *out = g_noalloc_addr[dev];
+    *out = s.addr;
     return IB_SUCCESSFUL;
 }
 
@@ -258,7 +289,9 @@ extern "C" int ib_cflTimestepNoAlloc(const ib_fluid *fluid, double gamma, const 
     double hmin = geo->h[0];
     if (sim > 1 && geo->h[1] < hmin) hmin = geo->h[1];
     if (sim > 2 && geo->h[2] < hmin) hmin = geo->h[2];
-    const int nb = (int)std::max<int64_t>(1, (n + kNoAllocCellsPerBlock - 1) / kNoAllocCellsPerBlock);
+    // as many blocks as launch_cfl uses (the kernel strides over the cells), within the array
+    const int nb = (int)std::max<int64_t>(
+        1, std::min<int64_t>((n + 255) / 256, std::min<int64_t>((int64_t)4 * num_sms(), kNoAllocMaxBlocks)));
     const int halve = (method == IB_METHOD_HLL || method == IB_METHOD_HLLC) ? 1 : 0;
     const double gg1 = gamma * (gamma - 1);
     const int64_t slab = g.slab_pitch;

@@ -149,6 +149,52 @@ typedef struct ib_thermo {
 /* Smallest legal slab pitch (doubles) for an nx*ny*nz array: numel rounded up to 32. */
 IB_API int64_t ib_slab_pitch(int32_t nx, int32_t ny, int32_t nz);
 
+/* ---------------------------------------------------------------------------------------------
+ * The reference's GPU tags (for the mex glue).  A Matlab GPU array crosses into a mex function as
+ * an int64 vector (cudaCommon.h:184-196):
+ *   [dim0, dim1, dim2, numSlabs, halo, partitionDir, nGPUs, exteriorHalo, permtag,
+ *    circularBits, vectorComponent, (deviceID, devicePtr) x nGPUs]
+ * These calls decode tags into the structs of this header.  Host only: no device is touched.
+ * ------------------------------------------------------------------------------------------- */
+#define IB_GPU_TAG_LENGTH 11
+#define IB_GPU_TAG_DIM0 0
+#define IB_GPU_TAG_DIM1 1
+#define IB_GPU_TAG_DIM2 2
+#define IB_GPU_TAG_DIMSLAB 3
+#define IB_GPU_TAG_HALO 4
+#define IB_GPU_TAG_PARTDIR 5
+#define IB_GPU_TAG_NGPUS 6
+#define IB_GPU_TAG_EXTERIORHALO 7
+#define IB_GPU_TAG_PERMTAG 8
+#define IB_GPU_TAG_CIRCULARBITS 9
+#define IB_GPU_TAG_VECTOR_COMPONENT 10
+#define IB_GPU_TAG_MAX_GPUS 4 /* MAX_GPUS_USED, cudaCommon.h:11 */
+
+/* Replaces decodeMatlabBCs (gpuclass/cudaCommonML.cu:203-232): the IB_BC_* mode of one of the
+ * bcModes strings "circ", "const", "linear", "mirror", "bcstatic", "wall", "outflow",
+ * "freebalance"; IB_ERROR_INVALID_ARGS for any other string. */
+IB_API int ib_bcModeFromString(const char *name);
+
+/* Replaces deserializeTagToMGArray (gpuclass/cudaCommon.cu:117-170) for one array, with the
+ * checks of sanityCheckTag (cudaCommonML.cu:109-198): the device pointer, the extents and slab
+ * pitch (numel * 8 bytes rounded up to 256, in doubles), and optionally the vector component and
+ * the halo-sharing bits.  This library runs one GPU with arrays in XYZ order: a tag with
+ * nGPUs > 1 or a permtag other than 1 (or 0, unset) returns IB_ERROR_NOIMPLEMENT; a malformed tag
+ * IB_ERROR_INVALID_ARGS. */
+IB_API int ib_arrayFromGpuTag(const int64_t *tag, int32_t taglen, double **ptr, ib_grid *grid,
+                              int32_t *vector_component, int32_t *circular_bits);
+
+/* Replaces MGA_accessFluidCanister (gpuclass/cudaCommonML.cu:400-432): the tags of a fluid's
+ * mass, ener, mom(1), mom(2), mom(3) arrays into one ib_fluid.  The five must be slabs of one
+ * allocation at the pitch MGA_allocSlab gives them (cudaCommon.cu:339-370; otherwise
+ * IB_ERROR_NOIMPLEMENT), with equal extents, device and halo-sharing bits and vector components
+ * 0, 0, 1, 2, 3.  bc_modes: the six IB_BC_* modes [-X, +X, -Y, +Y, -Z, +Z] decoded from the
+ * arrays' boundaryData.bcModes (ib_bcModeFromString); a face whose circularBits bit is set must
+ * be IB_BC_CIRCULAR.  With bc_modes NULL every face must have its bit set and is circular.  The
+ * boundary depth is 4 (run/starterRun.m:60-67); statics lists are left empty. */
+IB_API int ib_fluidFromGpuTags(const int64_t *const tags[5], const int32_t taglen[5], const int32_t *bc_modes,
+                               ib_fluid *out);
+
 /* Human-readable name of a status code. */
 IB_API const char *ib_status_string(int status);
 
@@ -179,6 +225,29 @@ IB_API int ib_fluidstep(ib_fluid *fluids, const ib_fluid_thermo *thermo, int nfl
                  const ib_geometry *geo, const double *params, int nparams,
                  const ib_numerics *num, void *stream);
 
+/* Two-fluid drag as the source term of a complete timestep: fluids[0] is the gas, fluids[1] the
+ * dust; method is one of IB_DRAG_* (ib_cudaSource2FluidDrag). */
+typedef struct ib_drag_source {
+    ib_thermo thermo_gas;
+    ib_thermo thermo_dust;
+    int32_t method;
+    int32_t reserved;
+} ib_drag_source;
+
+/* Replaces performCompleteTimestep (gpuclass/flux_multi.cu:174-272), the fluid part of the
+ * flux_multi mex and of imogenCore's main loop (gpuimogen_core.cu:954-1054): source half step,
+ * forward fluid step of every fluid, full source step, backward fluid step, source half step.
+ * params = [dt, purehydro, iteration, method].  The source is the two-fluid drag when drag is
+ * not NULL (nfluids must then be 2); with drag == NULL there is none (the reference's srcType 0)
+ * and each fluid runs its forward and backward step back to back.  The backward step's sweep
+ * order is the forward one's reversed, so the forward step's last sweep and the backward step's
+ * first are along the same axis with the same dt; when the boundary fill between them has
+ * nothing to do (both faces of that axis periodic, no statics) the two run as one double-sweep
+ * launch (HLL/HLLC), which gives the same result as ib_fluidstep(+1) then ib_fluidstep(-1). */
+IB_API int ib_completeTimestep(ib_fluid *fluids, const ib_fluid_thermo *thermo, int nfluids,
+                               const ib_geometry *geo, const double *params, int nparams,
+                               const ib_numerics *num, const ib_drag_source *drag, void *stream);
+
 /* Replaces the cudaSoundspeed mex for hydro (gpuclass/cudaSoundspeed.cu:54-105,
  * calculateSoundspeed :107-150): cs_out[N] = sqrt(max(0, gamma(gamma-1) e_int / rho)). */
 IB_API int ib_cudaSoundspeed(const ib_fluid *fluid, double gamma, double *cs_out, void *stream);
@@ -203,9 +272,10 @@ IB_API int ib_cflTimestepFused(const ib_fluid *fluid, double gamma, const ib_geo
  * synchronisation cudaMalloc/cudaFree can cause.  The reduction's scratch is a fixed array built
  * into the library (about 64 KB on every GPU that loads it, kept until exit), so the call
  * allocates nothing; the result goes to *tau_device (caller-owned device memory) and the call
- * does not synchronise.  Limit: at most 134,217,728 cells (8192 reduction blocks of 16384
- * cells); larger grids return IB_ERROR_INVALID_ARGS.  The first call on a device looks up the
- * array's device address, so make that first call outside any stream capture.  All calls on a
+ * does not synchronise.  Limit: at most 134,217,728 cells; larger grids return
+ * IB_ERROR_INVALID_ARGS.  The first call on a device (and the first under each new context, e.g.
+ * after cudaDeviceReset) looks up the array's device address, so make that first call outside
+ * any stream capture.  All calls on a
  * device share the array (its counter is cleared at the start of each call): calls that overlap
  * on the GPU, e.g. on two streams, race. */
 IB_API int ib_cflTimestepNoAlloc(const ib_fluid *fluid, double gamma, const ib_geometry *geo, int method,

@@ -38,8 +38,10 @@ def _geometry(shape):
     return g
 
 
+# 256^3 folds the minima of hundreds of reduction blocks (4 per SM); (300, 1, 1) with method 3
+# is the 1-D Xin-Jin case, which takes the HLL reduction without the halving
 @pytest.mark.parametrize("shape,method", [((64, 48, 40), 2), ((64, 48, 40), 3), ((300, 1, 1), 1),
-                                          ((200, 150, 1), 2)])
+                                          ((300, 1, 1), 3), ((200, 150, 1), 2), ((256, 256, 256), 2)])
 def test_no_alloc_cfl_matches_fused(shape, method):
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
