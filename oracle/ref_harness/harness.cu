@@ -176,7 +176,13 @@ static int fluid_update_3d(MGArray *fluid, ParallelTopology *topo, FluidStepPara
         const int dir = fluxcall[n][sweep];
         if (fluid->dim[0] > 3) {
             sp.stepDirection = dir;
-            rc = performFluidUpdate_1D(fluid, sp, topo, &tmp);
+            // Xin-Jin sweeps get NULL, so the reference allocates their temporary itself: its
+            // Xin-Jin branch sets the kernels' scratch pointers (wStepValues, a local array,
+            // cudaFluidStep.cu:315) only when it allocates the temporary (:362-371), so with a
+            // temporary that an earlier sweep or transpose already allocated the pressure/freeze
+            // and Xin-Jin kernels would get uninitialised pointers (performFluidUpdate_3D,
+            // flux.cu, passes one temporary to every sweep of a step)
+            rc = performFluidUpdate_1D(fluid, sp, topo, sp.stepMethod == METHOD_XINJIN ? (MGArray *)NULL : &tmp);
             if (rc == SUCCESSFUL) rc = setFluidBoundary(fluid, &fsp.geometry, dir);
             if (rc == SUCCESSFUL) rc = exchange_MPI_Halos(fluid, 5, topo, dir);
         }

@@ -69,9 +69,22 @@ FLUID_CASES = [
     ("kh_hllc_mc_100", "kh", (20, 16, 12), 2, "mc", 5 / 3.0, -1.0, ["circular"] * 6, 0.4, 100),
     ("jumpy_hll_ospre_100", "jumpy", (16, 12, 10), 1, "ospre", 1.4, -1.0, ["circular"] * 6, 0.3, 100),
 ]
-# No multi-dimensional Xin-Jin case: on a 32x32x1 periodic grid the reference's Xin-Jin prediction
-# kernel (cukern_XinJinHydro_step, cudaFluidStep.cu:421, launched with a 32x4 block) made an illegal
-# memory access on a B200, so the reference's Xin-Jin path is only run in 1-D here.
+# Multi-dimensional Xin-Jin: the harness hands each Xin-Jin sweep a NULL temporary (see
+# oracle/ref_harness/harness.cu, fluid_update_3d): the reference's Xin-Jin branch initialises its
+# scratch pointers only when it allocates the temporary itself (cudaFluidStep.cu:315, 362-371).
+# With a reused temporary its second sweep of a step used uninitialised pointers, which is how an
+# earlier 32x32x1 run of this harness ended in an illegal memory access.
+# The extents are ones the reference's Xin-Jin launch covers: it sizes its grid with
+# ROUNDUPTO(n, blocksize.x - 4) (cudaFluidStep.cu:410, 458), and ROUNDUPTO (cudaCommon.h:170) does
+# not parenthesise its second argument, so the grid holds (n + 24 - n % 32) / 28 blocks of 28
+# cells (n when n % 32 == 4): too few for many n (12 cells: no block at all, a launch error; 200
+# cells: 196 updated).  32, 64 and 256 are covered.
+FLUID_CASES += [
+    ("kh_xj_100", "kh", (32, 32, 32), 3, "ospre", 5 / 3.0, -1.0, ["circular"] * 6, 0.4, 100),
+    ("jumpy_xj_3d_bc", "jumpy", (32, 32, 32), 3, "ospre", 1.4, -1.0,
+     ["const", "const", "mirror", "mirror", "circular", "circular"], 0.3, 4),
+    ("kh_xj_2d", "kh", (32, 32, 1), 3, "ospre", 5 / 3.0, -1.0, ["circular"] * 6, 0.4, 6),
+]
 
 
 def make_input(gen, shape, gamma):
