@@ -7,7 +7,8 @@ call forms of the reference's mex functions.
 """
 from .imogen import (BC, DRAG, FLUXLIM, METHOD, PRECISION, SLOPE, Fluid, Geometry, ImogenError,  # noqa: F401
                      cflTimestep, cflTimestepFused, cudaFluidStep, cudaSoundspeed, cudaSource2FluidDrag,
-                     cudaStatics, device_wait_status, fluidstep, freezeAndPtot, load, numerics, setFluidBoundary,
+                     cudaStatics, completeTimestep, device_wait_status, fluidstep, freezeAndPtot, load, numerics,
+                     setFluidBoundary,
                      slab_pitch, use_variant)
 from .timestep import TimeManager, cfl_tau, run_iteration  # noqa: F401
 
@@ -15,4 +16,5 @@ __all__ = [
     "Fluid", "Geometry", "ImogenError", "TimeManager", "cudaFluidStep", "fluidstep", "cflTimestep",
     "cflTimestepFused", "cudaSoundspeed", "freezeAndPtot", "cudaStatics", "setFluidBoundary",
     "cudaSource2FluidDrag", "numerics", "load", "use_variant", "run_iteration", "cfl_tau", "device_wait_status",
+    "completeTimestep",
 ]

@@ -37,6 +37,7 @@ SOURCES = [
     "ib_reduce.cu",
     "ib_boundary.cu",
     "ib_drag.cu",
+    "ib_tags.cu",
 ]
 HEADERS = ["ib_common.cuh", "ib_internal.cuh", "ib_sweep.cuh", "ib_sweep_launch.cuh", "ib_tma.cuh", "ib_bc.cuh", "ib_cfl.cuh", "ib_drag.cuh", "ib_tcgen05.cuh"]
 

@@ -141,14 +141,15 @@ double *Scratch::bytes(size_t nbytes)
 }
 
 int launch_sweep(int method, int slope, int precision, int dir, double *q, int64_t slab, const int grid[3],
-                 double lambda, double gamma, double rho_min, double c_iso, cudaStream_t st)
+                 double lambda, double gamma, double rho_min, double c_iso, cudaStream_t st, int nsweep)
 {
     if (method == IB_METHOD_HLLC) {
         if (precision == IB_PREC_FP32_FLUX)
-            return launch_hllc32(slope, dir, q, slab, grid, lambda, gamma, rho_min, c_iso, st);
-        return launch_hllc64(slope, dir, q, slab, grid, lambda, gamma, rho_min, c_iso, st);
+            return launch_hllc32(slope, dir, q, slab, grid, lambda, gamma, rho_min, c_iso, st, nsweep);
+        return launch_hllc64(slope, dir, q, slab, grid, lambda, gamma, rho_min, c_iso, st, nsweep);
     }
-    if (method == IB_METHOD_HLL) return launch_hll64(slope, dir, q, slab, grid, lambda, gamma, rho_min, c_iso, st);
+    if (method == IB_METHOD_HLL)
+        return launch_hll64(slope, dir, q, slab, grid, lambda, gamma, rho_min, c_iso, st, nsweep);
     return IB_ERROR_INVALID_ARGS;
 }
 
@@ -192,17 +193,24 @@ static int get_numerics(const ib_numerics *num, Numerics &n)
     return IB_SUCCESSFUL;
 }
 
-// One directional update (performFluidUpdate_1D); gamma already 2 for isothermal fluids.
+// One directional update (performFluidUpdate_1D); gamma already 2 for isothermal fluids.  With
+// nsweep = 2 the same update is applied twice in a row (HLL/HLLC: one launch where the kernel
+// allows it; Xin-Jin: two launches).
 static int fluid_update_1d(ib_fluid *f, const ib_geometry *geo, int method, int dir, double dt, double gamma,
-                           double rho_min, double c_iso, const Numerics &nm, cudaStream_t st)
+                           double rho_min, double c_iso, const Numerics &nm, cudaStream_t st, int nsweep = 1)
 {
     const int grid[3] = {f->grid.nx, f->grid.ny, f->grid.nz};
     if (grid[dir - 1] < 3) return IB_SUCCESSFUL;  // cudaFluidStep.cu:313
     const double lambda = dt / geo->h[dir - 1];
-    if (method == IB_METHOD_XINJIN)
-        return launch_xj_sweep(nm.flim, dir, f->q, f->grid.slab_pitch, grid, lambda, gamma, rho_min, st);
+    if (method == IB_METHOD_XINJIN) {
+        for (int k = 0; k < nsweep; k++) {
+            int rc = launch_xj_sweep(nm.flim, dir, f->q, f->grid.slab_pitch, grid, lambda, gamma, rho_min, st);
+            if (rc) return rc;
+        }
+        return IB_SUCCESSFUL;
+    }
     return launch_sweep(method, nm.slope, nm.prec, dir, f->q, f->grid.slab_pitch, grid, lambda, gamma, rho_min, c_iso,
-                        st);
+                        st, nsweep);
 }
 
 static bool has_statics(const ib_fluid *f)
@@ -230,6 +238,94 @@ static int fluid_boundary(ib_fluid *f, int dir, cudaStream_t st)
         bc1[2 * (dir - 1) + (1 - side)] = IB_BC_CIRCULAR;
         if ((rc = launch_fluid_boundary(f->q, S, grid, bc1, f->halo, dir, st))) return rc;
     }
+    return IB_SUCCESSFUL;
+}
+
+// The sweep directions of one fluid step (performFluidUpdate_3D, flux.cu:27-165): sweep index
+// (iteration + 3 [direction > 0]) mod 6 selects a row of the ordering table (flux.cu:46-49).  The
+// backward step's order is the forward one's reversed, so the last sweep of the forward step and
+// the first of the backward step are along the same axis.
+static void sweep_order(int step_number, int sweep_dir, int out[3])
+{
+    static const int fluxcall[3][6] = {{1, 2, 1, 2, 3, 3}, {3, 1, 2, 3, 1, 2}, {2, 3, 3, 1, 2, 1}};
+    const int sweep = (step_number + 3 * (sweep_dir > 0)) % 6;
+    for (int n = 0; n < 3; n++) out[n] = fluxcall[n][(sweep + 6) % 6];
+}
+
+struct FluidParams {
+    double gamma, rho_min, c_iso;
+};
+
+static FluidParams fluid_params(const ib_fluid_thermo &t)
+{
+    FluidParams p{t.gamma, t.rho_min, t.c_isothermal};
+    if (p.c_iso != -1) p.gamma = 2;  // flux_ML_iface.cu:140-143
+    return p;
+}
+
+// One sweep of a fluid step and the boundary fill after it (flux.cu:102-110).
+static int sweep_and_fill(ib_fluid *f, const ib_geometry *geo, int method, int d, double dt, const FluidParams &fp,
+                          const Numerics &nm, cudaStream_t st, int nsweep = 1)
+{
+    const int ext[3] = {f->grid.nx, f->grid.ny, f->grid.nz};
+    if (ext[d - 1] <= 3) return IB_SUCCESSFUL;
+    int rc = fluid_update_1d(f, geo, method, d, dt, fp.gamma, fp.rho_min, fp.c_iso, nm, st, nsweep);
+    if (rc) return rc;
+    return fluid_boundary(f, d, st);
+}
+
+// One fluid step (forward or backward) of one fluid, all three sweeps; 1-D grids take the
+// shortcut of flux.cu:35-68 (one x sweep).
+static int fluid_step_one(ib_fluid *f, const ib_geometry *geo, int method, double dt, const FluidParams &fp,
+                          const Numerics &nm, int sweep_dir, int step_number, cudaStream_t st)
+{
+    const int ext[3] = {f->grid.nx, f->grid.ny, f->grid.nz};
+    if (ext[1] == 1 && ext[2] == 1) {
+        int rc = fluid_update_1d(f, geo, method, 1, dt, fp.gamma, fp.rho_min, fp.c_iso, nm, st);
+        if (rc) return rc;
+        return fluid_boundary(f, 1, st);
+    }
+    int order[3];
+    sweep_order(step_number, sweep_dir, order);
+    for (int n = 0; n < 3; n++) {
+        int rc = sweep_and_fill(f, geo, method, order[n], dt, fp, nm, st);
+        if (rc) return rc;
+    }
+    return IB_SUCCESSFUL;
+}
+
+// Forward then backward fluid step of one fluid with nothing in between.  The forward step's
+// last sweep and the backward step's first are along the same axis d with the same dt; when the
+// boundary fill between them does nothing (both faces of d periodic, no statics) they are one
+// double-sweep launch: the same updates in the same order, so the result is identical.
+static int fluid_fwd_bwd(ib_fluid *f, const ib_geometry *geo, int method, double dt, const FluidParams &fp,
+                         const Numerics &nm, int step_number, cudaStream_t st)
+{
+    const int ext[3] = {f->grid.nx, f->grid.ny, f->grid.nz};
+    const bool one_d = ext[1] == 1 && ext[2] == 1;
+    int fwd[3], bwd[3];
+    if (one_d) {
+        fwd[0] = fwd[1] = fwd[2] = 1;
+    } else {
+        sweep_order(step_number, 1, fwd);
+        sweep_order(step_number, -1, bwd);
+    }
+    const int d = one_d ? 1 : fwd[2];
+    const bool fuse = (one_d || bwd[0] == d) && ext[d - 1] > 3 && f->bc[2 * (d - 1)] == IB_BC_CIRCULAR &&
+                      f->bc[2 * (d - 1) + 1] == IB_BC_CIRCULAR && !has_statics(f);
+    if (!fuse) {
+        int rc = fluid_step_one(f, geo, method, dt, fp, nm, 1, step_number, st);
+        if (rc) return rc;
+        return fluid_step_one(f, geo, method, dt, fp, nm, -1, step_number, st);
+    }
+    int rc;
+    if (!one_d)
+        for (int n = 0; n < 2; n++)
+            if ((rc = sweep_and_fill(f, geo, method, fwd[n], dt, fp, nm, st))) return rc;
+    if ((rc = sweep_and_fill(f, geo, method, d, dt, fp, nm, st, 2))) return rc;
+    if (!one_d)
+        for (int n = 1; n < 3; n++)
+            if ((rc = sweep_and_fill(f, geo, method, bwd[n], dt, fp, nm, st))) return rc;
     return IB_SUCCESSFUL;
 }
 
@@ -309,7 +405,6 @@ int ib_cudaFluidStep(ib_fluid *fluid, const ib_geometry *geo, const double *para
 int ib_fluidstep(ib_fluid *fluids, const ib_fluid_thermo *thermo, int nfluids, const ib_geometry *geo,
                  const double *params, int nparams, const ib_numerics *num, void *stream)
 {
-    static const int fluxcall[3][6] = {{1, 2, 1, 2, 3, 3}, {3, 1, 2, 3, 1, 2}, {2, 3, 3, 1, 2, 1}};
     int rc;
     if (!fluids || !thermo || !geo || !params) return IB_ERROR_NULL_POINTER;
     if (nparams != 5 || nfluids < 1) return IB_ERROR_INVALID_ARGS;
@@ -325,27 +420,57 @@ int ib_fluidstep(ib_fluid *fluids, const ib_fluid_thermo *thermo, int nfluids, c
     if (method < IB_METHOD_HLL || method > IB_METHOD_XINJIN) return IB_ERROR_INVALID_ARGS;
     cudaStream_t st = (cudaStream_t)stream;
     for (int fi = 0; fi < nfluids; fi++) {
-        ib_fluid *f = &fluids[fi];
-        if ((rc = validate_fluid(f))) return rc;
-        double gamma = thermo[fi].gamma, c_iso = thermo[fi].c_isothermal;
-        if (c_iso != -1) gamma = 2;  // flux_ML_iface.cu:140-143
-        const double rho_min = thermo[fi].rho_min;
-        const int ext[3] = {f->grid.nx, f->grid.ny, f->grid.nz};
-        if (ext[1] == 1 && ext[2] == 1) {  // flux.cu:35-68
-            if ((rc = fluid_update_1d(f, geo, method, 1, dt, gamma, rho_min, c_iso, nm, st))) return rc;
-            if ((rc = fluid_boundary(f, 1, st))) return rc;
-            continue;
-        }
-        const int sweep = (step_number + 3 * (sweep_dir > 0)) % 6;
-        for (int n = 0; n < 3; n++) {
-            const int d = fluxcall[n][(sweep + 6) % 6];
-            if (ext[d - 1] > 3) {
-                if ((rc = fluid_update_1d(f, geo, method, d, dt, gamma, rho_min, c_iso, nm, st))) return rc;
-                if ((rc = fluid_boundary(f, d, st))) return rc;
-            }
-        }
+        if ((rc = validate_fluid(&fluids[fi]))) return rc;
+        if ((rc = fluid_step_one(&fluids[fi], geo, method, dt, fluid_params(thermo[fi]), nm, sweep_dir, step_number,
+                                 st)))
+            return rc;
     }
     return IB_SUCCESSFUL;
+}
+
+int ib_completeTimestep(ib_fluid *fluids, const ib_fluid_thermo *thermo, int nfluids, const ib_geometry *geo,
+                        const double *params, int nparams, const ib_numerics *num, const ib_drag_source *drag,
+                        void *stream)
+{
+    int rc;
+    if (!fluids || !thermo || !geo || !params) return IB_ERROR_NULL_POINTER;
+    if (nparams != 4 || nfluids < 1) return IB_ERROR_INVALID_ARGS;
+    Numerics nm;
+    if ((rc = get_numerics(num, nm))) return rc;
+    if (geo->shape != 0) return IB_ERROR_NOIMPLEMENT;
+    const double dt = params[0];
+    const int purehydro = (int)params[1];
+    const int step_number = (int)params[2];
+    const int method = (int)params[3];
+    if (purehydro != 1) return IB_ERROR_NOIMPLEMENT;
+    if (method < IB_METHOD_HLL || method > IB_METHOD_XINJIN) return IB_ERROR_INVALID_ARGS;
+    if (drag && nfluids != 2) return IB_ERROR_INVALID_ARGS;  // gas and dust
+    for (int fi = 0; fi < nfluids; fi++)
+        if ((rc = validate_fluid(&fluids[fi]))) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!drag) {
+        // no source between the two fluid steps (srcType 0, flux_multi.cu:161-163): the fluids
+        // are independent, each runs forward then backward
+        for (int fi = 0; fi < nfluids; fi++)
+            if ((rc = fluid_fwd_bwd(&fluids[fi], geo, method, dt, fluid_params(thermo[fi]), nm, step_number, st)))
+                return rc;
+        return IB_SUCCESSFUL;
+    }
+    // two-fluid drag (flux_multi.cu:174-272): drag dt/2, forward, drag dt, backward, drag dt/2
+    auto source = [&](double h) {
+        const double dp[2] = {h, (double)drag->method};
+        return ib_cudaSource2FluidDrag(&fluids[0], &fluids[1], &drag->thermo_gas, &drag->thermo_dust, geo, dp, 2,
+                                       stream);
+    };
+    if ((rc = source(0.5 * dt))) return rc;
+    for (int fi = 0; fi < 2; fi++)
+        if ((rc = fluid_step_one(&fluids[fi], geo, method, dt, fluid_params(thermo[fi]), nm, 1, step_number, st)))
+            return rc;
+    if ((rc = source(dt))) return rc;
+    for (int fi = 0; fi < 2; fi++)
+        if ((rc = fluid_step_one(&fluids[fi], geo, method, dt, fluid_params(thermo[fi]), nm, -1, step_number, st)))
+            return rc;
+    return source(0.5 * dt);
 }
 
 int ib_cudaSoundspeed(const ib_fluid *fluid, double gamma, double *cs_out, void *stream)

@@ -44,7 +44,7 @@ Scratch &scratch();
 
 // Launchers (return IB_* status)
 int launch_sweep(int method, int slope, int precision, int dir, double *q, int64_t slab, const int grid[3],
-                 double lambda, double gamma, double rho_min, double c_iso, cudaStream_t st);
+                 double lambda, double gamma, double rho_min, double c_iso, cudaStream_t st, int nsweep = 1);
 int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
                     double rho_min, cudaStream_t st);
 int launch_cfl(const double *q, const double *cs, int64_t slab, const int grid[3], const ib_geometry *geo,

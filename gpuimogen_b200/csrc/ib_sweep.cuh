@@ -9,12 +9,12 @@
 //  * row kernel (x sweeps, rows up to 1024 cells): one CTA holds one whole periodic row, one
 //    thread per cell (or two), neighbours exchanged through two shared-memory planes;
 //    coalesced loads and stores, no halo recomputation.
-//  * march kernel (y and z sweeps; x sweeps of longer rows): one thread marches along a chunk
-//    of one pencil keeping a sliding window of the stencil in registers, lanes of a warp on
-//    neighbouring pencils so every load and store is a full 256-byte line.  All chunks of a
-//    pencil live in the same CTA: each chunk defers writing its first four outputs until
-//    every chunk has finished reading (they are its left neighbour's right halo) and writes
-//    its others only after a barrier that follows every chunk's reads of its left halo.
+//  * pipeline kernels (y and z sweeps of pencils up to 512 cells): persistent CTAs walk blocks
+//    of adjacent whole pencils that arrive by TMA, double-buffered, and leave by TMA store.
+//  * chunked pipeline (pencils above 512 cells): chunks with 4 halo rows per side, the halos
+//    copied to a side buffer first so every chunk is an independent job.
+//  * tile kernel (whatever the TMA rules exclude: odd nx, long odd rows): a CTA walks four
+//    neighbouring pencils in chunks staged in shared memory.
 #pragma once
 
 #include "ib_common.cuh"
@@ -229,7 +229,8 @@ struct SweepArgs {
 template <int CPT, int NFIX>
 __host__ __device__ constexpr bool row_ssum() { return CPT == 1 && NFIX != 512; }
 
-template <int METHOD, int SLOPE, typename FT, int CPT, int NFIX = 0>
+// NS: sweeps applied in a row (1, or 2 for the two same-axis sweeps in the middle of an iteration)
+template <int METHOD, int SLOPE, typename FT, int CPT, int NFIX = 0, int NS = 1>
 __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_kernel(SweepArgs a, FluidConsts<FT> c)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -253,6 +254,17 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
         for (int k = 0; k < 5; k++) u0[m][k] = act[m] ? q[(int64_t)slot_of<METHOD, 1>(k) * S + i] : 1.0;
     }
 
+#pragma unroll
+    for (int sw = 0; sw < NS; sw++) {
+    if (NS > 1 && sw > 0) {
+        // the next sweep starts from this one's result; every thread must be done reading the
+        // planes before they are rewritten
+#pragma unroll
+        for (int m = 0; m < CPT; m++)
+#pragma unroll
+            for (int k = 0; k < 5; k++) u0[m][k] = u1[m][k];
+        __syncthreads();
+    }
 #pragma unroll
     for (int stage = 0; stage < 2; stage++) {
         double (*u)[5] = (stage == 0) ? u0 : u1;
@@ -322,6 +334,7 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
         }
         if (stage == 0) __syncthreads();
     }
+    }
 #pragma unroll
     for (int m = 0; m < CPT; m++) {
         int i = threadIdx.x + m * blockDim.x;
@@ -376,7 +389,8 @@ __device__ __forceinline__ void pipe_store(const CUtensorMap *tm, const double *
     else tma_store_5d(tm, src, (int)(b % a.npw) * W, 0, 0, (int)(b / a.npw), 0);
 }
 
-template <int METHOD, int SLOPE, typename FT, int DIR, int W, int CPT, int NFIX = 0>
+// NS: sweeps applied to each block in a row (1 or 2)
+template <int METHOD, int SLOPE, typename FT, int DIR, int W, int CPT, int NFIX = 0, int NS = 1>
 __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
     sweep_pipe_kernel(const __grid_constant__ CUtensorMap tm, PipeArgs a, FluidConsts<FT> c)
 {
@@ -460,6 +474,17 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
             for (int k = 0; k < 5; k++) u0[m][k] = act[m] ? Ut[SI(slots[k], ci[m])] : 1.0;
         V5<FT> keep[CPT];
 #pragma unroll
+        for (int sw = 0; sw < NS; sw++) {
+        if (NS > 1 && sw > 0) {
+            // the next sweep starts from this one's result in the output tile (each thread reads
+            // the cells it wrote); the planes are rewritten only after every thread is done
+#pragma unroll
+            for (int m = 0; m < CPT; m++)
+#pragma unroll
+                for (int k = 0; k < 5; k++) u0[m][k] = act[m] ? O[SI(slots[k], ci[m])] : 1.0;
+            __syncthreads();
+        }
+#pragma unroll
         for (int stage = 0; stage < 2; stage++) {
             double (*u)[5] = (stage == 0) ? u0 : u1;
 #pragma unroll
@@ -478,7 +503,7 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
                 }
             }
             __syncthreads();
-            if (stage == 0 && leader) {
+            if (stage == 0 && sw == 0 && leader) {
                 // every thread has read tile t: prefetch the block after next into it
                 const int64_t bn = b + 2 * step;
                 if (bn < a.nblocks) {
@@ -535,9 +560,10 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
             }
             if (stage == 0) {
                 // the previous block's store must have read O before stage 1 rewrites it
-                if (leader) bulk_wait_read_all();
+                if (leader && sw == 0) bulk_wait_read_all();
                 __syncthreads();
             }
+        }
         }
         fence_proxy_async_smem();
         __syncthreads();
@@ -555,7 +581,7 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
 // shared-memory planes sized for one group.  Results overwrite the tile in place and leave by one
 // TMA store, so two tiles fit: the refill of a tile is issued after the store from it has read
 // it, one block ahead (block b + grid is requested while block b is computed).
-template <int METHOD, int SLOPE, typename FT, int DIR, int W, int G, int CPT, int NFIX = 0>
+template <int METHOD, int SLOPE, typename FT, int DIR, int W, int G, int CPT, int NFIX = 0, int NS = 1>
 __global__ void __launch_bounds__(512, 1)
     sweep_pipe_wide_kernel(const __grid_constant__ CUtensorMap tm, PipeArgs a, FluidConsts<FT> c)
 {
@@ -633,6 +659,16 @@ __global__ void __launch_bounds__(512, 1)
                 for (int k = 0; k < 5; k++) u0[m][k] = act[m] ? Ut[TI(slots[k], ci[m])] : 1.0;
             V5<FT> keep[CPT];
 #pragma unroll
+            for (int sw = 0; sw < NS; sw++) {
+            if (NS > 1 && sw > 0) {
+                // the previous sweep's result, in place in the tile (each thread's own cells);
+                // the loop below ends with a barrier, so the planes are free
+#pragma unroll
+                for (int m = 0; m < CPT; m++)
+#pragma unroll
+                    for (int k = 0; k < 5; k++) u0[m][k] = act[m] ? Ut[TI(slots[k], ci[m])] : 1.0;
+            }
+#pragma unroll
             for (int stage = 0; stage < 2; stage++) {
                 double (*u)[5] = (stage == 0) ? u0 : u1;
 #pragma unroll
@@ -644,7 +680,7 @@ __global__ void __launch_bounds__(512, 1)
                     }
                 }
                 __syncthreads();
-                if (stage == 0 && g == 0 && it > 0 && leader) {
+                if (stage == 0 && sw == 0 && g == 0 && it > 0 && leader) {
                     // the other tile's block has been stored: once that store has read it,
                     // request the next block into it
                     bulk_wait_read_all();
@@ -695,7 +731,8 @@ __global__ void __launch_bounds__(512, 1)
                         }
                     }
                 }
-                __syncthreads();  // the planes are rewritten next (stage 1, or the next group)
+                __syncthreads();  // the planes are rewritten next (stage 1, the next sweep or group)
+            }
             }
         }
         fence_proxy_async_smem();
@@ -933,150 +970,11 @@ __global__ void __launch_bounds__(512, 2)
 // stage_prims floors u in place, and u1 holds the floored prediction.  Both match the
 // reference, whose pressure passes write the floors back to memory before each stage.
 
-// ------------------------------------------------------------------------------------------
-// March kernel: blockDim = (PW pencils, C chunks); chunk c of pencil p covers cells
-// [c*L, min((c+1)*L, n)).  Shared memory: deferred first-four outputs, 20 doubles per thread.
-// ------------------------------------------------------------------------------------------
-struct MarchArgs {
-    double *q;
-    int64_t slab;
-    int nx, ny, nz;
-    int n;            // pencil length
-    int64_t npencil;
-    int L;            // chunk length
-    double lambda;
-};
-
 __device__ __forceinline__ int mod_n(int j, int n)
 {
     int r = j % n;
     return r < 0 ? r + n : r;
 }
-
-template <int METHOD, int SLOPE, typename FT, int DIR>
-__global__ void __launch_bounds__(256) sweep_march_kernel(MarchArgs a, FluidConsts<FT> c)
-{
-    extern __shared__ __align__(16) double defer[];  // [20][blockDim.x*blockDim.y]
-    const int nthr = blockDim.x * blockDim.y;
-    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int chunk = threadIdx.y;
-    const int n = a.n;
-    const bool live_p = p < a.npencil;
-    const int j0 = chunk * a.L;
-    const int j1 = min(j0 + a.L, n);
-    const bool live = live_p && (j0 < n);
-    const int64_t S = a.slab;
-    const double lambda = a.lambda;
-
-    int64_t base, stride;
-    if (DIR == 1) { base = p * a.nx; stride = 1; }
-    else if (DIR == 2) { base = (p % a.nx) + (int64_t)a.nx * a.ny * (p / a.nx); stride = a.nx; }
-    else { base = p; stride = (int64_t)a.nx * a.ny; }
-    double *q = a.q + (live ? base : 0);
-
-    constexpr int s0 = slot_of<METHOD, DIR>(0), s1 = slot_of<METHOD, DIR>(1), s2 = slot_of<METHOD, DIR>(2),
-                  s3 = slot_of<METHOD, DIR>(3), s4 = slot_of<METHOD, DIR>(4);
-
-    // Sliding windows.  At step s the cell j = j0-4+s arrives:
-    //   stage A: prims of j-1 (wA), its backward difference (dA), right face of j-2 (RA),
-    //            flux through face j-5/2 (FA), U0 history j-1..j-4 (ua1..ua4)
-    //   stage B works on k = j-2 with the same roles (wB, dB, RB, FB), U1 history k-1, k-2
-    V5<FT> wA, dA, RA, FA;
-    V5<FT> wB, dB, RB, FB;
-    double ua1[5], ua2[5], ua3[5], ua4[5];
-    double ub1[5], ub2[5];
-    double nxt[5];
-
-    const int nsteps = (j1 - j0) + 8;
-    if (live) {
-        int64_t off = (int64_t)mod_n(j0 - 4, n) * stride;
-        nxt[0] = q[s0 * S + off]; nxt[1] = q[s1 * S + off]; nxt[2] = q[s2 * S + off];
-        nxt[3] = q[s3 * S + off]; nxt[4] = q[s4 * S + off];
-    }
-
-    auto step = [&](int s) {
-        const int j = j0 - 4 + s;
-        double u[5];
-#pragma unroll
-        for (int k = 0; k < 5; k++) u[k] = nxt[k];
-        if (s + 1 < nsteps) {  // prefetch the next cell
-            int64_t off = (int64_t)mod_n(j + 1, n) * stride;
-            nxt[0] = q[s0 * S + off]; nxt[1] = q[s1 * S + off]; nxt[2] = q[s2 * S + off];
-            nxt[3] = q[s3 * S + off]; nxt[4] = q[s4 * S + off];
-        }
-        // ---- stage A ----
-        V5<FT> w = stage_prims<METHOD, DIR, FT>(u, c);  // floors u in place for HLL
-        V5<FT> d = v5_sub(w, wA);
-        V5<FT> Lf, Rf, f;
-        double u1[5];
-        if (s >= 2) stage_faces<METHOD, SLOPE, FT>(c, wA, dA, d, Lf, Rf);  // faces of j-1
-        if (s >= 3) f = stage_flux<METHOD, FT>(c, RA, Lf);                 // face j-3/2
-        if (s >= 4) {                                                       // U1[j-2]
-#pragma unroll
-            for (int k = 0; k < 5; k++) u1[k] = ua2[k] - lambda * ((double)f.a[k] - (double)FA.a[k]);
-        }
-        if (s >= 2) RA = Rf;
-        if (s >= 3) FA = f;
-        dA = d;
-        wA = w;
-        // ---- stage B on k = j-2 ----
-        if (s >= 4) {
-            const int sb = s - 4;
-            V5<FT> wb = stage_prims<METHOD, DIR, FT>(u1, c);  // floors u1 in place for HLL
-            V5<FT> db = v5_sub(wb, wB);
-            V5<FT> Lb, Rb, fb;
-            if (sb >= 2) stage_faces<METHOD, SLOPE, FT>(c, wB, dB, db, Lb, Rb);
-            if (sb >= 3) fb = stage_flux<METHOD, FT>(c, RB, Lb);
-            if (sb >= 4) {
-                // final update of cell k-2 = j-4: .5*(U1 + U0 - lambda*dF)
-                const int jo = j - 4;
-                double out[5];
-#pragma unroll
-                for (int k = 0; k < 5; k++)
-                    out[k] = .5 * (ub2[k] + ua4[k] - lambda * ((double)fb.a[k] - (double)FB.a[k]));
-                if (jo - j0 < 4) {
-                    const int slot = jo - j0;
-#pragma unroll
-                    for (int k = 0; k < 5; k++) defer[(slot * 5 + k) * nthr + tid] = out[k];
-                } else {
-                    int64_t off = (int64_t)jo * stride;
-                    q[s0 * S + off] = out[0]; q[s1 * S + off] = out[1]; q[s2 * S + off] = out[2];
-                    q[s3 * S + off] = out[3]; q[s4 * S + off] = out[4];
-                }
-            }
-            if (sb >= 2) RB = Rb;
-            if (sb >= 3) FB = fb;
-            dB = db;
-            wB = wb;
-#pragma unroll
-            for (int k = 0; k < 5; k++) { ub2[k] = ub1[k]; ub1[k] = u1[k]; }
-        }
-#pragma unroll
-        for (int k = 0; k < 5; k++) { ua4[k] = ua3[k]; ua3[k] = ua2[k]; ua2[k] = ua1[k]; ua1[k] = u[k]; }
-    };
-
-    // prologue: the first eight cells (j0-4 .. j0+3) are read before any chunk writes
-    if (live) {
-        for (int s = 0; s < 8 && s < nsteps; s++) step(s);
-    }
-    __syncthreads();
-    if (live) {
-        for (int s = 8; s < nsteps; s++) step(s);
-    }
-    __syncthreads();
-    if (live) {
-        for (int slot = 0; slot < 4 && j0 + slot < j1; slot++) {
-            int64_t off = (int64_t)(j0 + slot) * stride;
-            q[s0 * S + off] = defer[(slot * 5 + 0) * nthr + tid];
-            q[s1 * S + off] = defer[(slot * 5 + 1) * nthr + tid];
-            q[s2 * S + off] = defer[(slot * 5 + 2) * nthr + tid];
-            q[s3 * S + off] = defer[(slot * 5 + 3) * nthr + tid];
-            q[s4 * S + off] = defer[(slot * 5 + 4) * nthr + tid];
-        }
-    }
-}
-
 
 // ------------------------------------------------------------------------------------------
 // Tile-march kernel (y and z sweeps, long x rows).  One CTA owns W neighbouring pencils and

@@ -5,6 +5,7 @@
 #include "ib_sweep.cuh"
 
 #include <cstdlib>
+#include <type_traits>
 
 namespace ib {
 
@@ -49,7 +50,8 @@ int launch_tile_dw(double *q, int64_t slab, const int grid[3], double lambda, co
 // G > 1 selects sweep_pipe_wide_kernel: blocks of W*G columns (one TMA box), computed W at a time,
 // results stored from the input tile; pencils up to 256 cells, y/z sweeps only.
 template <int METHOD, int SLOPE, typename FT, int DIR, int W, int CPT, int NFIX = 0, int G = 1>
-int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c, cudaStream_t st)
+int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c, cudaStream_t st,
+                int nsweep)
 {
     const int nx = grid[0], ny = grid[1], nz = grid[2];
     const int n = grid[DIR - 1];
@@ -92,15 +94,20 @@ int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const
                        (size_t)10 * W * n * sizeof(FT);
     if (NFIX && n != NFIX) return IB_ERROR_NOIMPLEMENT;
     if (shm > 227 * 1024) return IB_ERROR_NOIMPLEMENT;
-    auto kern = [] {
-        if constexpr (G == 1) return &sweep_pipe_kernel<METHOD, SLOPE, FT, DIR, W, CPT, NFIX>;
-        else return &sweep_pipe_wide_kernel<METHOD, SLOPE, FT, DIR, W, G, CPT, NFIX>;
+    const int ns = (nsweep == 2) ? 2 : 1;
+    auto kern = [ns] {
+        if constexpr (G == 1)
+            return ns == 2 ? &sweep_pipe_kernel<METHOD, SLOPE, FT, DIR, W, CPT, NFIX, 2>
+                           : &sweep_pipe_kernel<METHOD, SLOPE, FT, DIR, W, CPT, NFIX, 1>;
+        else
+            return ns == 2 ? &sweep_pipe_wide_kernel<METHOD, SLOPE, FT, DIR, W, G, CPT, NFIX, 2>
+                           : &sweep_pipe_wide_kernel<METHOD, SLOPE, FT, DIR, W, G, CPT, NFIX, 1>;
     }();
-    static int attr_bytes = 0;
-    if ((int)shm > attr_bytes) {
+    static int attr_bytes[2] = {0, 0};
+    if ((int)shm > attr_bytes[ns - 1]) {
         rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
         if (rc) return rc;
-        attr_bytes = (int)shm;
+        attr_bytes[ns - 1] = (int)shm;
     }
     int per_sm = 0;
     rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, shm));
@@ -199,9 +206,12 @@ int launch_tile_t(int dir, double *q, int64_t slab, const int grid[3], double la
     return launch_tile_dw<METHOD, SLOPE, FT, 3, 4>(q, slab, grid, lambda, c, st, 56);
 }
 
+// One sweep along dir, or nsweep = 2 sweeps in a row with the same lambda (the two same-axis
+// sweeps in the middle of an iteration).  The row and pipeline kernels apply both to a block
+// while it is on chip; the chunked pipeline and the tile kernel are launched once per sweep.
 template <int METHOD, int SLOPE, typename FT>
 int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c,
-                   cudaStream_t st)
+                   cudaStream_t st, int nsweep = 1)
 {
     const int nx = grid[0], ny = grid[1], nz = grid[2];
     const int n = grid[dir - 1];
@@ -228,35 +238,35 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
             return (e && e[0] == '0') ? 0 : 1;
         }();
         if (dir == 1) {
-            if (n <= 256) rc = launch_pipe<METHOD, SLOPE, FT, 1, 1, 1>(q, slab, grid, lambda, c, st);
+            if (n <= 256) rc = launch_pipe<METHOD, SLOPE, FT, 1, 1, 1>(q, slab, grid, lambda, c, st, nsweep);
         } else if (n == 256 && !wide) {
-            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1, 256>(q, slab, grid, lambda, c, st);
-            else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1, 256>(q, slab, grid, lambda, c, st);
+            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1, 256>(q, slab, grid, lambda, c, st, nsweep);
+            else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1, 256>(q, slab, grid, lambda, c, st, nsweep);
         } else if (n == 128 && !wide) {
-            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1, 128>(q, slab, grid, lambda, c, st);
-            else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1, 128>(q, slab, grid, lambda, c, st);
+            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1, 128>(q, slab, grid, lambda, c, st, nsweep);
+            else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1, 128>(q, slab, grid, lambda, c, st, nsweep);
         } else if (n <= 256 && !wide) {
-            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1>(q, slab, grid, lambda, c, st);
-            else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1>(q, slab, grid, lambda, c, st);
+            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1>(q, slab, grid, lambda, c, st, nsweep);
+            else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1>(q, slab, grid, lambda, c, st, nsweep);
         } else if (n == 256) {
             // FP32 flux: 8-column blocks (64-byte rows) computed 4 columns at a time (3.48 -> 2.52
             // ms at 512 x 512 x 256).  FP64 is bound by its arithmetic there and keeps 4 columns:
             // its planes leave room for only 2 columns per group, which is slower.
             if constexpr (sizeof(FT) == 4) {
-                if (wide8 == 1) rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2, 256, 2>(q, slab, grid, lambda, c, st);
+                if (wide8 == 1) rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2, 256, 2>(q, slab, grid, lambda, c, st, nsweep);
             }
-            if (rc == IB_ERROR_NOIMPLEMENT) rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2, 256>(q, slab, grid, lambda, c, st);
+            if (rc == IB_ERROR_NOIMPLEMENT) rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2, 256>(q, slab, grid, lambda, c, st, nsweep);
         } else if (n <= 256) {
             if constexpr (sizeof(FT) == 4) {
-                if (wide8 == 1) rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2, 0, 2>(q, slab, grid, lambda, c, st);
+                if (wide8 == 1) rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2, 0, 2>(q, slab, grid, lambda, c, st, nsweep);
             }
-            if (rc == IB_ERROR_NOIMPLEMENT) rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2>(q, slab, grid, lambda, c, st);
+            if (rc == IB_ERROR_NOIMPLEMENT) rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2>(q, slab, grid, lambda, c, st, nsweep);
         } else if (n == 512) {
-            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 2, 512>(q, slab, grid, lambda, c, st);
-            else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 2, 512>(q, slab, grid, lambda, c, st);
+            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 2, 512>(q, slab, grid, lambda, c, st, nsweep);
+            else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 2, 512>(q, slab, grid, lambda, c, st, nsweep);
         } else {
-            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 2>(q, slab, grid, lambda, c, st);
-            else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 2>(q, slab, grid, lambda, c, st);
+            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 2>(q, slab, grid, lambda, c, st, nsweep);
+            else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 2>(q, slab, grid, lambda, c, st, nsweep);
         }
         if (rc != IB_ERROR_NOIMPLEMENT) return rc;
     }
@@ -268,6 +278,11 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
     }();
     if (use_pipe && use_chunk && n > 512 && (dir > 1 || nx > 1024)) {
         int rc;
+        if (nsweep > 1) {
+            rc = launch_sweep_t<METHOD, SLOPE, FT>(dir, q, slab, grid, lambda, c, st, 1);
+            if (rc) return rc;
+            return launch_sweep_t<METHOD, SLOPE, FT>(dir, q, slab, grid, lambda, c, st, nsweep - 1);
+        }
         if (dir == 1) rc = launch_chunk<METHOD, SLOPE, FT, 1, 1, 256>(q, slab, grid, lambda, c, st);
         else if (dir == 2) rc = launch_chunk<METHOD, SLOPE, FT, 2, 4, 128>(q, slab, grid, lambda, c, st);
         else rc = launch_chunk<METHOD, SLOPE, FT, 3, 4, 128>(q, slab, grid, lambda, c, st);
@@ -289,84 +304,69 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
         auto opt_in = [](auto kern, size_t bytes) {
             return check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
         };
-        if (cpt == 1) {
-            int nt = ((nx + 31) / 32) * 32;
-            const size_t max1 = (size_t)10 * 512 * sizeof(FT) + (size_t)40 * 512;
-            // common row lengths get the length at compile time (cheaper shared-memory indexing)
-            if (nx == 256) {
-                sweep_row_kernel<METHOD, SLOPE, FT, 1, 256><<<(unsigned)rows, nt, shm, st>>>(a, c);
-            } else if (nx == 512) {
-                static const int rc0 = opt_in(sweep_row_kernel<METHOD, SLOPE, FT, 1, 512>, max1);
-                if (rc0) return rc0;
-                sweep_row_kernel<METHOD, SLOPE, FT, 1, 512><<<(unsigned)rows, nt, shm, st>>>(a, c);
-            } else if (nx == 128) {
-                sweep_row_kernel<METHOD, SLOPE, FT, 1, 128><<<(unsigned)rows, nt, shm, st>>>(a, c);
+        auto launch_rows = [&](auto ns_tag) -> int {
+            constexpr int NS = decltype(ns_tag)::value;
+            if (cpt == 1) {
+                int nt = ((nx + 31) / 32) * 32;
+                const size_t max1 = (size_t)10 * 512 * sizeof(FT) + (size_t)40 * 512;
+                // common row lengths get the length at compile time (cheaper shared-memory indexing)
+                if (nx == 256) {
+                    sweep_row_kernel<METHOD, SLOPE, FT, 1, 256, NS><<<(unsigned)rows, nt, shm, st>>>(a, c);
+                } else if (nx == 512) {
+                    static const int rc0 = opt_in(sweep_row_kernel<METHOD, SLOPE, FT, 1, 512, NS>, max1);
+                    if (rc0) return rc0;
+                    sweep_row_kernel<METHOD, SLOPE, FT, 1, 512, NS><<<(unsigned)rows, nt, shm, st>>>(a, c);
+                } else if (nx == 128) {
+                    sweep_row_kernel<METHOD, SLOPE, FT, 1, 128, NS><<<(unsigned)rows, nt, shm, st>>>(a, c);
+                } else {
+                    static const int rc1 = opt_in(sweep_row_kernel<METHOD, SLOPE, FT, 1, 0, NS>, max1);
+                    if (rc1) return rc1;
+                    sweep_row_kernel<METHOD, SLOPE, FT, 1, 0, NS><<<(unsigned)rows, nt, shm, st>>>(a, c);
+                }
             } else {
-                static const int rc1 = opt_in(sweep_row_kernel<METHOD, SLOPE, FT, 1>, max1);
-                if (rc1) return rc1;
-                sweep_row_kernel<METHOD, SLOPE, FT, 1><<<(unsigned)rows, nt, shm, st>>>(a, c);
+                int nt = (((nx + 1) / 2 + 31) / 32) * 32;
+                static const int rc2 =
+                    opt_in(sweep_row_kernel<METHOD, SLOPE, FT, 2, 0, NS>, (size_t)10 * 1024 * sizeof(FT));
+                if (rc2) return rc2;
+                sweep_row_kernel<METHOD, SLOPE, FT, 2, 0, NS><<<(unsigned)rows, nt, shm, st>>>(a, c);
             }
-        } else {
-            int nt = (((nx + 1) / 2 + 31) / 32) * 32;
-            static const int rc2 = opt_in(sweep_row_kernel<METHOD, SLOPE, FT, 2>, (size_t)10 * 1024 * sizeof(FT));
-            if (rc2) return rc2;
-            sweep_row_kernel<METHOD, SLOPE, FT, 2><<<(unsigned)rows, nt, shm, st>>>(a, c);
-        }
+            return IB_SUCCESSFUL;
+        };
+        int rc = (nsweep == 2) ? launch_rows(std::integral_constant<int, 2>{})
+                               : launch_rows(std::integral_constant<int, 1>{});
+        if (rc) return rc;
         return check_launch();
     }
 
-    const int64_t npencil = N / n;
-    static const bool use_march = [] {
-        const char *e = getenv("IMOGEN_B200_MARCH");
-        return e && e[0] == '1';
-    }();
-    if (!use_march) return launch_tile_t<METHOD, SLOPE, FT>(dir, q, slab, grid, lambda, c, st);
-
-    // register-march kernel: PW pencils x C chunks per CTA, C*PW <= 256
-    int PW = 32;
-    if (dir == 1) PW = 32;  // lanes on different rows: correct, uncoalesced fallback for long rows
-    // target ~4 resident waves of threads; chunk length at least 16 cells
-    const int64_t target_threads = (int64_t)num_sms() * 1024;
-    int C = 1;
-    while (C < 64 && (npencil * C) < target_threads && n / (2 * C) >= 16) C *= 2;
-    while (PW * C > 256 && PW > 4) PW /= 2;
-    while (PW * C > 256) C /= 2;
-    int L = (n + C - 1) / C;
-    C = (n + L - 1) / L;
-    MarchArgs a{q, slab, nx, ny, nz, n, npencil, L, lambda};
-    dim3 block(PW, C);
-    dim3 gridd((unsigned)((npencil + PW - 1) / PW));
-    size_t shm = (size_t)20 * sizeof(double) * PW * C;
-    switch (dir) {
-    case 1: sweep_march_kernel<METHOD, SLOPE, FT, 1><<<gridd, block, shm, st>>>(a, c); break;
-    case 2: sweep_march_kernel<METHOD, SLOPE, FT, 2><<<gridd, block, shm, st>>>(a, c); break;
-    default: sweep_march_kernel<METHOD, SLOPE, FT, 3><<<gridd, block, shm, st>>>(a, c); break;
+    for (int k = 0; k < nsweep; k++) {
+        int rc = launch_tile_t<METHOD, SLOPE, FT>(dir, q, slab, grid, lambda, c, st);
+        if (rc) return rc;
     }
-    return check_launch();
+    return IB_SUCCESSFUL;
 }
 
 template <int METHOD, typename FT>
 int launch_sweep_slope(int slope, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
-                       double rho_min, double c_iso, cudaStream_t st)
+                       double rho_min, double c_iso, cudaStream_t st, int nsweep)
 {
     FluidConsts<FT> c = make_consts<FT>(gamma, rho_min, c_iso);
     switch (slope) {
-    case IB_SLOPE_OSPRE: return launch_sweep_t<METHOD, IB_SLOPE_OSPRE, FT>(dir, q, slab, grid, lambda, c, st);
-    case IB_SLOPE_MC: return launch_sweep_t<METHOD, IB_SLOPE_MC, FT>(dir, q, slab, grid, lambda, c, st);
-    case IB_SLOPE_VANLEER: return launch_sweep_t<METHOD, IB_SLOPE_VANLEER, FT>(dir, q, slab, grid, lambda, c, st);
-    case IB_SLOPE_MINMOD: return launch_sweep_t<METHOD, IB_SLOPE_MINMOD, FT>(dir, q, slab, grid, lambda, c, st);
-    case IB_SLOPE_SUPERBEE: return launch_sweep_t<METHOD, IB_SLOPE_SUPERBEE, FT>(dir, q, slab, grid, lambda, c, st);
-    case IB_SLOPE_VANALBADA: return launch_sweep_t<METHOD, IB_SLOPE_VANALBADA, FT>(dir, q, slab, grid, lambda, c, st);
-    case IB_SLOPE_ZERO: return launch_sweep_t<METHOD, IB_SLOPE_ZERO, FT>(dir, q, slab, grid, lambda, c, st);
+    case IB_SLOPE_OSPRE: return launch_sweep_t<METHOD, IB_SLOPE_OSPRE, FT>(dir, q, slab, grid, lambda, c, st, nsweep);
+    case IB_SLOPE_MC: return launch_sweep_t<METHOD, IB_SLOPE_MC, FT>(dir, q, slab, grid, lambda, c, st, nsweep);
+    case IB_SLOPE_VANLEER: return launch_sweep_t<METHOD, IB_SLOPE_VANLEER, FT>(dir, q, slab, grid, lambda, c, st, nsweep);
+    case IB_SLOPE_MINMOD: return launch_sweep_t<METHOD, IB_SLOPE_MINMOD, FT>(dir, q, slab, grid, lambda, c, st, nsweep);
+    case IB_SLOPE_SUPERBEE: return launch_sweep_t<METHOD, IB_SLOPE_SUPERBEE, FT>(dir, q, slab, grid, lambda, c, st, nsweep);
+    case IB_SLOPE_VANALBADA: return launch_sweep_t<METHOD, IB_SLOPE_VANALBADA, FT>(dir, q, slab, grid, lambda, c, st, nsweep);
+    case IB_SLOPE_ZERO: return launch_sweep_t<METHOD, IB_SLOPE_ZERO, FT>(dir, q, slab, grid, lambda, c, st, nsweep);
     default: return IB_ERROR_INVALID_ARGS;
     }
 }
 
 int launch_hllc64(int slope, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
-                  double rho_min, double c_iso, cudaStream_t st);
+                  double rho_min, double c_iso, cudaStream_t st, int nsweep);
 int launch_hllc32(int slope, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
-                  double rho_min, double c_iso, cudaStream_t st);
+                  double rho_min, double c_iso, cudaStream_t st, int nsweep);
 int launch_hll64(int slope, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
-                 double rho_min, double c_iso, cudaStream_t st);
+                 double rho_min, double c_iso, cudaStream_t st, int nsweep);
 
 }  // namespace ib

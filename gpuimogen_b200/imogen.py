@@ -82,6 +82,11 @@ class IbThermo(ctypes.Structure):
                 ("c_isothermal", ctypes.c_double)]
 
 
+class IbDragSource(ctypes.Structure):
+    _fields_ = [("thermo_gas", IbThermo), ("thermo_dust", IbThermo), ("method", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
 class IbDragModel(ctypes.Structure):
     _fields_ = [("params", ctypes.c_void_p), ("feature_shift", ctypes.c_float * 5),
                 ("feature_scale", ctypes.c_float * 5), ("out_shift", ctypes.c_float), ("out_scale", ctypes.c_float),
@@ -116,6 +121,10 @@ EXPORTS = {
     "ib_fluidstep": (ctypes.c_int, [ctypes.POINTER(IbFluid), ctypes.POINTER(IbFluidThermo), ctypes.c_int,
                                     ctypes.POINTER(IbGeometry), ctypes.POINTER(ctypes.c_double),
                                     ctypes.c_int, ctypes.POINTER(IbNumerics), ctypes.c_void_p]),
+    "ib_completeTimestep": (ctypes.c_int, [ctypes.POINTER(IbFluid), ctypes.POINTER(IbFluidThermo), ctypes.c_int,
+                                           ctypes.POINTER(IbGeometry), ctypes.POINTER(ctypes.c_double),
+                                           ctypes.c_int, ctypes.POINTER(IbNumerics), ctypes.POINTER(IbDragSource),
+                                           ctypes.c_void_p]),
     "ib_cudaSoundspeed": (ctypes.c_int, [ctypes.POINTER(IbFluid), ctypes.c_double, ctypes.c_void_p,
                                          ctypes.c_void_p]),
     "ib_cflTimestep": (ctypes.c_int, [ctypes.POINTER(IbFluid), ctypes.c_void_p, ctypes.POINTER(IbGeometry),
@@ -148,6 +157,12 @@ EXPORTS = {
     "ib_cflTimestepNoAlloc": (ctypes.c_int, [ctypes.POINTER(IbFluid), ctypes.c_double,
                                              ctypes.POINTER(IbGeometry), ctypes.c_int, ctypes.c_void_p,
                                              ctypes.c_void_p]),
+    "ib_bcModeFromString": (ctypes.c_int, [ctypes.c_char_p]),
+    "ib_arrayFromGpuTag": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p),
+                                          ctypes.POINTER(IbGrid), ctypes.POINTER(ctypes.c_int32),
+                                          ctypes.POINTER(ctypes.c_int32)]),
+    "ib_fluidFromGpuTags": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int32),
+                                           ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(IbFluid)]),
     "ib_freezeAndPtot": (ctypes.c_int, [ctypes.POINTER(IbFluid), ctypes.c_double, ctypes.c_int,
                                         ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
                                         ctypes.c_void_p]),
@@ -347,6 +362,27 @@ def fluidstep(fluids, geometry, params, num=None):
     p, n = _dvec(params)
     nm = ctypes.byref(num) if num is not None else None
     _check("ib_fluidstep", _lib().ib_fluidstep(fs, th, len(fluids), ctypes.byref(g), p, n, nm, _stream()))
+
+
+def completeTimestep(fluids, geometry, params, num=None, drag=None):
+    """performCompleteTimestep(fluids, [dt, purehydro, iteration, method]): source half step,
+    forward fluid step, source step, backward fluid step, source half step.  drag = (thermo_gas,
+    thermo_dust, method) makes fluids [gas, dust] exchange momentum by the two-fluid drag; without
+    it there is no source and the two same-axis sweeps mid-step run as one launch where they can."""
+    if isinstance(fluids, Fluid):
+        fluids = [fluids]
+    fs = (IbFluid * len(fluids))(*[f.c_struct() for f in fluids])
+    th = (IbFluidThermo * len(fluids))(*[f.thermo() for f in fluids])
+    g = geometry.c_struct()
+    p, n = _dvec(params)
+    nm = ctypes.byref(num) if num is not None else None
+    ds = None
+    if drag is not None:
+        tg, td, method = drag
+        ds = ctypes.byref(IbDragSource(thermo_struct(tg), thermo_struct(td),
+                                       DRAG[method] if isinstance(method, str) else int(method), 0))
+    _check("ib_completeTimestep", _lib().ib_completeTimestep(fs, th, len(fluids), ctypes.byref(g), p, n, nm, ds,
+                                                             _stream()))
 
 
 def cudaSoundspeed(fluid, gamma):

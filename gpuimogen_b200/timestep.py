@@ -53,17 +53,20 @@ def cfl_tau(fluids, geometry, method):
     return tau
 
 
-def run_iteration(fluids, geometry, tm, method, num=None, source=None):
-    """One main-loop iteration; `source(fluids, dt_fraction)` applies the sources if given."""
+def run_iteration(fluids, geometry, tm, method, num=None, source=None, drag=None):
+    """One main-loop iteration; `source(fluids, dt_fraction)` applies the sources if given
+    (forward and backward fluid steps through fluidstep, as the Matlab loop calls them);
+    otherwise the complete timestep runs through completeTimestep (performCompleteTimestep), with
+    the two-fluid drag between the steps when drag = (thermo_gas, thermo_dust, method)."""
     tau = cfl_tau(fluids, geometry, method)
     dt = tm.update(tau)
     if source is not None:
         source(fluids, 0.5 * dt)
-    ib.fluidstep(fluids, geometry, [dt, 1, 1, tm.iteration, method], num)
-    if source is not None:
+        ib.fluidstep(fluids, geometry, [dt, 1, 1, tm.iteration, method], num)
         source(fluids, dt)
-    ib.fluidstep(fluids, geometry, [dt, 1, -1, tm.iteration, method], num)
-    if source is not None:
+        ib.fluidstep(fluids, geometry, [dt, 1, -1, tm.iteration, method], num)
         source(fluids, 0.5 * dt)
+    else:
+        ib.completeTimestep(fluids, geometry, [dt, 1, tm.iteration, method], num, drag=drag)
     tm.step()
     return dt
