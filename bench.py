@@ -366,6 +366,168 @@ def cpu_reference_sample(shape, iterations=1):
     return cells * iterations / sec / 1e6, sec, threads
 
 
+def bench_config(shape, world):
+    """The workload's config dict, the same for both arms of the benchmark."""
+    return {"workload": "kelvin_helmholtz_3d_hllc_fp64", "grid": list(shape), "gamma": GAMMA, "cfl": CFL,
+            "limiter": "MC", "method": "HLLC", "time_scheme": "SSPRK2", "boundaries": "periodic",
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2_policy": "state %.0f MB > 126 MB L2, no flush needed"
+                         % (5 * 8 * ((shape[0] * shape[1] * shape[2] + 31) // 32 * 32) / 1e6)}
+
+
+def _stats(xs):
+    """Median and spread of repeated measurements."""
+    xs = sorted(xs)
+    return {"median": float(np.median(xs)), "min": float(xs[0]), "max": float(xs[-1]), "n": len(xs)}
+
+
+def _events_ms(fn, stream=None):
+    """CUDA-event time of fn() on the current stream (synchronised on both sides)."""
+    import torch
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b)
+
+
+def form_fp32_flux(reps=5, iters=10, l1_steps=200, shape=(512, 512, 256)):
+    """Precision form, KH 512 x 512 x 256 HLLC MC: FP64 and FP32-flux throughput (median of `reps`
+    timings of `iters` iterations each, after warm-up) and the FP32-flux result's relative L1 error
+    against the FP64 run after `l1_steps` iterations from the same seeded state."""
+    import torch
+    import gpuimogen_b200 as ib
+    from gpuimogen_b200 import problems
+    q0 = torch.from_numpy(problems.kelvin_helmholtz(shape, gamma=GAMMA, seed=12345)).cuda()
+    cells = shape[0] * shape[1] * shape[2]
+    geo = ib.Geometry(shape)
+    out = {"workload": "kelvin_helmholtz_3d_hllc_mc", "grid": list(shape), "iterations_per_timing": iters}
+    finals = {}
+    for prec in ("fp64", "fp32flux"):
+        num = ib.numerics(slope="mc", precision=prec)
+        fl = ib.Fluid(shape, q=q0.clone(), gamma=GAMMA)
+        tm = ib.TimeManager(cfl=CFL)
+        for _ in range(3):
+            ib.run_iteration([fl], geo, tm, METHOD, num)
+        vals = []
+        for _ in range(reps):
+            ms = _events_ms(lambda: [ib.run_iteration([fl], geo, tm, METHOD, num) for _ in range(iters)])
+            vals.append(cells * iters / (ms / 1e3) / 1e6)
+        out[prec] = {"mcell_updates_per_s": _stats(vals)}
+        fl.q.copy_(q0)
+        tm = ib.TimeManager(cfl=CFL)
+        for _ in range(l1_steps):
+            ib.run_iteration([fl], geo, tm, METHOD, num)
+        finals[prec] = fl.q[:, :cells].clone()
+        del fl
+    a, b = finals["fp32flux"], finals["fp64"]
+    rel = ((a - b).abs().sum(dim=1) / b.abs().sum(dim=1)).cpu().numpy()
+    mom = float(((a[2:] - b[2:]).abs().sum() / b[2:].abs().sum()).item())
+    out["rel_l1_vs_fp64_after_%d" % l1_steps] = {"rho": float(rel[0]), "E": float(rel[1]), "momentum": mom}
+    out["speedup_fp32flux"] = (out["fp32flux"]["mcell_updates_per_s"]["median"] /
+                               out["fp64"]["mcell_updates_per_s"]["median"])
+    return out
+
+
+def form_ensemble(reps=5, nprob=4096):
+    """Batching form: 4096 HLLC Riemann problems, N ~ U{256..4096}, each to t = 0.1 in one
+    persistent graph-captured launch (autotuned shape), FP64 and FP32 flux: Mcell-updates/s as the
+    median of `reps` graph replays, and the FP32-flux density error against FP64."""
+    import torch
+    from gpuimogen_b200 import ensemble
+    ens = ensemble.RiemannEnsemble.random(nprob, seed=1)
+    out = {"workload": "riemann_ensemble_hllc", "problems": nprob, "cells": ens.cells, "t_end": 0.1}
+    final = {}
+    for prec in ("fp64", "fp32flux"):
+        tune = ensemble.autotune(ens, t_end=0.1, cfl=CFL, slope="mc", precision=prec)
+        g = ens.capture(t_end=0.1, cfl=CFL, slope="mc", precision=prec, tuning=tune)
+        vals = []
+        for _ in range(reps):
+            ms = _events_ms(g.replay)
+            vals.append(ens.cell_updates() / (ms / 1e3) / 1e6)
+        final[prec] = ens.q[0, :ens.cells].clone()
+        out[prec] = {"mcell_updates_per_s": _stats(vals), "tuning": tune, "cell_updates": ens.cell_updates()}
+        del g
+    a, b = final["fp32flux"], final["fp64"]
+    out["fp32flux_rel_l1_rho_vs_fp64"] = float(((a - b).abs().sum() / b.abs().sum()).item())
+    out["speedup_fp32flux"] = (out["fp32flux"]["mcell_updates_per_s"]["median"] /
+                               out["fp64"]["mcell_updates_per_s"]["median"])
+    return out
+
+
+def form_two_fluid(reps=5, iters=10, l1_steps=500, n=2048):
+    """Learned-drag form, 2-D gas + dust on 2048^2: a drag model trained on 1e7 exact samples (the
+    library's training kernels), then exact LogTrap2 vs learned drag: one drag call (median of
+    `reps`, each on the initial state), one two-fluid iteration (median of `reps` timings of
+    `iters` iterations) and the learned run's relative L1 against the exact run after `l1_steps`."""
+    import torch
+    from gpuimogen_b200 import dusty
+    from gpuimogen_b200 import learned_drag as ld
+    model, hist = ld.train(n_samples=10_000_000, epochs=10, seed=2024)
+    runs = {"exact": dusty.DustyRun(n), "learned": dusty.DustyRun(n, model=model)}
+    cells = n * n
+    out = {"workload": "gas_dust_2d", "grid": [n, n], "training_val_rmse_log_s": hist["val_rmse_log_s"][-1]}
+    for name, r in runs.items():
+        call = []
+        for _ in range(reps + 1):
+            r.reset()
+            call.append(_events_ms(lambda: r.drag([r.gas, r.dust], 4e-5)))
+        r.reset()
+        r.run(2)
+        it = []
+        for _ in range(reps):
+            it.append(_events_ms(lambda: r.run(iters)) / iters)
+        out[name] = {"drag_call_ms": _stats(call[1:]), "iteration_ms": _stats(it),
+                     "mcell_updates_per_s": cells / (float(np.median(it)) / 1e3) / 1e6}
+    for r in runs.values():
+        r.reset()
+        r.run(l1_steps)
+    torch.cuda.synchronize()
+    ex, le = runs["exact"], runs["learned"]
+
+    def rel(a, b):
+        return [float((a[k, :cells] - b[k, :cells]).abs().sum() / max(float(b[k, :cells].abs().sum()), 1e-300))
+                for k in range(5)]
+    out["learned_vs_exact_rel_l1_after_%d" % l1_steps] = {"gas": rel(le.gas.q, ex.gas.q),
+                                                          "dust": rel(le.dust.q, ex.dust.q)}
+    out["learned_fallback_cells"] = int(le.fallbacks.item())
+    out["speedup_drag_call"] = out["exact"]["drag_call_ms"]["median"] / out["learned"]["drag_call_ms"]["median"]
+    out["speedup_iteration"] = out["exact"]["iteration_ms"]["median"] / out["learned"]["iteration_ms"]["median"]
+    return out
+
+
+def reference_gpu_sample(shape, warmup=3, iters=20, reps=3):
+    """The reference's own GPU kernels (its gpuclass sources compiled for sm_100a into oracle/_ref,
+    MC limiter) on the same workload and GPU: Mcell-updates/s, median of `reps` timings of `iters`
+    iterations (the reference's host-side timing of its own loop, which allocates temporaries every
+    call).  None when the reference build is absent."""
+    import ctypes
+    from gpuimogen_b200 import problems
+    path = os.path.join(ROOT, "oracle", "_ref", "libimogen_ref_mc.so")
+    if not os.path.exists(path):
+        return None
+    L = ctypes.CDLL(path)
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.ref_time.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int64, ctypes.c_double,
+                           ctypes.c_int, dp, ctypes.c_double, ctypes.c_int, ctypes.c_int, dp]
+    q = problems.kelvin_helmholtz(shape, gamma=GAMMA, seed=12345)
+    h = np.array([1.0 / s for s in shape])
+    cells = shape[0] * shape[1] * shape[2]
+    vals = []
+    for _ in range(reps):
+        ms = ctypes.c_double(0)
+        qq = q.copy()
+        rc = L.ref_time(qq.ctypes.data_as(dp), shape[0], shape[1], shape[2], q.shape[1], GAMMA, METHOD,
+                        h.ctypes.data_as(dp), CFL, warmup, iters, ctypes.byref(ms))
+        if rc != 0:
+            return {"error": "reference returned %d" % rc}
+        vals.append(cells * iters / (ms.value / 1e3) / 1e6)
+    return {"mcell_updates_per_s": _stats(vals), "iterations": iters,
+            "build": "reference gpuclass sources, MC limiter, nvcc -O2 sm_100a (oracle/ref_harness)"}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return 0
@@ -385,8 +547,7 @@ def run_reference(args, world, rank):
         "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": "kelvin_helmholtz_3d_hllc_fp64", "grid": list(shape), "gamma": GAMMA, "cfl": CFL,
-                   "limiter": "MC", "method": "HLLC", "time_scheme": "SSPRK2", "boundaries": "periodic"},
+        "config": bench_config(shape, world),
         "cpu_baseline": {"value": value, "unit": "Mcell-updates/s", "cores": thr, "kind": "port",
                          "sample": "%d iteration(s) of the %dx%dx%d workload per step, oracle C restatement of the "
                                    "reference kernels (the reference has no CPU implementation of this path)"
@@ -552,22 +713,25 @@ def main():
     e2e_val = job_value(world, cells, e2e_steps, max_over_ranks(e2e_ms, world, dev))
     nbytes = 5 * slab * 8
 
-    # ---------------- CPU baseline (rank 0, N = 1 only) ----------------
+    # ---------------- north-star forms (rank 0, N = 1 only) ----------------
+    forms = None
+    if rank == 0 and world == 1 and os.environ.get("IMOGEN_BENCH_SKIP_FORMS") != "1":
+        forms = {"fp32_flux": form_fp32_flux(), "ensemble": form_ensemble(), "two_fluid": form_two_fluid()}
+
+    # ---------------- baselines (rank 0, N = 1 only) ----------------
     cpu = None
     if rank == 0 and world == 1 and os.environ.get("IMOGEN_BENCH_SKIP_CPU") != "1":
         v, s, thr = cpu_reference_sample(shape, 1)
         cpu = {"value": v, "unit": "Mcell-updates/s", "cores": thr, "kind": "port",
-               "sample": "1 iteration of the %dx%dx%d workload (%.1f s), oracle C restatement, OpenMP" % (*shape, s)}
+               "sample": "1 iteration of the %dx%dx%d workload (%.1f s), oracle C restatement, OpenMP" % (*shape, s),
+               "reference_gpu": reference_gpu_sample(shape)}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "Mcell-updates/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "kelvin_helmholtz_3d_hllc_fp64", "grid": list(shape), "gamma": GAMMA,
-                       "cfl": CFL, "limiter": "MC", "method": "HLLC", "time_scheme": "SSPRK2",
-                       "boundaries": "periodic", "parallelism": "replicas" if world > 1 else "single",
-                       "l2_policy": "state %.0f MB > 126 MB L2, no flush needed" % (nbytes / 1e6)},
+            "config": bench_config(shape, world),
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": "Mcell-updates/s", "h2d_bytes_per_step": nbytes,
@@ -576,6 +740,7 @@ def main():
                               "overlap step i)" % NB},
             "gpu_launches": launches,
             "clocks": clocks,
+            "forms": forms,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

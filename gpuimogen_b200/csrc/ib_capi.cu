@@ -51,6 +51,14 @@ int num_sms()
     return cache[dev];
 }
 
+static std::atomic<long long> g_tile_wait_limit{-1};
+
+uint32_t tile_wait_limit()
+{
+    const long long v = g_tile_wait_limit.load(std::memory_order_relaxed);
+    return v < 0 ? (uint32_t)IB_TMA_SPIN_LIMIT : (uint32_t)v;
+}
+
 static std::mutex g_scratch_mu;
 
 Scratch &scratch()
@@ -361,6 +369,12 @@ const char *ib_status_string(int status)
 int ib_last_cuda_error(void) { return g_last_cuda_error; }
 
 long long ib_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int ib_setTileWaitLimit(long long polls)
+{
+    g_tile_wait_limit.store(polls < 0 ? -1 : std::min<long long>(polls, IB_TMA_SPIN_LIMIT), std::memory_order_relaxed);
+    return IB_SUCCESSFUL;
+}
 
 int ib_device_wait_status(int clear)
 {

@@ -132,16 +132,20 @@ __device__ __forceinline__ float dsqrt<float>(float x) { return sqrtf(x); }
 // ------------------------------------------------------------------------------------------
 // Einfeldt wave-speed bounds (cudaFluidStep.cu:1728-1755, isothermal 1780-1799)
 // ------------------------------------------------------------------------------------------
+// irL, irR: 1/rhoL and 1/rhoR as the product build forms them (the HLLC star flux reuses them)
 template <typename FT>
 __device__ __forceinline__ void einfeldt(const FluidConsts<FT> &c, FT rhoL, FT vL, FT PL, FT rhoR,
-                                         FT vR, FT PR, FT dvsq, FT &sl, FT &sr)
+                                         FT vR, FT PR, FT dvsq, FT &sl, FT &sr, FT &irL, FT &irR)
 {
 #ifdef IB_STRICT_ARITH
     FT csql = c.gamma * PL / rhoL;
     FT csqr = c.gamma * PR / rhoR;
     FT Fa = dsqrt<FT>(rhoR / rhoL);
+    irL = (FT)1.0 / rhoL;  // unused by the strict star flux, which divides as the reference does
+    irR = (FT)1.0 / rhoR;
 #else
-    const FT irL = (FT)1.0 / rhoL, irR = (FT)1.0 / rhoR;
+    irL = (FT)1.0 / rhoL;
+    irR = (FT)1.0 / rhoR;
     FT csql = c.gamma * PL * irL;
     FT csqr = c.gamma * PR * irR;
     FT Fa = dsqrt<FT>(rhoR * irL);
@@ -155,6 +159,14 @@ __device__ __forceinline__ void einfeldt(const FluidConsts<FT> &c, FT rhoL, FT v
     sl = (Croe < sl) ? Croe : sl;
     Croe = 2 * Vroe - Croe;
     sr = (Croe > sr) ? Croe : sr;
+}
+
+template <typename FT>
+__device__ __forceinline__ void einfeldt(const FluidConsts<FT> &c, FT rhoL, FT vL, FT PL, FT rhoR,
+                                         FT vR, FT PR, FT dvsq, FT &sl, FT &sr)
+{
+    FT irL, irR;
+    einfeldt<FT>(c, rhoL, vL, PL, rhoR, vR, PR, dvsq, sl, sr, irL, irR);
 }
 
 template <typename FT>
@@ -223,8 +235,8 @@ __device__ __forceinline__ V5<FT> hllc_flux(const FluidConsts<FT> &c, const V5<F
     D = vyL - vyR;
     E = vzL - vzR;
     C = C * C + D * D + E * E;
-    FT sl, sr;
-    einfeldt<FT>(c, rhoL, vxL, PL, rhoR, vxR, PR, C, sl, sr);
+    FT sl, sr, irL, irR;
+    einfeldt<FT>(c, rhoL, vxL, PL, rhoR, vxR, PR, C, sl, sr, irL, irR);
     C = sl;
     D = sr;
     A = rhoL * (C - vxL);
@@ -256,7 +268,7 @@ __device__ __forceinline__ V5<FT> hllc_flux(const FluidConsts<FT> &c, const V5<F
 #ifdef IB_STRICT_ARITH
             G = D * E * (c.govergm1 * PL / rhoL + G + C);
 #else
-            G = D * E * (c.govergm1 * PL * ((FT)1.0 / rhoL) + G + C);
+            G = D * E * (c.govergm1 * PL * irL + G + C);
 #endif
             f.a[0] = A; f.a[1] = G; f.a[2] = B; f.a[3] = F; f.a[4] = H;
         }
@@ -274,7 +286,7 @@ __device__ __forceinline__ V5<FT> hllc_flux(const FluidConsts<FT> &c, const V5<F
 #ifdef IB_STRICT_ARITH
             G = C * E * (c.govergm1 * PR / rhoR + G + D);
 #else
-            G = C * E * (c.govergm1 * PR * ((FT)1.0 / rhoR) + G + D);
+            G = C * E * (c.govergm1 * PR * irR + G + D);
 #endif
             f.a[0] = A; f.a[1] = G; f.a[2] = B; f.a[3] = F; f.a[4] = H;
         } else {  // right state

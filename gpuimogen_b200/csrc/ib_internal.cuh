@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "ib_common.cuh"
+#include "ib_tma.cuh"
 
 namespace ib {
 
@@ -13,6 +14,8 @@ namespace ib {
 int check_cuda(cudaError_t e);
 int check_launch();
 int num_sms();
+// Poll limit of the TMA-fed kernels' tile waits (IB_TMA_SPIN_LIMIT unless ib_setTileWaitLimit set one).
+uint32_t tile_wait_limit();
 
 // Reusable per-device scratch: grown on demand, never shrunk, freed at process exit.  The
 // reference allocates and frees a 6-slab temporary per call (cudaFluidStep.cu:508-513); the

@@ -257,25 +257,27 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
 #pragma unroll
     for (int sw = 0; sw < NS; sw++) {
     if (NS > 1 && sw > 0) {
-        // the next sweep starts from this one's result; every thread must be done reading the
-        // planes before they are rewritten
+        // the next sweep starts from this one's result (the planes alternate: no barrier)
 #pragma unroll
         for (int m = 0; m < CPT; m++)
 #pragma unroll
             for (int k = 0; k < 5; k++) u0[m][k] = u1[m][k];
-        __syncthreads();
     }
 #pragma unroll
     for (int stage = 0; stage < 2; stage++) {
         double (*u)[5] = (stage == 0) ? u0 : u1;
-        // (a) primitives -> SA
+        // the planes swap roles between the stages, so neither stage rewrites the plane the
+        // other's last phase reads and no barrier separates them
+        FT *PX = (stage == 0) ? SA : SB;  // primitives, then fluxes
+        FT *PY = (stage == 0) ? SB : SA;  // left faces
+        // (a) primitives -> PX
 #pragma unroll
         for (int m = 0; m < CPT; m++) {
             int i = threadIdx.x + m * blockDim.x;
             if (act[m]) {
                 V5<FT> w = stage_prims<METHOD, 1, FT>(u[m], c);
 #pragma unroll
-                for (int k = 0; k < 5; k++) SA[k * n + i] = w.a[k];
+                for (int k = 0; k < 5; k++) PX[k * n + i] = w.a[k];
                 if (row_ssum<CPT, NFIX>() && stage == 1) {  // after the prims: HLL floors u1 in place
 #pragma unroll
                     for (int k = 0; k < 5; k++) SS[k * n + i] = u1[m][k] + u0[m][k];
@@ -283,7 +285,7 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
             }
         }
         __syncthreads();
-        // (b) limited faces; left faces -> SB, right faces kept
+        // (b) limited faces; left faces -> PY, right faces kept
 #pragma unroll
         for (int m = 0; m < CPT; m++) {
             int i = threadIdx.x + m * blockDim.x;
@@ -292,17 +294,17 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
                 V5<FT> w, dl, dr, L;
 #pragma unroll
                 for (int k = 0; k < 5; k++) {
-                    w.a[k] = SA[k * n + i];
-                    dl.a[k] = w.a[k] - SA[k * n + il];
-                    dr.a[k] = SA[k * n + ir] - w.a[k];
+                    w.a[k] = PX[k * n + i];
+                    dl.a[k] = w.a[k] - PX[k * n + il];
+                    dr.a[k] = PX[k * n + ir] - w.a[k];
                 }
                 stage_faces<METHOD, SLOPE, FT>(c, w, dl, dr, L, keep[m]);
 #pragma unroll
-                for (int k = 0; k < 5; k++) SB[k * n + i] = L.a[k];
+                for (int k = 0; k < 5; k++) PY[k * n + i] = L.a[k];
             }
         }
         __syncthreads();
-        // (c) flux through face i+1/2 -> SA
+        // (c) flux through face i+1/2 -> PX
 #pragma unroll
         for (int m = 0; m < CPT; m++) {
             int i = threadIdx.x + m * blockDim.x;
@@ -310,10 +312,10 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
                 int ir = (i == n - 1) ? 0 : i + 1;
                 V5<FT> Lr;
 #pragma unroll
-                for (int k = 0; k < 5; k++) Lr.a[k] = SB[k * n + ir];
+                for (int k = 0; k < 5; k++) Lr.a[k] = PY[k * n + ir];
                 keep[m] = stage_flux<METHOD, FT>(c, keep[m], Lr);
 #pragma unroll
-                for (int k = 0; k < 5; k++) SA[k * n + i] = keep[m].a[k];
+                for (int k = 0; k < 5; k++) PX[k * n + i] = keep[m].a[k];
             }
         }
         __syncthreads();
@@ -325,14 +327,13 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
                 int il = (i == 0) ? n - 1 : i - 1;
 #pragma unroll
                 for (int k = 0; k < 5; k++) {
-                    double df = (double)keep[m].a[k] - (double)SA[k * n + il];
+                    double df = (double)keep[m].a[k] - (double)PX[k * n + il];
                     if (stage == 0) u1[m][k] = u0[m][k] - lambda * df;
                     else if (row_ssum<CPT, NFIX>()) u1[m][k] = .5 * (SS[k * n + i] - lambda * df);
                     else u1[m][k] = .5 * (u1[m][k] + u0[m][k] - lambda * df);
                 }
             }
         }
-        if (stage == 0) __syncthreads();
     }
     }
 #pragma unroll
@@ -363,6 +364,7 @@ struct PipeArgs {
     int64_t nblocks;    // pencil blocks in the grid
     double lambda;
     unsigned int *err;  // set to 1 when a TMA wait ran out
+    uint32_t spin;      // poll limit of the tile waits
 };
 
 __host__ __device__ __forceinline__ size_t pipe_tile_bytes(int n, int W)
@@ -402,8 +404,8 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
     // input tile t (computed, not an indexed array, which would live in local memory)
     auto Ub = [&](int t) { return reinterpret_cast<double *>(smem_raw + t * tb); };
     double *O = reinterpret_cast<double *>(smem_raw + 2 * tb);
-    FT *SA = reinterpret_cast<FT *>(smem_raw + 3 * tb);
-    FT *SB = SA + 5 * NW;
+    FT *PA = reinterpret_cast<FT *>(smem_raw + 3 * tb);
+    FT *PB = PA + 5 * NW;
     const uint32_t tile_tx = (uint32_t)(40 * NW);
     // u1 + u0 through the second stage in the output tile rather than registers: fewer spills for
     // the FP64 one-cell-per-thread blocks (64 registers); the others are faster without it
@@ -454,7 +456,7 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
         const int t = it & 1;
         double *Ut = Ub(t);
         const uint32_t par = t ? phase1 : phase0;
-        const bool ok = mbar_wait_cta(&full[t], par);  // uniform across the CTA
+        const bool ok = mbar_wait_cta(&full[t], par, a.spin);  // uniform across the CTA
         if (t) phase1 ^= 1; else phase0 ^= 1;
         if (!ok) {
             // a tile never arrived: report, drain what is still in flight, leave
@@ -477,22 +479,25 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
         for (int sw = 0; sw < NS; sw++) {
         if (NS > 1 && sw > 0) {
             // the next sweep starts from this one's result in the output tile (each thread reads
-            // the cells it wrote); the planes are rewritten only after every thread is done
+            // the cells it wrote)
 #pragma unroll
             for (int m = 0; m < CPT; m++)
 #pragma unroll
                 for (int k = 0; k < 5; k++) u0[m][k] = act[m] ? O[SI(slots[k], ci[m])] : 1.0;
-            __syncthreads();
         }
 #pragma unroll
         for (int stage = 0; stage < 2; stage++) {
             double (*u)[5] = (stage == 0) ? u0 : u1;
+            // the planes swap roles between the stages: neither stage rewrites the plane that the
+            // other's last phase reads, so no barrier separates them
+            FT *X = (stage == 0) ? PA : PB;  // primitives, then fluxes
+            FT *Y = (stage == 0) ? PB : PA;  // left faces
 #pragma unroll
             for (int m = 0; m < CPT; m++) {
                 if (act[m]) {
                     V5<FT> w = stage_prims<METHOD, DIR, FT>(u[m], c);
 #pragma unroll
-                    for (int k = 0; k < 5; k++) SA[SI(k, ci[m])] = w.a[k];
+                    for (int k = 0; k < 5; k++) X[SI(k, ci[m])] = w.a[k];
                     if (SSUM && stage == 1) {
                         // u1 + u0 of the SSPRK average goes to this block's output tile, so
                         // neither state stays in registers through the second stage (after the
@@ -520,13 +525,13 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
                     V5<FT> w, dl, dr, L;
 #pragma unroll
                     for (int k = 0; k < 5; k++) {
-                        w.a[k] = SA[SI(k, ci[m])];
-                        dl.a[k] = w.a[k] - SA[SI(k, il[m])];
-                        dr.a[k] = SA[SI(k, ir[m])] - w.a[k];
+                        w.a[k] = X[SI(k, ci[m])];
+                        dl.a[k] = w.a[k] - X[SI(k, il[m])];
+                        dr.a[k] = X[SI(k, ir[m])] - w.a[k];
                     }
                     stage_faces<METHOD, SLOPE, FT>(c, w, dl, dr, L, keep[m]);
 #pragma unroll
-                    for (int k = 0; k < 5; k++) SB[SI(k, ci[m])] = L.a[k];
+                    for (int k = 0; k < 5; k++) Y[SI(k, ci[m])] = L.a[k];
                 }
             }
             __syncthreads();
@@ -535,19 +540,21 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
                 if (act[m]) {
                     V5<FT> Lr;
 #pragma unroll
-                    for (int k = 0; k < 5; k++) Lr.a[k] = SB[SI(k, ir[m])];
+                    for (int k = 0; k < 5; k++) Lr.a[k] = Y[SI(k, ir[m])];
                     keep[m] = stage_flux<METHOD, FT>(c, keep[m], Lr);
 #pragma unroll
-                    for (int k = 0; k < 5; k++) SA[SI(k, ci[m])] = keep[m].a[k];
+                    for (int k = 0; k < 5; k++) X[SI(k, ci[m])] = keep[m].a[k];
                 }
             }
+            // the previous block's store must have read O before stage 1 writes it
+            if (stage == 0 && sw == 0 && leader) bulk_wait_read_all();
             __syncthreads();
 #pragma unroll
             for (int m = 0; m < CPT; m++) {
                 if (act[m]) {
 #pragma unroll
                     for (int k = 0; k < 5; k++) {
-                        double df = (double)keep[m].a[k] - (double)SA[SI(k, il[m])];
+                        double df = (double)keep[m].a[k] - (double)X[SI(k, il[m])];
                         if (stage == 0) u1[m][k] = u0[m][k] - lambda * df;
                         else if (SSUM) {
                             double &o = O[SI(slots[k], ci[m])];
@@ -557,11 +564,6 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
                         }
                     }
                 }
-            }
-            if (stage == 0) {
-                // the previous block's store must have read O before stage 1 rewrites it
-                if (leader && sw == 0) bulk_wait_read_all();
-                __syncthreads();
             }
         }
         }
@@ -573,6 +575,132 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
         }
     }
     if (leader) bulk_wait_all();
+}
+
+// ------------------------------------------------------------------------------------------
+// Pencil-pair kernel (y and z sweeps, pencils up to 256 cells, x even): the row kernel's layout
+// applied to a TMA box.  One CTA per block of two adjacent pencils, n threads (one cell each, as
+// the x row kernel), up to four CTAs per SM; thread 0 loads the block's 5-slab box (2 x n x 5
+// doubles, 16-byte rows) with one TMA copy, the CTA sweeps the two pencils one after the other
+// through the row kernel's phases (two shared-memory planes that swap roles between the stages,
+// the SSPRK sum u1 + u0 in a third), writes each pencil's result over its own column of the box
+// and leaves by one TMA store.  No persistent pipeline: the other CTAs on the SM hide a block's
+// load, as they hide the row kernel's.
+// Dynamic shared memory: the box (pipe_tile_bytes(n, 2)), 2 planes of 5 n elements of FT and
+// 5 n doubles for the SSPRK sum.
+// ------------------------------------------------------------------------------------------
+__host__ __device__ __forceinline__ size_t pair_smem_bytes(int n, int ftsize)
+{
+    return pipe_tile_bytes(n, 2) + (size_t)10 * n * ftsize + (size_t)40 * n;
+}
+
+template <int METHOD, int SLOPE, typename FT, int DIR, int NFIX = 0, int NS = 1>
+__global__ void __launch_bounds__(256, 4)
+    sweep_pair_kernel(const __grid_constant__ CUtensorMap tm, PipeArgs a, FluidConsts<FT> c)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full;
+    const int n = NFIX ? NFIX : a.n;
+    double *T = reinterpret_cast<double *>(smem_raw);  // the box: [slab][cell][column]
+    FT *SA = reinterpret_cast<FT *>(smem_raw + pipe_tile_bytes(n, 2));
+    FT *SB = SA + 5 * n;
+    double *SS = reinterpret_cast<double *>(SB + 5 * n);
+    constexpr int s0 = slot_of<METHOD, DIR>(0), s1 = slot_of<METHOD, DIR>(1), s2 = slot_of<METHOD, DIR>(2),
+                  s3 = slot_of<METHOD, DIR>(3), s4 = slot_of<METHOD, DIR>(4);
+    const int slots[5] = {s0, s1, s2, s3, s4};
+    const int64_t b = blockIdx.x;
+    const int i = threadIdx.x;
+    const bool act = i < n;
+    const int il = (i == 0) ? n - 1 : i - 1, ir = (i == n - 1) ? 0 : i + 1;
+    const double lambda = a.lambda;
+    const bool leader = threadIdx.x == 0;
+    if (leader) {
+        mbar_init(&full, 1);
+        fence_mbar_init();
+        mbar_arrive_expect_tx(&full, (uint32_t)(80 * n));
+        pipe_load<DIR>(T, &tm, b, a, 2, &full);
+    }
+    const bool ok = mbar_wait_cta(&full, 0, a.spin);  // uniform across the CTA
+    if (!ok) {
+        if (leader) {
+            atomicOr(a.err, 1u);
+            mbar_wait(&full, 0);  // one more bounded wait for the late box
+        }
+        return;
+    }
+#pragma unroll 1
+    for (int col = 0; col < 2; col++) {
+        auto TI = [&](int k) { return (k * n + i) * 2 + col; };
+        double u0[5], u1[5];
+        V5<FT> keep;
+#pragma unroll
+        for (int k = 0; k < 5; k++) u0[k] = act ? T[TI(slots[k])] : 1.0;
+#pragma unroll
+        for (int sw = 0; sw < NS; sw++) {
+            if (NS > 1 && sw > 0) {
+#pragma unroll
+                for (int k = 0; k < 5; k++) u0[k] = u1[k];
+            }
+#pragma unroll
+            for (int stage = 0; stage < 2; stage++) {
+                double *u = (stage == 0) ? u0 : u1;
+                FT *PX = (stage == 0) ? SA : SB;  // primitives, then fluxes
+                FT *PY = (stage == 0) ? SB : SA;  // left faces
+                if (act) {
+                    V5<FT> w = stage_prims<METHOD, DIR, FT>(u, c);
+#pragma unroll
+                    for (int k = 0; k < 5; k++) PX[k * n + i] = w.a[k];
+                    if (stage == 1) {
+#pragma unroll
+                        for (int k = 0; k < 5; k++) SS[k * n + i] = u1[k] + u0[k];
+                    }
+                }
+                __syncthreads();
+                if (act) {
+                    V5<FT> w, dl, dr, L;
+#pragma unroll
+                    for (int k = 0; k < 5; k++) {
+                        w.a[k] = PX[k * n + i];
+                        dl.a[k] = w.a[k] - PX[k * n + il];
+                        dr.a[k] = PX[k * n + ir] - w.a[k];
+                    }
+                    stage_faces<METHOD, SLOPE, FT>(c, w, dl, dr, L, keep);
+#pragma unroll
+                    for (int k = 0; k < 5; k++) PY[k * n + i] = L.a[k];
+                }
+                __syncthreads();
+                if (act) {
+                    V5<FT> Lr;
+#pragma unroll
+                    for (int k = 0; k < 5; k++) Lr.a[k] = PY[k * n + ir];
+                    keep = stage_flux<METHOD, FT>(c, keep, Lr);
+#pragma unroll
+                    for (int k = 0; k < 5; k++) PX[k * n + i] = keep.a[k];
+                }
+                __syncthreads();
+                if (act) {
+#pragma unroll
+                    for (int k = 0; k < 5; k++) {
+                        double df = (double)keep.a[k] - (double)PX[k * n + il];
+                        if (stage == 0) u1[k] = u0[k] - lambda * df;
+                        else u1[k] = .5 * (SS[k * n + i] - lambda * df);
+                    }
+                }
+            }
+        }
+        // this pencil's result over its own column of the box (its inputs were read above)
+        if (act) {
+#pragma unroll
+            for (int k = 0; k < 5; k++) T[TI(slots[k])] = u1[k];
+        }
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (leader) {
+        pipe_store<DIR>(&tm, T, b, a, 2);
+        bulk_commit();
+        bulk_wait_all();
+    }
 }
 
 // Wide-block variant for z sweeps of large x-y planes.  A block is WL = G*W adjacent columns of
@@ -636,7 +764,7 @@ __global__ void __launch_bounds__(512, 1)
     for (int64_t b = blockIdx.x; b < a.nblocks; b += step, it++) {
         const int t = it & 1;
         double *Ut = Ub(t);
-        const bool ok = mbar_wait_cta(&full[t], (phase >> t) & 1);  // uniform across the CTA
+        const bool ok = mbar_wait_cta(&full[t], (phase >> t) & 1, a.spin);  // uniform across the CTA
         if (!ok) {
             if (leader) {
                 atomicOr(a.err, 1u);
@@ -775,6 +903,7 @@ struct ChunkArgs {
     int64_t ngroups;     // pencil blocks in the grid
     double lambda;
     unsigned int *err;   // set to 1 when a TMA wait ran out
+    uint32_t spin;       // poll limit of the tile waits
 };
 
 __host__ __device__ constexpr size_t chunk_smem_bytes(int W, int R, int ftsize)
@@ -875,7 +1004,7 @@ __global__ void __launch_bounds__(512, 2)
         const int cc = (int)(j % C);
         const int c0 = cc * L;                    // first cell of the chunk
         const int cend = (c0 + L < n) ? c0 + L : n;
-        const bool ok = mbar_wait_cta(&full[buf], (phase >> buf) & 1);
+        const bool ok = mbar_wait_cta(&full[buf], (phase >> buf) & 1, a.spin);
         if (!ok) {
             if (leader) {
                 atomicOr(a.err, 1u);

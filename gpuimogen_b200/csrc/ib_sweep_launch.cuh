@@ -115,8 +115,50 @@ int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const
     if (per_sm < 1) return IB_ERROR_NOIMPLEMENT;
     const int64_t want = (int64_t)per_sm * num_sms();
     const unsigned nblk = (unsigned)std::min<int64_t>(want, nblocks);
-    PipeArgs a{n, npw, bh, nh, nblocks, lambda, err};
+    PipeArgs a{n, npw, bh, nh, nblocks, lambda, err, tile_wait_limit()};
     kern<<<nblk, nt, shm, st>>>(tm, a, c);
+    return check_launch();
+}
+
+// Pencil-pair kernel (sweep_pair_kernel): y/z pencils of at most 256 cells, x even; one CTA per
+// block of two adjacent pencils.  Returns IB_ERROR_NOIMPLEMENT (caller falls back) otherwise.
+template <int METHOD, int SLOPE, typename FT, int DIR, int NFIX = 0>
+int launch_pair(double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c, cudaStream_t st,
+                int nsweep)
+{
+    static_assert(DIR != 1, "x rows take the row kernel");
+    const int nx = grid[0], ny = grid[1], nz = grid[2];
+    const int n = grid[DIR - 1];
+    if (n > 256 || (nx & 1)) return IB_ERROR_NOIMPLEMENT;
+    if (NFIX && n != NFIX) return IB_ERROR_NOIMPLEMENT;
+    if (((uintptr_t)q & 15) || (slab * 8) % 16) return IB_ERROR_NOIMPLEMENT;
+    const uint64_t other = (DIR == 2) ? nz : ny;
+    const uint64_t rs = (DIR == 2) ? (uint64_t)nx * 8 : (uint64_t)nx * ny * 8;   // along the pencil
+    const uint64_t os = (DIR == 2) ? (uint64_t)nx * ny * 8 : (uint64_t)nx * 8;   // across pencils
+    uint64_t dims[5] = {(uint64_t)nx, (uint64_t)n, 1, other, 5};
+    uint64_t strides[4] = {rs, rs * n, os, (uint64_t)slab * 8};
+    uint32_t box[5] = {2, (uint32_t)n, 1, 1, 5};
+    const int npw = nx / 2;
+    const int64_t nblocks = (int64_t)npw * other;
+    if (nblocks >= (int64_t)1 << 31) return IB_ERROR_NOIMPLEMENT;
+    CUtensorMap tm;
+    int rc = encode_tmap_f64(&tm, q, 5, dims, strides, box);
+    if (rc) return rc;
+    unsigned int *err = scratch().wait_flag();
+    if (!err) return IB_ERROR_NOMEM;
+    const int nt = (n + 31) / 32 * 32;
+    const size_t shm = pair_smem_bytes(n, (int)sizeof(FT));
+    const int ns = (nsweep == 2) ? 2 : 1;
+    auto kern = ns == 2 ? &sweep_pair_kernel<METHOD, SLOPE, FT, DIR, NFIX, 2>
+                        : &sweep_pair_kernel<METHOD, SLOPE, FT, DIR, NFIX, 1>;
+    static int attr_bytes[2] = {0, 0};
+    if ((int)shm > attr_bytes[ns - 1]) {
+        rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        if (rc) return rc;
+        attr_bytes[ns - 1] = (int)shm;
+    }
+    PipeArgs a{n, npw, n, 1, nblocks, lambda, err, tile_wait_limit()};
+    kern<<<(unsigned)nblocks, nt, shm, st>>>(tm, a, c);
     return check_launch();
 }
 
@@ -167,6 +209,7 @@ int launch_chunk(double *q, int64_t slab, const int grid[3], double lambda, cons
     if (rc) return rc;
     a.err = scratch().wait_flag();
     if (!a.err) return IB_ERROR_NOMEM;
+    a.spin = tile_wait_limit();
     // halo rows of every chunk boundary, copied before the sweep overwrites them
     const int64_t nside = a.ngroups * a.C * 40 * W;
     double *side = scratch().bytes((size_t)nside * sizeof(double));
@@ -240,7 +283,14 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
         if (dir == 1) {
             if (n <= 256) rc = launch_pipe<METHOD, SLOPE, FT, 1, 1, 1>(q, slab, grid, lambda, c, st, nsweep);
         } else if (n == 256 && !wide) {
-            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1, 256>(q, slab, grid, lambda, c, st, nsweep);
+            static const bool pair = [] {
+                const char *e = getenv("IMOGEN_B200_YZPAIR");
+                return e && e[0] == '1';
+            }();
+            if (pair) {
+                if (dir == 2) rc = launch_pair<METHOD, SLOPE, FT, 2, 256>(q, slab, grid, lambda, c, st, nsweep);
+                else rc = launch_pair<METHOD, SLOPE, FT, 3, 256>(q, slab, grid, lambda, c, st, nsweep);
+            } else if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1, 256>(q, slab, grid, lambda, c, st, nsweep);
             else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1, 256>(q, slab, grid, lambda, c, st, nsweep);
         } else if (n == 128 && !wide) {
             if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1, 128>(q, slab, grid, lambda, c, st, nsweep);

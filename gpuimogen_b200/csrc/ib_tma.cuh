@@ -5,8 +5,9 @@
 //   * loads and stores are tiled, non-multicast, to and from this CTA's own shared memory;
 //   * the innermost (x) box coordinate times 8 bytes is a multiple of 16 bytes (x even);
 //   * stores start at non-negative in-range coordinates;
-//   * every mbarrier wait is bounded (IB_TMA_SPIN_LIMIT polls); a wait that runs out sets the
-//     caller's error word and the kernel drains what it issued before returning.
+//   * every mbarrier wait is bounded (IB_TMA_SPIN_LIMIT polls; the tile waits take the limit from
+//     their launch, which ib_setTileWaitLimit can lower); a wait that runs out sets the caller's
+//     error word and the kernel drains what it issued, with the full limit, before returning.
 #pragma once
 
 #include <cstdint>
@@ -49,10 +50,10 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
 }
 
 // Polls the mbarrier phase with the given parity; false when the poll limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit = IB_TMA_SPIN_LIMIT)
 {
     const uint32_t a = smem_u32(bar);
-    for (uint32_t i = 0; i < IB_TMA_SPIN_LIMIT; i++) {
+    for (uint32_t i = 0; i < limit; i++) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -66,13 +67,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
     return false;
 }
 
-// CTA-wide wait with one poller: thread 0 polls (bounded), the CTA meets at a barrier that also
-// agrees on the outcome, and every thread then takes its own acquire of the completed phase (a
-// test that succeeds at once), so the other threads sleep in the barrier instead of polling.
-__device__ __forceinline__ bool mbar_wait_cta(uint64_t *bar, uint32_t parity)
+// CTA-wide wait with one poller: thread 0 polls (at most `limit` times), the CTA meets at a
+// barrier that also agrees on the outcome, and every thread then takes its own acquire of the
+// completed phase (a test that succeeds at once), so the other threads sleep in the barrier
+// instead of polling.
+__device__ __forceinline__ bool mbar_wait_cta(uint64_t *bar, uint32_t parity, uint32_t limit = IB_TMA_SPIN_LIMIT)
 {
     bool ok = true;
-    if (threadIdx.x == 0) ok = mbar_wait(bar, parity);
+    if (threadIdx.x == 0) ok = mbar_wait(bar, parity, limit);
     ok = __syncthreads_and(ok);
     if (ok) ok = mbar_wait(bar, parity);
     return ok;

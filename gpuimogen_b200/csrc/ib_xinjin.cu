@@ -44,7 +44,10 @@ __device__ __forceinline__ double freeze_cell(const double (&X)[5], double invrh
 
 // The left- and right-going limited fluxes of one component, flux_limit<FLIM>(A1, B1) and
 // flux_limit<FLIM>(A2, B2).  Product build, Ospre and van Leer: their two divisions share one
-// (1/(d1 d2) times d2 and d1) when d1 d2 is a normal number; the strict build divides twice.
+// (1/(d1 d2) times d2 and d1) when d1, d2 and d1 d2 are all normal numbers, so that neither
+// reciprocal can overflow; otherwise (subnormal denominators of momenta near 1e-154, where a
+// reciprocal of infinity times an underflowed zero numerator would give NaN) each divides on
+// its own, as the strict build always does.
 template <int FLIM>
 __device__ __forceinline__ void flux_limit_pair(double A1, double B1, double A2, double B2, double &o1, double &o2)
 {
@@ -72,17 +75,15 @@ __device__ __forceinline__ void flux_limit_pair(double A1, double B1, double A2,
         d1 = p1 ? d1 : 1.0;
         d2 = p2 ? d2 : 1.0;
         const double pd = d1 * d2;
-        double i1, i2;
-        if (fabs(pd) >= 2.2250738585072014e-308 && fabs(pd) <= 1.7976931348623157e308) {
+        constexpr double kMinNormal = 2.2250738585072014e-308, kMax = 1.7976931348623157e308;
+        if (fabs(d1) >= kMinNormal && fabs(d2) >= kMinNormal && fabs(pd) >= kMinNormal && fabs(pd) <= kMax) {
             const double rr = 1.0 / pd;
-            i1 = d2 * rr;
-            i2 = d1 * rr;
+            o1 = p1 ? n1 * (d2 * rr) : 0.0;
+            o2 = p2 ? n2 * (d1 * rr) : 0.0;
         } else {
-            i1 = 1.0 / d1;
-            i2 = 1.0 / d2;
+            o1 = p1 ? n1 / d1 : 0.0;
+            o2 = p2 ? n2 / d2 : 0.0;
         }
-        o1 = p1 ? n1 * i1 : 0.0;
-        o2 = p2 ? n2 * i2 : 0.0;
         return;
     }
 #endif

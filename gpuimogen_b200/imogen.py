@@ -134,6 +134,7 @@ EXPORTS = {
                                            ctypes.POINTER(ctypes.c_double), ctypes.c_void_p,
                                            ctypes.c_void_p]),
     "ib_device_wait_status": (ctypes.c_int, [ctypes.c_int]),
+    "ib_setTileWaitLimit": (ctypes.c_int, [ctypes.c_longlong]),
     "ib_mlpWorkspaceFloats": (ctypes.c_int64, [ctypes.c_int64]),
     "ib_mlpLossGrad": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),

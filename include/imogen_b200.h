@@ -211,6 +211,14 @@ IB_API long long ib_launch_count(void);
  * status code.  clear != 0 resets the flag. */
 IB_API int ib_device_wait_status(int clear);
 
+/* For failure-detection tests (no reference counterpart): how many times the TMA-fed sweep
+ * kernels poll for each tile before their wait gives up, for launches after this call from any
+ * thread; polls < 0 restores the default (2^26 polls, seconds).  A wait that gives up makes the
+ * kernel wait (with the default limit) for the copies it has in flight, leave without finishing
+ * its sweep and set the flag ib_device_wait_status reads; with polls = 0 every tile wait gives up
+ * at once, so a test can exercise that path without any fault. */
+IB_API int ib_setTileWaitLimit(long long polls);
+
 /* Replaces the cudaFluidStep mex (gpuclass/cudaFluidStep.cu:161-227): one SSPRK2 directional
  * sweep of one fluid, in place, without boundary fill.
  * params = [dt, purehydro, gamma, rho_min, method (1 HLL | 2 HLLC | 3 XJ), direction (1..3)

@@ -7,6 +7,9 @@ one vector at the IB_MLP_OFF_* offsets) restated in numpy:
   * forward_bf16(params, x)      the tensor-core arithmetic: weights and every layer input rounded
                                  to BF16 (round to nearest even), products summed exactly (FP64),
                                  bias and ReLU in FP32 after the sum
+  * forward_tc_emulation(p, x)   the tensor-core kernel's own order of roundings (bias split into
+                                 BF16 parts inside the first MMA, FP32 accumulation per K = 16 MMA,
+                                 FP32 output sums)
 and a restatement of the drag law's LogTrap2 decay exponent (cudaSource2FluidDrag.cu:819-890,
 1531-1660) for spot checks of the exact training targets.
 """
@@ -70,6 +73,42 @@ def forward_bf16(p, x):
         h = np.maximum(z, np.float32(0))
         a = h.astype(np.float64) if last else to_bf16(h)
     return a @ w4 + b4
+
+
+def _f32(a):
+    return np.asarray(a, dtype=np.float64).astype(np.float32).astype(np.float64)
+
+
+def forward_tc_emulation(p, x):
+    """The tensor-core kernel's arithmetic step by step (ib_drag_learned.cu, mlp_tc_kernel):
+    layer 1 is one K = 16 MMA whose inputs 14 and 15 are 1 and whose weight columns there hold the
+    bias as BF16 high part and BF16 remainder; layers 2 and 3 are four K = 16 MMAs accumulated in
+    FP32 (each chunk's products summed exactly, then added to the FP32 accumulator); hidden biases
+    are added in FP32 before ReLU and the BF16 conversion; the output is b4 + the FP32 fused
+    multiply-add sums of the even and of the odd hidden units."""
+    W1, b1, W2, b2, W3, b3, w4, b4 = unpack(np.asarray(p, dtype=np.float32))
+    n = len(x)
+    a = to_bf16(np.asarray(x, dtype=np.float32))
+    a[:, 14:16] = 1.0
+    Wb = to_bf16(W1)
+    hi = to_bf16(b1.astype(np.float32))
+    lo = to_bf16((b1.astype(np.float32) - hi.astype(np.float32)).astype(np.float32))
+    Wb[:, 14], Wb[:, 15] = hi, lo
+    z = _f32(a @ Wb.T)
+    a = to_bf16(np.maximum(z, 0).astype(np.float32))
+    for W, b in ((W2, b2), (W3, b3)):
+        Wq = to_bf16(W)
+        acc = np.zeros((n, H))
+        for c in range(0, H, 16):
+            acc = _f32(acc + _f32(a[:, c:c + 16] @ Wq[:, c:c + 16].T))
+        z = np.maximum(_f32(acc + _f32(b)), 0)
+        a = to_bf16(z.astype(np.float32)) if W is W2 else z
+    w4 = _f32(w4)
+    ye, yo = np.zeros(n), np.zeros(n)
+    for j in range(0, H, 2):
+        ye = _f32(w4[j] * a[:, j] + ye)
+        yo = _f32(w4[j + 1] * a[:, j + 1] + yo)
+    return _f32(_f32(b4) + _f32(ye + yo))
 
 
 def drag_constants(tg, td):

@@ -123,3 +123,36 @@ def test_hll_isothermal_and_floors_strict(cuda, ib, po):
             finally:
                 ib.use_variant("product")
             assert bits_equal(out, ref, n), (direction, len(params), first_diff(out, ref, n))
+
+
+@pytest.mark.parametrize("direction", [1, 2])
+def test_xinjin_tiny_momenta_stay_finite(cuda, ib, po, direction):
+    """Momenta near 1e-154 next to exact zeros (as the outflow boundary's transverse momentum
+    leaves them while it decays into the grid) make the Xin-Jin flux limiter's denominators
+    subnormal: the product build's shared reciprocal must not turn 0 / d into 0 * inf."""
+    n = 64
+    shape = (n, 1, 1) if direction == 1 else (4, n, 1)
+    N = shape[0] * shape[1]
+    q = problems.sod(N)
+    q[:, :N] = 0
+    q[0, :N] = 1.0
+    q[1, :N] = 2.5
+    tiny = np.zeros(n)
+    tiny[10:20] = 1e-150 * 10.0 ** (-2.0 * np.arange(10))   # 1e-150 ... 1e-168, then zeros
+    slab = 3 if direction == 1 else 2                       # a transverse momentum
+    q[slab, :N] = np.tile(tiny, N // n) if direction == 1 else np.repeat(tiny, shape[0])
+    geo = ib.Geometry(shape)
+    sp = po.step_params(1e-4, geo.h, 1.4, method=3)
+    ref = q.copy()
+    po.fluid_sweep(ref, shape, sp, direction)
+    assert np.all(np.isfinite(ref[:, :N]))
+    for variant in ("product", "strict"):
+        fl = to_fluid(q.copy(), shape, gamma=1.4)
+        ib.use_variant(variant)
+        try:
+            ib.cudaFluidStep(fl, geo, [1e-4, 1, 1.4, 1e-5, 3, direction])
+        finally:
+            ib.use_variant("product")
+        out = host(fl)
+        assert np.all(np.isfinite(out[:, :N])), variant
+        assert np.allclose(out[:, :N], ref[:, :N], rtol=1e-12, atol=1e-300), variant
