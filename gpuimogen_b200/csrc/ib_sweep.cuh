@@ -578,9 +578,10 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
 }
 
 // ------------------------------------------------------------------------------------------
-// Pencil-pair kernel (y and z sweeps, pencils up to 256 cells, x even): the row kernel's layout
-// applied to a TMA box.  One CTA per block of two adjacent pencils, n threads (one cell each, as
-// the x row kernel), up to four CTAs per SM; thread 0 loads the block's 5-slab box (2 x n x 5
+// Pencil-pair kernel (y and z sweeps, pencils up to 256 cells or of 512, x even): the row kernel's
+// layout applied to a TMA box.  One CTA per block of two adjacent pencils, n threads (one cell
+// each, as the x row kernel), four CTAs per SM (two of 512 threads for 512-cell pencils); thread
+// 0 loads the block's 5-slab box (2 x n x 5
 // doubles, 16-byte rows) with one TMA copy, the CTA sweeps the two pencils one after the other
 // through the row kernel's phases (two shared-memory planes that swap roles between the stages,
 // the SSPRK sum u1 + u0 in a third), writes each pencil's result over its own column of the box
@@ -595,7 +596,7 @@ __host__ __device__ __forceinline__ size_t pair_smem_bytes(int n, int ftsize)
 }
 
 template <int METHOD, int SLOPE, typename FT, int DIR, int NFIX = 0, int NS = 1>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
     sweep_pair_kernel(const __grid_constant__ CUtensorMap tm, PipeArgs a, FluidConsts<FT> c)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];

@@ -120,8 +120,9 @@ int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const
     return check_launch();
 }
 
-// Pencil-pair kernel (sweep_pair_kernel): y/z pencils of at most 256 cells, x even; one CTA per
-// block of two adjacent pencils.  Returns IB_ERROR_NOIMPLEMENT (caller falls back) otherwise.
+// Pencil-pair kernel (sweep_pair_kernel): y/z pencils of at most 256 cells or of 512 (the box
+// arrives as two rows of 256), x even; one CTA per block of two adjacent pencils.  Returns
+// IB_ERROR_NOIMPLEMENT (caller falls back) otherwise.
 template <int METHOD, int SLOPE, typename FT, int DIR, int NFIX = 0>
 int launch_pair(double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c, cudaStream_t st,
                 int nsweep)
@@ -129,15 +130,17 @@ int launch_pair(double *q, int64_t slab, const int grid[3], double lambda, const
     static_assert(DIR != 1, "x rows take the row kernel");
     const int nx = grid[0], ny = grid[1], nz = grid[2];
     const int n = grid[DIR - 1];
-    if (n > 256 || (nx & 1)) return IB_ERROR_NOIMPLEMENT;
+    if ((n > 256 && !(NFIX == 512 && n == 512)) || (nx & 1)) return IB_ERROR_NOIMPLEMENT;
     if (NFIX && n != NFIX) return IB_ERROR_NOIMPLEMENT;
     if (((uintptr_t)q & 15) || (slab * 8) % 16) return IB_ERROR_NOIMPLEMENT;
     const uint64_t other = (DIR == 2) ? nz : ny;
     const uint64_t rs = (DIR == 2) ? (uint64_t)nx * 8 : (uint64_t)nx * ny * 8;   // along the pencil
     const uint64_t os = (DIR == 2) ? (uint64_t)nx * ny * 8 : (uint64_t)nx * 8;   // across pencils
-    uint64_t dims[5] = {(uint64_t)nx, (uint64_t)n, 1, other, 5};
-    uint64_t strides[4] = {rs, rs * n, os, (uint64_t)slab * 8};
-    uint32_t box[5] = {2, (uint32_t)n, 1, 1, 5};
+    // TMA boxes are at most 256 rows: a 512-cell pencil comes as two rows of 256 (half, row)
+    const int bh = (n > 256) ? n / 2 : n, nh = (n > 256) ? 2 : 1;
+    uint64_t dims[5] = {(uint64_t)nx, (uint64_t)bh, (uint64_t)nh, other, 5};
+    uint64_t strides[4] = {rs, rs * bh, os, (uint64_t)slab * 8};
+    uint32_t box[5] = {2, (uint32_t)bh, (uint32_t)nh, 1, 5};
     const int npw = nx / 2;
     const int64_t nblocks = (int64_t)npw * other;
     if (nblocks >= (int64_t)1 << 31) return IB_ERROR_NOIMPLEMENT;
@@ -157,7 +160,7 @@ int launch_pair(double *q, int64_t slab, const int grid[3], double lambda, const
         if (rc) return rc;
         attr_bytes[ns - 1] = (int)shm;
     }
-    PipeArgs a{n, npw, n, 1, nblocks, lambda, err, tile_wait_limit()};
+    PipeArgs a{n, npw, bh, nh, nblocks, lambda, err, tile_wait_limit()};
     kern<<<(unsigned)nblocks, nt, shm, st>>>(tm, a, c);
     return check_launch();
 }
@@ -276,6 +279,11 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
         // z pencils of large x-y planes: blocks 4 columns wide (32-byte rows), which the memory
         // system serves far better than 16-byte rows at megabyte strides
         const bool wide = (dir == 3) && ((int64_t)nx * ny * 8 > (1 << 20));
+        // y/z pencils of up to 256 cells and of 512 take the pencil-pair kernel (one 2-pencil box
+        // per 256-thread CTA, four CTAs per SM: 256^3 FP64 y 0.93 -> 0.76 ms, FP32 flux
+        // 0.52 -> 0.44 ms; 512-cell y pencils 4.01 -> 3.60 ms at 512 x 512 x 256) rather than the
+        // persistent pipeline, which remains for other lengths when the pair kernel declines
+        constexpr bool pair = true, pair512 = true;
         static const int wide8 = [] {
             const char *e = getenv("IMOGEN_B200_WIDE8");  // 0 = 4-column blocks for wide z planes
             return (e && e[0] == '0') ? 0 : 1;
@@ -283,21 +291,26 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
         if (dir == 1) {
             if (n <= 256) rc = launch_pipe<METHOD, SLOPE, FT, 1, 1, 1>(q, slab, grid, lambda, c, st, nsweep);
         } else if (n == 256 && !wide) {
-            static const bool pair = [] {
-                const char *e = getenv("IMOGEN_B200_YZPAIR");
-                return e && e[0] == '1';
-            }();
             if (pair) {
                 if (dir == 2) rc = launch_pair<METHOD, SLOPE, FT, 2, 256>(q, slab, grid, lambda, c, st, nsweep);
                 else rc = launch_pair<METHOD, SLOPE, FT, 3, 256>(q, slab, grid, lambda, c, st, nsweep);
             } else if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1, 256>(q, slab, grid, lambda, c, st, nsweep);
             else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1, 256>(q, slab, grid, lambda, c, st, nsweep);
         } else if (n == 128 && !wide) {
-            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1, 128>(q, slab, grid, lambda, c, st, nsweep);
+            if (pair) {
+                if (dir == 2) rc = launch_pair<METHOD, SLOPE, FT, 2, 128>(q, slab, grid, lambda, c, st, nsweep);
+                else rc = launch_pair<METHOD, SLOPE, FT, 3, 128>(q, slab, grid, lambda, c, st, nsweep);
+            } else if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1, 128>(q, slab, grid, lambda, c, st, nsweep);
             else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1, 128>(q, slab, grid, lambda, c, st, nsweep);
         } else if (n <= 256 && !wide) {
-            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1>(q, slab, grid, lambda, c, st, nsweep);
-            else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1>(q, slab, grid, lambda, c, st, nsweep);
+            if (pair) {
+                if (dir == 2) rc = launch_pair<METHOD, SLOPE, FT, 2>(q, slab, grid, lambda, c, st, nsweep);
+                else rc = launch_pair<METHOD, SLOPE, FT, 3>(q, slab, grid, lambda, c, st, nsweep);
+            }
+            if (rc == IB_ERROR_NOIMPLEMENT) {
+                if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 1>(q, slab, grid, lambda, c, st, nsweep);
+                else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1>(q, slab, grid, lambda, c, st, nsweep);
+            }
         } else if (n == 256) {
             // FP32 flux: 8-column blocks (64-byte rows) computed 4 columns at a time (3.48 -> 2.52
             // ms at 512 x 512 x 256).  FP64 is bound by its arithmetic there and keeps 4 columns:
@@ -312,8 +325,14 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
             }
             if (rc == IB_ERROR_NOIMPLEMENT) rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2>(q, slab, grid, lambda, c, st, nsweep);
         } else if (n == 512) {
-            if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 2, 512>(q, slab, grid, lambda, c, st, nsweep);
-            else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 2, 512>(q, slab, grid, lambda, c, st, nsweep);
+            if (pair512) {
+                if (dir == 2) rc = launch_pair<METHOD, SLOPE, FT, 2, 512>(q, slab, grid, lambda, c, st, nsweep);
+                else rc = launch_pair<METHOD, SLOPE, FT, 3, 512>(q, slab, grid, lambda, c, st, nsweep);
+            }
+            if (rc == IB_ERROR_NOIMPLEMENT) {
+                if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 2, 512>(q, slab, grid, lambda, c, st, nsweep);
+                else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 2, 512>(q, slab, grid, lambda, c, st, nsweep);
+            }
         } else {
             if (dir == 2) rc = launch_pipe<METHOD, SLOPE, FT, 2, 2, 2>(q, slab, grid, lambda, c, st, nsweep);
             else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 2>(q, slab, grid, lambda, c, st, nsweep);
