@@ -229,7 +229,58 @@ def case_all(args):
     print("case all done")
 
 
-CASES = {"sweeps": case_sweeps, "time-sweeps": case_time_sweeps, "cfl": case_cfl, "drag": case_drag,
+def graph_loop_timing(n_sod=1024, n_dust=2048, dust_iters=40):
+    """Per-iteration time of the host loop (run_iteration: the CFL time read to the host every
+    iteration) and of the device-time loop replayed from CUDA graphs (GraphLoop), CUDA events:
+    Sod 1024 cells, Xin-Jin, to t = 0.2 (launch- and latency-bound), and 2-D gas + dust with
+    exact LogTrap2 drag on n_dust^2 for dust_iters iterations after the graphs' six warm-up
+    iterations."""
+    import torch
+    import gpuimogen_b200 as ib
+    from gpuimogen_b200 import dusty, problems
+    out = {}
+    shape = (n_sod, 1, 1)
+    geo = ib.Geometry(shape)
+    for name in ("host_loop", "graph_loop"):
+        fl = ib.Fluid(shape, bc="const", q=torch.from_numpy(problems.sod(n_sod)).cuda(), gamma=1.4)
+        if name == "host_loop":
+            tm = ib.TimeManager(cfl=CFL, tmax=0.2)
+
+            def go():
+                while tm.running:
+                    ib.run_iteration([fl], geo, tm, 3)
+            ms = _events_ms(go)
+            iters = tm.iteration
+        else:
+            loop = ib.GraphLoop([fl], geo, 3, cfl=CFL, tmax=0.2)   # 6 eager iterations, then capture
+            it0 = loop.iteration
+            ms = _events_ms(lambda: loop.run(check_every=64))
+            iters = loop.iteration - it0
+        out.setdefault("sod_1024_xj", {})[name] = {"us_per_iteration": 1e3 * ms / iters, "iterations": iters}
+    drag = (dusty.ld.THERMO_GAS, dusty.ld.THERMO_DUST, "logtrap2")
+    num = ib.numerics(slope="mc")
+    for name in ("host_loop", "graph_loop"):
+        run = dusty.DustyRun(n_dust)
+        fl = [run.gas, run.dust]
+        if name == "host_loop":
+            tm = ib.TimeManager(cfl=CFL)
+            for _ in range(6):
+                ib.run_iteration(fl, run.geo, tm, 2, num, drag=drag)
+            ms = _events_ms(lambda: [ib.run_iteration(fl, run.geo, tm, 2, num, drag=drag) for _ in range(dust_iters)])
+        else:
+            loop = ib.GraphLoop(fl, run.geo, 2, num, drag=drag, cfl=CFL)
+            ms = _events_ms(lambda: loop.run(dust_iters, check_every=dust_iters + 1))
+        out.setdefault("gas_dust_%d_exact_drag" % n_dust, {})[name] = {"ms_per_iteration": ms / dust_iters}
+        del run
+    return out
+
+
+def case_graph(args):
+    """Host loop against the device-time CUDA-graph loop (graph_loop_timing)."""
+    print(json.dumps({"case": "graph", **graph_loop_timing()}))
+
+
+CASES = {"graph": case_graph, "sweeps": case_sweeps, "time-sweeps": case_time_sweeps, "cfl": case_cfl, "drag": case_drag,
          "all": case_all}
 
 

@@ -10,11 +10,11 @@ from .imogen import (BC, DRAG, FLUXLIM, METHOD, PRECISION, SLOPE, Fluid, Geometr
                      cudaStatics, completeTimestep, device_wait_status, fluidstep, freezeAndPtot, load, numerics,
                      setFluidBoundary,
                      slab_pitch, use_variant)
-from .timestep import TimeManager, cfl_tau, run_iteration  # noqa: F401
+from .timestep import GraphLoop, TimeManager, cfl_tau, run_iteration  # noqa: F401
 
 __all__ = [
     "Fluid", "Geometry", "ImogenError", "TimeManager", "cudaFluidStep", "fluidstep", "cflTimestep",
     "cflTimestepFused", "cudaSoundspeed", "freezeAndPtot", "cudaStatics", "setFluidBoundary",
     "cudaSource2FluidDrag", "numerics", "load", "use_variant", "run_iteration", "cfl_tau", "device_wait_status",
-    "completeTimestep",
+    "completeTimestep", "GraphLoop",
 ]

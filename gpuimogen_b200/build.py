@@ -38,8 +38,12 @@ SOURCES = [
     "ib_boundary.cu",
     "ib_drag.cu",
     "ib_tags.cu",
+    "ib_time.cu",
+    "ib_sweep_cyl.cu",
+    "ib_cylsrc.cu",
 ]
-HEADERS = ["ib_common.cuh", "ib_internal.cuh", "ib_sweep.cuh", "ib_sweep_launch.cuh", "ib_tma.cuh", "ib_bc.cuh", "ib_cfl.cuh", "ib_drag.cuh", "ib_tcgen05.cuh"]
+HEADERS = ["ib_common.cuh", "ib_internal.cuh", "ib_sweep.cuh", "ib_sweep_launch.cuh", "ib_tma.cuh", "ib_bc.cuh",
+           "ib_cfl.cuh", "ib_drag.cuh", "ib_tcgen05.cuh", "ib_cyl.cuh"]
 
 BASE_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",

@@ -149,7 +149,7 @@ double *Scratch::bytes(size_t nbytes)
 }
 
 int launch_sweep(int method, int slope, int precision, int dir, double *q, int64_t slab, const int grid[3],
-                 double lambda, double gamma, double rho_min, double c_iso, cudaStream_t st, int nsweep)
+                 DevScalar lambda, double gamma, double rho_min, double c_iso, cudaStream_t st, int nsweep)
 {
     if (method == IB_METHOD_HLLC) {
         if (precision == IB_PREC_FP32_FLUX)
@@ -185,7 +185,7 @@ static int validate_fluid(const ib_fluid *f)
 }
 
 struct Numerics {
-    int slope = IB_SLOPE_OSPRE, flim = IB_FLUX_OSPRE, prec = IB_PREC_FP64;
+    int slope = IB_SLOPE_OSPRE, flim = IB_FLUX_OSPRE, prec = IB_PREC_FP64, flags = 0;
 };
 
 static int get_numerics(const ib_numerics *num, Numerics &n)
@@ -194,25 +194,90 @@ static int get_numerics(const ib_numerics *num, Numerics &n)
         n.slope = num->slope_limiter;
         n.flim = num->flux_limiter;
         n.prec = num->precision;
+        n.flags = num->flags;
     }
     if (n.slope < IB_SLOPE_OSPRE || n.slope > IB_SLOPE_ZERO) return IB_ERROR_INVALID_ARGS;
     if (n.flim < IB_FLUX_OSPRE || n.flim > IB_FLUX_ZERO) return IB_ERROR_INVALID_ARGS;
     if (n.prec != IB_PREC_FP64 && n.prec != IB_PREC_FP32_FLUX) return IB_ERROR_INVALID_ARGS;
+    if (n.flags & ~IB_FLAG_CYL_GEOMETRIC_RADIUS) return IB_ERROR_INVALID_ARGS;
     return IB_SUCCESSFUL;
 }
+
+static bool geometry_ok(const ib_geometry *geo)
+{
+    return geo->shape == IB_GEOMETRY_SQUARE || geo->shape == IB_GEOMETRY_CYLINDRICAL;
+}
+
+// The cylindrical form of a sweep along dir (cudaFluidStep.cu:264-278): x = r, y = theta (z
+// sweeps are plain).  theta_layout: 0 = the reference's memory layout theta,r,z (FLUX_THETA_213),
+// 1 = theta,z,r (FLUX_THETA_231).  The theta radius rule (ib_cyl.cuh): the cell centre radius
+// with IB_FLAG_CYL_GEOMETRIC_RADIUS, else the reference's arithmetic with the theta cell size as
+// its radial step, whose launch treats the radial axis as the second one when a theta,z,r grid
+// has nz = 1 (block index, and so the radius term, 0) and the z axis as the second one when a
+// theta,r,z grid has nx = 1 < nz (cudaFluidStep.cu:325-329).
+static CylSweep cyl_sweep(const ib_geometry *geo, const ib_grid &g, int dir, int theta_layout, const Numerics &nm)
+{
+    CylSweep cs{CYL_NONE, CylPencil{0.0, 0.0, 0, 0}};
+    if (geo->shape != IB_GEOMETRY_CYLINDRICAL || dir == 3) return cs;
+    if (dir == 1) {
+        cs.kind = CYL_RADIAL;
+        cs.pencil = CylPencil{geo->r_inner, geo->h[0], RMODE_GEOMETRIC, 0};
+        return cs;
+    }
+    cs.kind = theta_layout ? CYL_THETA_LAM : CYL_THETA_DIV;
+    if (nm.flags & IB_FLAG_CYL_GEOMETRIC_RADIUS)
+        cs.pencil = CylPencil{geo->r_inner, geo->h[0], RMODE_GEOMETRIC, 0};
+    else if (theta_layout)
+        cs.pencil = CylPencil{geo->r_inner, geo->h[1], g.nz == 1 ? RMODE_INNER : RMODE_INDEX, 0};
+    else
+        cs.pencil = CylPencil{geo->r_inner, geo->h[1], RMODE_ACC4, (g.nx == 1 && g.nz > 1) ? 1 : 0};
+    return cs;
+}
+
+// Which theta layout the theta sweep of a fluid step has in the reference: the permutations of
+// performFluidUpdate_3D (flux.cu:46-49, cudaArrayRotateB.cu:580-643) leave r third in memory for
+// sweep indices 0 and 5, second for the others.
+static int theta_layout_of(int sweep_dir, int step_number)
+{
+    const int sweep = (step_number + 3 * (sweep_dir > 0)) % 6;
+    return (sweep == 0 || sweep == 5) ? 1 : 0;
+}
+
+// The timestep of a call: a host value, or the address of a device value that the kernels read
+// themselves (loops that keep dt on the device and replay a captured graph).
+struct StepDt {
+    double dt;
+    const double *dtp;
+    // a sweep's lambda = dt / h (the same division in either form)
+    DevScalar lambda(double h) const { return dtp ? DevScalar::device(dtp, 1.0, h) : DevScalar::of(dt / h); }
+    // frac * dt for a source step (frac 1 or 1/2: exact in either form)
+    DevScalar part(double frac) const { return dtp ? DevScalar::device(dtp, frac, 1.0) : DevScalar::of(frac * dt); }
+};
 
 // One directional update (performFluidUpdate_1D); gamma already 2 for isothermal fluids.  With
 // nsweep = 2 the same update is applied twice in a row (HLL/HLLC: one launch where the kernel
 // allows it; Xin-Jin: two launches).
-static int fluid_update_1d(ib_fluid *f, const ib_geometry *geo, int method, int dir, double dt, double gamma,
-                           double rho_min, double c_iso, const Numerics &nm, cudaStream_t st, int nsweep = 1)
+static int fluid_update_1d(ib_fluid *f, const ib_geometry *geo, int method, int dir, const StepDt &dt, double gamma,
+                           double rho_min, double c_iso, const Numerics &nm, cudaStream_t st, int nsweep = 1,
+                           int theta_layout = 0)
 {
     const int grid[3] = {f->grid.nx, f->grid.ny, f->grid.nz};
     if (grid[dir - 1] < 3) return IB_SUCCESSFUL;  // cudaFluidStep.cu:313
-    const double lambda = dt / geo->h[dir - 1];
+    const DevScalar lambda = dt.lambda(geo->h[dir - 1]);
+    const CylSweep cs = cyl_sweep(geo, f->grid, dir, theta_layout, nm);
     if (method == IB_METHOD_XINJIN) {
         for (int k = 0; k < nsweep; k++) {
-            int rc = launch_xj_sweep(nm.flim, dir, f->q, f->grid.slab_pitch, grid, lambda, gamma, rho_min, st);
+            int rc = launch_xj_sweep(nm.flim, dir, f->q, f->grid.slab_pitch, grid, lambda, gamma, rho_min, st,
+                                     cs.kind != CYL_NONE ? &cs : nullptr);
+            if (rc) return rc;
+        }
+        return IB_SUCCESSFUL;
+    }
+    if (cs.kind != CYL_NONE) {
+        if (nm.prec != IB_PREC_FP64) return IB_ERROR_NOIMPLEMENT;  // cylindrical sweeps are FP64
+        for (int k = 0; k < nsweep; k++) {
+            int rc = launch_sweep_cyl(method, nm.slope, f->q, f->grid.slab_pitch, grid, lambda, gamma, rho_min, c_iso,
+                                      st, cs);
             if (rc) return rc;
         }
         return IB_SUCCESSFUL;
@@ -272,19 +337,19 @@ static FluidParams fluid_params(const ib_fluid_thermo &t)
 }
 
 // One sweep of a fluid step and the boundary fill after it (flux.cu:102-110).
-static int sweep_and_fill(ib_fluid *f, const ib_geometry *geo, int method, int d, double dt, const FluidParams &fp,
-                          const Numerics &nm, cudaStream_t st, int nsweep = 1)
+static int sweep_and_fill(ib_fluid *f, const ib_geometry *geo, int method, int d, const StepDt &dt, const FluidParams &fp,
+                          const Numerics &nm, cudaStream_t st, int nsweep = 1, int theta_layout = 0)
 {
     const int ext[3] = {f->grid.nx, f->grid.ny, f->grid.nz};
     if (ext[d - 1] <= 3) return IB_SUCCESSFUL;
-    int rc = fluid_update_1d(f, geo, method, d, dt, fp.gamma, fp.rho_min, fp.c_iso, nm, st, nsweep);
+    int rc = fluid_update_1d(f, geo, method, d, dt, fp.gamma, fp.rho_min, fp.c_iso, nm, st, nsweep, theta_layout);
     if (rc) return rc;
     return fluid_boundary(f, d, st);
 }
 
 // One fluid step (forward or backward) of one fluid, all three sweeps; 1-D grids take the
 // shortcut of flux.cu:35-68 (one x sweep).
-static int fluid_step_one(ib_fluid *f, const ib_geometry *geo, int method, double dt, const FluidParams &fp,
+static int fluid_step_one(ib_fluid *f, const ib_geometry *geo, int method, const StepDt &dt, const FluidParams &fp,
                           const Numerics &nm, int sweep_dir, int step_number, cudaStream_t st)
 {
     const int ext[3] = {f->grid.nx, f->grid.ny, f->grid.nz};
@@ -295,8 +360,9 @@ static int fluid_step_one(ib_fluid *f, const ib_geometry *geo, int method, doubl
     }
     int order[3];
     sweep_order(step_number, sweep_dir, order);
+    const int layout = theta_layout_of(sweep_dir, step_number);
     for (int n = 0; n < 3; n++) {
-        int rc = sweep_and_fill(f, geo, method, order[n], dt, fp, nm, st);
+        int rc = sweep_and_fill(f, geo, method, order[n], dt, fp, nm, st, 1, layout);
         if (rc) return rc;
     }
     return IB_SUCCESSFUL;
@@ -306,7 +372,7 @@ static int fluid_step_one(ib_fluid *f, const ib_geometry *geo, int method, doubl
 // last sweep and the backward step's first are along the same axis d with the same dt; when the
 // boundary fill between them does nothing (both faces of d periodic, no statics) they are one
 // double-sweep launch: the same updates in the same order, so the result is identical.
-static int fluid_fwd_bwd(ib_fluid *f, const ib_geometry *geo, int method, double dt, const FluidParams &fp,
+static int fluid_fwd_bwd(ib_fluid *f, const ib_geometry *geo, int method, const StepDt &dt, const FluidParams &fp,
                          const Numerics &nm, int step_number, cudaStream_t st)
 {
     const int ext[3] = {f->grid.nx, f->grid.ny, f->grid.nz};
@@ -319,8 +385,10 @@ static int fluid_fwd_bwd(ib_fluid *f, const ib_geometry *geo, int method, double
         sweep_order(step_number, -1, bwd);
     }
     const int d = one_d ? 1 : fwd[2];
+    // (cylindrical: the two steps' theta sweeps can differ in form, so they stay apart)
     const bool fuse = (one_d || bwd[0] == d) && ext[d - 1] > 3 && f->bc[2 * (d - 1)] == IB_BC_CIRCULAR &&
-                      f->bc[2 * (d - 1) + 1] == IB_BC_CIRCULAR && !has_statics(f);
+                      f->bc[2 * (d - 1) + 1] == IB_BC_CIRCULAR && !has_statics(f) &&
+                      geo->shape == IB_GEOMETRY_SQUARE;
     if (!fuse) {
         int rc = fluid_step_one(f, geo, method, dt, fp, nm, 1, step_number, st);
         if (rc) return rc;
@@ -335,6 +403,121 @@ static int fluid_fwd_bwd(ib_fluid *f, const ib_geometry *geo, int method, double
         for (int n = 1; n < 3; n++)
             if ((rc = sweep_and_fill(f, geo, method, bwd[n], dt, fp, nm, st))) return rc;
     return IB_SUCCESSFUL;
+}
+
+// Two-fluid drag over dt (sourcefunction_2FluidDrag, cudaSource2FluidDrag.cu:189-246): the drag
+// constants of the two fluids' microphysics, then the integrator's kernel(s).
+static int drag_source(ib_fluid *gas, ib_fluid *dust, const ib_thermo *tg, const ib_thermo *td,
+                       const ib_geometry *geo, DevScalar dt, int method, cudaStream_t st)
+{
+    int rc;
+    if (!gas || !dust || !tg || !td || !gas->q || !dust->q) return IB_ERROR_NULL_POINTER;
+    if ((rc = validate_grid(gas->grid))) return rc;
+    if (gas->grid.nx != dust->grid.nx || gas->grid.ny != dust->grid.ny || gas->grid.nz != dust->grid.nz ||
+        gas->grid.slab_pitch != dust->grid.slab_pitch)
+        return IB_ERROR_INVALID_ARGS;
+    if (method < IB_DRAG_EMP || method > IB_DRAG_LOGTRAP3) return IB_ERROR_INVALID_ARGS;
+    // drag constants (cudaSource2FluidDrag.cu:196-218; dragparams[7] = dt goes to the kernels
+    // separately)
+    double dp[11];
+    const double gam = tg->gamma;
+    const double ddust = sqrt(td->sigma0 / 3.141592653589793);
+    dp[0] = tg->mu0;
+    dp[1] = -tg->mu_t_index;
+    dp[2] = tg->sigma_t_index;
+    dp[3] = tg->mass * (gam - 1.0) / (298.15 * tg->k_bolt);
+    dp[4] = sqrt(2.0) * tg->mass / (tg->sigma0 * ddust);
+    dp[5] = ddust / tg->mu0;
+    dp[6] = td->sigma0 / (1.0 * td->mass);
+    dp[7] = 0.0;
+    dp[8] = (gam - 1.0);
+    dp[9] = .25 * td->sigma0 / td->mass;
+    dp[10] = 16 * (gam - 1.0) / 3.0;
+    const int grid[3] = {gas->grid.nx, gas->grid.ny, gas->grid.nz};
+    if (method == IB_DRAG_ETDRK2) {
+        // the pressure gradient needs the cell sizes (prepareForExpMethod, cudaSource2FluidDrag.cu:1728-1741)
+        if (!geo) return IB_ERROR_NULL_POINTER;
+        if (geo->shape != 0) return IB_ERROR_NOIMPLEMENT;  // cylindrical gradients: out of scope
+    }
+    return launch_drag(gas->q, dust->q, gas->grid.slab_pitch, grid, geo ? geo->h : nullptr, dp, dt, method, st);
+}
+
+// performCompleteTimestep (flux_multi.cu:174-272); params = [purehydro, iteration, method].
+static int complete_timestep(ib_fluid *fluids, const ib_fluid_thermo *thermo, int nfluids, const ib_geometry *geo,
+                             const StepDt &dt, const double *params, const ib_numerics *num,
+                             const ib_drag_source *drag, cudaStream_t st)
+{
+    int rc;
+    if (!fluids || !thermo || !geo) return IB_ERROR_NULL_POINTER;
+    if (nfluids < 1) return IB_ERROR_INVALID_ARGS;
+    Numerics nm;
+    if ((rc = get_numerics(num, nm))) return rc;
+    if (!geometry_ok(geo)) return IB_ERROR_NOIMPLEMENT;
+    const bool cyl = geo->shape == IB_GEOMETRY_CYLINDRICAL;
+    const int purehydro = (int)params[0];
+    const int step_number = (int)params[1];
+    const int method = (int)params[2];
+    if (purehydro != 1) return IB_ERROR_NOIMPLEMENT;
+    if (method < IB_METHOD_HLL || method > IB_METHOD_XINJIN) return IB_ERROR_INVALID_ARGS;
+    if (drag && nfluids != 2) return IB_ERROR_INVALID_ARGS;  // gas and dust
+    for (int fi = 0; fi < nfluids; fi++)
+        if ((rc = validate_fluid(&fluids[fi]))) return rc;
+    if (!drag && !cyl) {
+        // no source between the two fluid steps (srcType 0, flux_multi.cu:161-163): the fluids
+        // are independent, each runs forward then backward
+        for (int fi = 0; fi < nfluids; fi++)
+            if ((rc = fluid_fwd_bwd(&fluids[fi], geo, method, dt, fluid_params(thermo[fi]), nm, step_number, st)))
+                return rc;
+        return IB_SUCCESSFUL;
+    }
+    // Sources (flux_multi.cu:174-272): source dt/2, forward, source dt, backward, source dt/2, the
+    // source being the two-fluid drag (srcType 8, src___D), the cylindrical terms of every fluid
+    // (1, srcC___) or both split as cylinder dt/2, drag, cylinder dt/2 (9, srcC__D;
+    // sourceStep.cu:200-226, 300-329, 498-562).  The cylinder sources end with
+    // setAllBoundaryConditions (sourceStep.cu:276-291), which fills fluid 0's boundaries in
+    // directions 1, 2, 3 once per fluid: its loop indexes fluids[0].  Directions of 3 cells or
+    // fewer are left alone, as inside the fluid step.
+    const int grid[3] = {fluids[0].grid.nx, fluids[0].grid.ny, fluids[0].grid.nz};
+    auto cyl_terms = [&](double frac) -> int {
+        for (int fi = 0; fi < nfluids; fi++) {
+            const int g3[3] = {fluids[fi].grid.nx, fluids[fi].grid.ny, fluids[fi].grid.nz};
+            int r = launch_cyl_source(fluids[fi].q, fluids[fi].grid.slab_pitch, g3, geo->h[0], geo->r_inner,
+                                      dt.part(frac), st);
+            if (r) return r;
+        }
+        return IB_SUCCESSFUL;
+    };
+    auto all_boundaries = [&]() -> int {
+        for (int fi = 0; fi < nfluids; fi++)
+            for (int d = 1; d <= 3; d++) {
+                if (grid[d - 1] <= 3) continue;
+                int r = fluid_boundary(&fluids[0], d, st);
+                if (r) return r;
+            }
+        return IB_SUCCESSFUL;
+    };
+    auto source = [&](double frac) -> int {
+        int r;
+        if (cyl) {
+            if ((r = cyl_terms(drag ? 0.5 * frac : frac))) return r;
+            if (drag && (r = drag_source(&fluids[0], &fluids[1], &drag->thermo_gas, &drag->thermo_dust, geo,
+                                         dt.part(frac), drag->method, st)))
+                return r;
+            if (drag && (r = cyl_terms(0.5 * frac))) return r;
+            return all_boundaries();
+        }
+        return drag_source(&fluids[0], &fluids[1], &drag->thermo_gas, &drag->thermo_dust, geo, dt.part(frac),
+                           drag->method, st);
+    };
+    if ((rc = source(0.5))) return rc;
+    for (int fi = 0; fi < nfluids; fi++)
+        if ((rc = fluid_step_one(&fluids[fi], geo, method, dt, fluid_params(thermo[fi]), nm, 1, step_number, st)))
+            return rc;
+    if ((rc = source(1.0))) return rc;
+    for (int fi = 0; fi < nfluids; fi++)
+        if ((rc = fluid_step_one(&fluids[fi], geo, method, dt, fluid_params(thermo[fi]), nm, -1, step_number, st)))
+            return rc;
+    return source(0.5);
 }
 
 }  // namespace ib
@@ -396,10 +579,10 @@ int ib_cudaFluidStep(ib_fluid *fluid, const ib_geometry *geo, const double *para
     int rc;
     if (!geo || !params) return IB_ERROR_NULL_POINTER;
     if ((rc = validate_fluid(fluid))) return rc;
-    if (nparams != 6 && nparams != 7) return IB_ERROR_INVALID_ARGS;
+    if (nparams < 6 || nparams > 8) return IB_ERROR_INVALID_ARGS;
     Numerics nm;
     if ((rc = get_numerics(num, nm))) return rc;
-    if (geo->shape != 0) return IB_ERROR_NOIMPLEMENT;  // cylindrical sweeps are not built
+    if (!geometry_ok(geo)) return IB_ERROR_NOIMPLEMENT;
     const double dt = params[0];
     const int purehydro = (int)params[1];
     double gamma = params[2];
@@ -407,13 +590,16 @@ int ib_cudaFluidStep(ib_fluid *fluid, const ib_geometry *geo, const double *para
     const int method = (int)params[4];
     const int dir = (int)params[5];
     double c_iso = -1;
-    if (nparams == 7) {
+    if (nparams == 7 || (nparams == 8 && params[6] != -1)) {  // 8 parameters: -1 = adiabatic
         c_iso = params[6];
         gamma = 2;
     }
+    const int theta_layout = (nparams == 8) ? (int)params[7] : 0;
+    if (theta_layout != 0 && theta_layout != 1) return IB_ERROR_INVALID_ARGS;
     if (purehydro != 1) return IB_ERROR_NOIMPLEMENT;  // the MHD sweeps are dead in the reference
     if (method < IB_METHOD_HLL || method > IB_METHOD_XINJIN || dir < 1 || dir > 3) return IB_ERROR_INVALID_ARGS;
-    return fluid_update_1d(fluid, geo, method, dir, dt, gamma, rho_min, c_iso, nm, (cudaStream_t)stream);
+    return fluid_update_1d(fluid, geo, method, dir, StepDt{dt, nullptr}, gamma, rho_min, c_iso, nm,
+                           (cudaStream_t)stream, 1, theta_layout);
 }
 
 int ib_fluidstep(ib_fluid *fluids, const ib_fluid_thermo *thermo, int nfluids, const ib_geometry *geo,
@@ -424,8 +610,8 @@ int ib_fluidstep(ib_fluid *fluids, const ib_fluid_thermo *thermo, int nfluids, c
     if (nparams != 5 || nfluids < 1) return IB_ERROR_INVALID_ARGS;
     Numerics nm;
     if ((rc = get_numerics(num, nm))) return rc;
-    if (geo->shape != 0) return IB_ERROR_NOIMPLEMENT;
-    const double dt = params[0];
+    if (!geometry_ok(geo)) return IB_ERROR_NOIMPLEMENT;
+    const StepDt dt{params[0], nullptr};
     const int purehydro = (int)params[1];
     const int sweep_dir = (int)params[2];
     const int step_number = (int)params[3];
@@ -446,45 +632,20 @@ int ib_completeTimestep(ib_fluid *fluids, const ib_fluid_thermo *thermo, int nfl
                         const double *params, int nparams, const ib_numerics *num, const ib_drag_source *drag,
                         void *stream)
 {
-    int rc;
-    if (!fluids || !thermo || !geo || !params) return IB_ERROR_NULL_POINTER;
-    if (nparams != 4 || nfluids < 1) return IB_ERROR_INVALID_ARGS;
-    Numerics nm;
-    if ((rc = get_numerics(num, nm))) return rc;
-    if (geo->shape != 0) return IB_ERROR_NOIMPLEMENT;
-    const double dt = params[0];
-    const int purehydro = (int)params[1];
-    const int step_number = (int)params[2];
-    const int method = (int)params[3];
-    if (purehydro != 1) return IB_ERROR_NOIMPLEMENT;
-    if (method < IB_METHOD_HLL || method > IB_METHOD_XINJIN) return IB_ERROR_INVALID_ARGS;
-    if (drag && nfluids != 2) return IB_ERROR_INVALID_ARGS;  // gas and dust
-    for (int fi = 0; fi < nfluids; fi++)
-        if ((rc = validate_fluid(&fluids[fi]))) return rc;
-    cudaStream_t st = (cudaStream_t)stream;
-    if (!drag) {
-        // no source between the two fluid steps (srcType 0, flux_multi.cu:161-163): the fluids
-        // are independent, each runs forward then backward
-        for (int fi = 0; fi < nfluids; fi++)
-            if ((rc = fluid_fwd_bwd(&fluids[fi], geo, method, dt, fluid_params(thermo[fi]), nm, step_number, st)))
-                return rc;
-        return IB_SUCCESSFUL;
-    }
-    // two-fluid drag (flux_multi.cu:174-272): drag dt/2, forward, drag dt, backward, drag dt/2
-    auto source = [&](double h) {
-        const double dp[2] = {h, (double)drag->method};
-        return ib_cudaSource2FluidDrag(&fluids[0], &fluids[1], &drag->thermo_gas, &drag->thermo_dust, geo, dp, 2,
-                                       stream);
-    };
-    if ((rc = source(0.5 * dt))) return rc;
-    for (int fi = 0; fi < 2; fi++)
-        if ((rc = fluid_step_one(&fluids[fi], geo, method, dt, fluid_params(thermo[fi]), nm, 1, step_number, st)))
-            return rc;
-    if ((rc = source(dt))) return rc;
-    for (int fi = 0; fi < 2; fi++)
-        if ((rc = fluid_step_one(&fluids[fi], geo, method, dt, fluid_params(thermo[fi]), nm, -1, step_number, st)))
-            return rc;
-    return source(0.5 * dt);
+    if (!params) return IB_ERROR_NULL_POINTER;
+    if (nparams != 4) return IB_ERROR_INVALID_ARGS;
+    return complete_timestep(fluids, thermo, nfluids, geo, StepDt{params[0], nullptr}, params + 1, num, drag,
+                             (cudaStream_t)stream);
+}
+
+int ib_completeTimestepDeviceDt(ib_fluid *fluids, const ib_fluid_thermo *thermo, int nfluids,
+                                const ib_geometry *geo, const double *dt_device, const double *params, int nparams,
+                                const ib_numerics *num, const ib_drag_source *drag, void *stream)
+{
+    if (!params || !dt_device) return IB_ERROR_NULL_POINTER;
+    if (nparams != 3) return IB_ERROR_INVALID_ARGS;
+    return complete_timestep(fluids, thermo, nfluids, geo, StepDt{0.0, dt_device}, params, num, drag,
+                             (cudaStream_t)stream);
 }
 
 int ib_cudaSoundspeed(const ib_fluid *fluid, double gamma, double *cs_out, void *stream)
@@ -504,7 +665,7 @@ static int cfl_common(const ib_fluid *fluid, const double *cs, double gamma, con
     if (!fluid || !geo || !fluid->q) return IB_ERROR_NULL_POINTER;
     if ((rc = validate_grid(fluid->grid))) return rc;
     if (method < IB_METHOD_HLL || method > IB_METHOD_XINJIN) return IB_ERROR_INVALID_ARGS;
-    if (geo->shape != 0) return IB_ERROR_NOIMPLEMENT;
+    if (!geometry_ok(geo)) return IB_ERROR_NOIMPLEMENT;
     if (!tau_host && !tau_device) return IB_ERROR_NULL_POINTER;
     cudaStream_t st = (cudaStream_t)stream;
     double *tau = tau_device ? tau_device : scratch().cfl_tau();
@@ -583,39 +744,9 @@ int ib_setFluidBoundary(ib_fluid *fluid, int direction, void *stream)
 int ib_cudaSource2FluidDrag(ib_fluid *gas, ib_fluid *dust, const ib_thermo *tg, const ib_thermo *td,
                             const ib_geometry *geo, const double *params, int nparams, void *stream)
 {
-    int rc;
-    if (!gas || !dust || !tg || !td || !params || !gas->q || !dust->q) return IB_ERROR_NULL_POINTER;
+    if (!params) return IB_ERROR_NULL_POINTER;
     if (nparams != 2) return IB_ERROR_INVALID_ARGS;  // cudaSource2FluidDrag.cu:157-163
-    if ((rc = validate_grid(gas->grid))) return rc;
-    if (gas->grid.nx != dust->grid.nx || gas->grid.ny != dust->grid.ny || gas->grid.nz != dust->grid.nz ||
-        gas->grid.slab_pitch != dust->grid.slab_pitch)
-        return IB_ERROR_INVALID_ARGS;
-    const double dt = params[0];
-    const int method = (int)params[1];
-    if (method < IB_DRAG_EMP || method > IB_DRAG_LOGTRAP3) return IB_ERROR_INVALID_ARGS;
-    // drag constants (cudaSource2FluidDrag.cu:196-218)
-    double dp[11];
-    const double gam = tg->gamma;
-    const double ddust = sqrt(td->sigma0 / 3.141592653589793);
-    dp[0] = tg->mu0;
-    dp[1] = -tg->mu_t_index;
-    dp[2] = tg->sigma_t_index;
-    dp[3] = tg->mass * (gam - 1.0) / (298.15 * tg->k_bolt);
-    dp[4] = sqrt(2.0) * tg->mass / (tg->sigma0 * ddust);
-    dp[5] = ddust / tg->mu0;
-    dp[6] = td->sigma0 / (1.0 * td->mass);
-    dp[7] = dt;
-    dp[8] = (gam - 1.0);
-    dp[9] = .25 * td->sigma0 / td->mass;
-    dp[10] = 16 * (gam - 1.0) / 3.0;
-    const int grid[3] = {gas->grid.nx, gas->grid.ny, gas->grid.nz};
-    if (method == IB_DRAG_ETDRK2) {
-        // the pressure gradient needs the cell sizes (prepareForExpMethod, cudaSource2FluidDrag.cu:1728-1741)
-        if (!geo) return IB_ERROR_NULL_POINTER;
-        if (geo->shape != 0) return IB_ERROR_NOIMPLEMENT;  // cylindrical gradients: out of scope
-    }
-    return launch_drag(gas->q, dust->q, gas->grid.slab_pitch, grid, geo ? geo->h : nullptr, dp, dt, method,
-                       (cudaStream_t)stream);
+    return drag_source(gas, dust, tg, td, geo, DevScalar::of(params[0]), (int)params[1], (cudaStream_t)stream);
 }
 
 }  // extern "C"

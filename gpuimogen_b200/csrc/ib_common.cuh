@@ -17,6 +17,23 @@
 namespace ib {
 
 // ------------------------------------------------------------------------------------------
+// A timestep-derived factor (a sweep's lambda = dt / h, a source step's dt) given either by value
+// or, for loops that keep their timestep on the device (a captured CUDA graph replayed
+// iteration after iteration), as (*p * mul) / div read by the kernel itself.  The device form
+// performs the division the host would (dt / h), so both give the same bits.  A device
+// timestep of exactly 0 marks an iteration after the end time: kernels then return at once.
+// ------------------------------------------------------------------------------------------
+struct DevScalar {
+    double v;
+    const double *p;
+    double mul, div;
+    static DevScalar of(double x) { return DevScalar{x, nullptr, 1.0, 1.0}; }
+    static DevScalar device(const double *dtp, double mul, double div) { return DevScalar{0.0, dtp, mul, div}; }
+    __device__ __forceinline__ double get() const { return p ? (*p * mul) / div : v; }
+    __device__ __forceinline__ bool off() const { return p && *p == 0.0; }
+};
+
+// ------------------------------------------------------------------------------------------
 // Per-sweep thermodynamic constants (cudaFluidStep.cu:289-311), passed by value.
 // ------------------------------------------------------------------------------------------
 template <typename FT>

@@ -12,8 +12,10 @@ namespace ib {
 
 template <int ORDER>
 __global__ void __launch_bounds__(256) logtrap_kernel(double *__restrict__ gas, double *__restrict__ dust, int64_t S,
-                                                      int64_t n, DragParams d, double t)
+                                                      int64_t n, DragParams d, DevScalar dts)
 {
+    if (dts.off()) return;  // a device timestep of 0: after the end time
+    const double t = dts.get();
     for (int64_t x = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; x < n; x += (int64_t)blockDim.x * gridDim.x) {
         double *g = gas + x, *ds = dust + x;
         const double g0 = g[0], gE = g[S], g2 = g[2 * S], g3 = g[3 * S], g4 = g[4 * S];
@@ -30,8 +32,10 @@ __global__ void __launch_bounds__(256) logtrap_kernel(double *__restrict__ gas, 
 // reference divides by |dv| there).
 template <bool RK4>
 __global__ void __launch_bounds__(256) rk_drag_kernel(double *__restrict__ gas, double *__restrict__ dust, int64_t S,
-                                                      int64_t n, DragParams d, double dt)
+                                                      int64_t n, DragParams d, DevScalar dts)
 {
+    if (dts.off()) return;
+    const double dt = dts.get();
     for (int64_t x = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; x < n; x += (int64_t)blockDim.x * gridDim.x) {
         double *g = gas + x, *ds = dust + x;
         double w0, u0, f, acc, stage, wf;
@@ -64,8 +68,10 @@ __global__ void __launch_bounds__(256) rk_drag_kernel(double *__restrict__ gas, 
 // Euler with the drag rate at t = 0; cells with |dv| < 1e-9 (k = 0) are left unchanged (the
 // reference evaluates 0/0 there).
 __global__ void __launch_bounds__(256) etdrk1_kernel(double *__restrict__ gas, double *__restrict__ dust, int64_t S,
-                                                     int64_t n, DragParams d, double t)
+                                                     int64_t n, DragParams d, DevScalar dts)
 {
+    if (dts.off()) return;
+    const double t = dts.get();
     for (int64_t x = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; x < n; x += (int64_t)blockDim.x * gridDim.x) {
         double *g = gas + x, *ds = dust + x;
         const double g0 = g[0], gE = g[S], g2 = g[2 * S], g3 = g[3 * S], g4 = g[4 * S];
@@ -104,8 +110,11 @@ struct Etd2Grid {
 };
 
 __global__ void __launch_bounds__(256) etdrk2_kernel(double *__restrict__ gas, double *__restrict__ dust, int64_t S,
-                                                     const double *__restrict__ P, Etd2Grid G, DragParams d, double t)
+                                                     const double *__restrict__ P, Etd2Grid G, DragParams d,
+                                                     DevScalar dts)
 {
+    if (dts.off()) return;
+    const double t = dts.get();
     const int64_t chunks = (G.nx + blockDim.x - 1) / blockDim.x;
     const int64_t work = chunks * G.ny * G.nz;
     for (int64_t w = blockIdx.x; w < work; w += gridDim.x) {
@@ -176,7 +185,7 @@ __global__ void __launch_bounds__(256) etdrk2_kernel(double *__restrict__ gas, d
 }
 
 int launch_drag(double *gas, double *dust, int64_t slab, const int grid[3], const double h[3], const double dp[11],
-                double dt, int method, cudaStream_t st)
+                DevScalar dt, int method, cudaStream_t st)
 {
     DragParams d{dp[0], dp[1], dp[2], dp[3], dp[4], dp[5], dp[6]};
     const int64_t n = (int64_t)grid[0] * grid[1] * grid[2];

@@ -7,6 +7,7 @@
 
 #include "ib_common.cuh"
 #include "ib_tma.cuh"
+#include "ib_cyl.cuh"
 
 namespace ib {
 
@@ -47,9 +48,14 @@ Scratch &scratch();
 
 // Launchers (return IB_* status)
 int launch_sweep(int method, int slope, int precision, int dir, double *q, int64_t slab, const int grid[3],
-                 double lambda, double gamma, double rho_min, double c_iso, cudaStream_t st, int nsweep = 1);
-int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
-                    double rho_min, cudaStream_t st);
+                 DevScalar lambda, double gamma, double rho_min, double c_iso, cudaStream_t st, int nsweep = 1);
+int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3], DevScalar lambda, double gamma,
+                    double rho_min, cudaStream_t st, const CylSweep *cyl = nullptr);
+// cylindrical geometry: HLL/HLLC radial (x) and theta (y) sweeps; the source terms over dt
+int launch_sweep_cyl(int method, int slope, double *q, int64_t slab, const int grid[3], DevScalar lambda,
+                     double gamma, double rho_min, double c_iso, cudaStream_t st, const CylSweep &cs);
+int launch_cyl_source(double *q, int64_t slab, const int grid[3], double dr, double r_inner, DevScalar dt,
+                      cudaStream_t st);
 int launch_cfl(const double *q, const double *cs, int64_t slab, const int grid[3], const ib_geometry *geo,
                int method, double gamma, double *tau_dev, cudaStream_t st);
 int launch_soundspeed(const double *q, int64_t slab, int64_t n, double gamma, double *cs, cudaStream_t st);
@@ -61,6 +67,6 @@ int launch_array_boundary(double *phi, const int grid[3], int mode, int dir, int
                           cudaStream_t st);
 int launch_statics(double *phi, const ib_statics *st_list, int64_t numel, cudaStream_t st);
 int launch_drag(double *gas, double *dust, int64_t slab, const int grid[3], const double h[3], const double dp[11],
-                double dt, int method, cudaStream_t st);
+                DevScalar dt, int method, cudaStream_t st);
 
 }  // namespace ib

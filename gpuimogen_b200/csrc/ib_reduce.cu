@@ -24,11 +24,12 @@ __global__ void soundspeed_kernel(const double *__restrict__ q, int64_t slab, in
     }
 }
 
-template <int SIM, bool XJ, bool FUSED>
+template <int SIM, bool XJ, bool FUSED, bool CYL = false>
 __global__ void __launch_bounds__(256) cfl_kernel(const double *__restrict__ q, const double *__restrict__ cs_in,
                                                   int64_t slab, int64_t n, double gg1, double hmin, double hx,
                                                   double hy, double hz, int halve, double *__restrict__ partial,
-                                                  unsigned int *__restrict__ counter, double *__restrict__ tau_out)
+                                                  unsigned int *__restrict__ counter, double *__restrict__ tau_out,
+                                                  int nx = 1, double rin = 0.0)
 {
     double tmin = 1e37;
     for (int64_t x = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; x < n; x += (int64_t)blockDim.x * gridDim.x) {
@@ -41,7 +42,10 @@ __global__ void __launch_bounds__(256) cfl_kernel(const double *__restrict__ q, 
         } else {
             cs = cs_in[x];
         }
-        tmin = min_keep(tmin, cfl_cell<SIM, XJ>(rho, px, py, pz, cs, hmin, hx, hy, hz));
+        if constexpr (CYL)
+            tmin = min_keep(tmin, cfl_cell_cyl<SIM, XJ>(rho, px, py, pz, cs, hmin, hx, hy, hz, rin, (int)(x % nx)));
+        else
+            tmin = min_keep(tmin, cfl_cell<SIM, XJ>(rho, px, py, pz, cs, hmin, hx, hy, hz));
     }
     // warp then block reduction
 #pragma unroll
@@ -90,9 +94,14 @@ int launch_cfl(const double *q, const double *cs, int64_t slab, const int grid[3
     if (geo->global_rez[1] > 1) sim = 2;
     if (geo->global_rez[2] > 1) sim = 3;
     const bool xj = (method == IB_METHOD_XINJIN) && (sim > 1);  // 1-D XJ uses the HLL kernel
+    const bool cyl = (geo->shape == IB_GEOMETRY_CYLINDRICAL);
     double hmin = geo->h[0];
-    if (sim > 1 && geo->h[1] < hmin) hmin = geo->h[1];
-    if (sim > 2 && geo->h[2] < hmin) hmin = geo->h[2];
+    if (cyl) {
+        if (sim == 3) hmin = (hmin < geo->h[2]) ? hmin : geo->h[2];  // dr, dz (cflTimestep.cu:301-304)
+    } else {
+        if (sim > 1 && geo->h[1] < hmin) hmin = geo->h[1];
+        if (sim > 2 && geo->h[2] < hmin) hmin = geo->h[2];
+    }
     int64_t n = (int64_t)grid[0] * grid[1] * grid[2];
     int nb = (int)std::min<int64_t>((n + 255) / 256, (int64_t)4 * num_sms());
     if (nb < 1) nb = 1;
@@ -103,10 +112,21 @@ int launch_cfl(const double *q, const double *cs, int64_t slab, const int grid[3
     int halve = (method == IB_METHOD_HLL || method == IB_METHOD_HLLC) ? 1 : 0;
     double gg1 = gamma * (gamma - 1);
     bool fused = (cs == nullptr);
-#define IB_CFL_LAUNCH(S, X, F)                                                                            \
-    cfl_kernel<S, X, F><<<nb, 256, 0, st>>>(q, cs, slab, n, gg1, hmin, geo->h[0], geo->h[1], geo->h[2], halve, \
-                                            partial, counter, tau_dev)
-    if (fused) {
+#define IB_CFL_LAUNCH_C(S, X, F, C)                                                                          \
+    cfl_kernel<S, X, F, C><<<nb, 256, 0, st>>>(q, cs, slab, n, gg1, hmin, geo->h[0], geo->h[1], geo->h[2], halve, \
+                                               partial, counter, tau_dev, grid[0], geo->r_inner)
+#define IB_CFL_LAUNCH(S, X, F) IB_CFL_LAUNCH_C(S, X, F, false)
+    if (cyl && fused) {
+        if (xj) { if (sim == 2) IB_CFL_LAUNCH_C(2, true, true, true); else IB_CFL_LAUNCH_C(3, true, true, true); }
+        else if (sim == 1) IB_CFL_LAUNCH_C(1, false, true, true);
+        else if (sim == 2) IB_CFL_LAUNCH_C(2, false, true, true);
+        else IB_CFL_LAUNCH_C(3, false, true, true);
+    } else if (cyl) {
+        if (xj) { if (sim == 2) IB_CFL_LAUNCH_C(2, true, false, true); else IB_CFL_LAUNCH_C(3, true, false, true); }
+        else if (sim == 1) IB_CFL_LAUNCH_C(1, false, false, true);
+        else if (sim == 2) IB_CFL_LAUNCH_C(2, false, false, true);
+        else IB_CFL_LAUNCH_C(3, false, false, true);
+    } else if (fused) {
         if (xj) { if (sim == 2) IB_CFL_LAUNCH(2, true, true); else IB_CFL_LAUNCH(3, true, true); }
         else if (sim == 1) IB_CFL_LAUNCH(1, false, true);
         else if (sim == 2) IB_CFL_LAUNCH(2, false, true);
@@ -118,6 +138,7 @@ int launch_cfl(const double *q, const double *cs, int64_t slab, const int grid[3
         else IB_CFL_LAUNCH(3, false, false);
     }
 #undef IB_CFL_LAUNCH
+#undef IB_CFL_LAUNCH_C
     return check_launch();
 }
 

@@ -17,8 +17,11 @@
 //    neighbouring pencils in chunks staged in shared memory.
 #pragma once
 
+#include <type_traits>
+
 #include "ib_common.cuh"
 #include "ib_tma.cuh"
+#include "ib_cyl.cuh"
 
 namespace ib {
 
@@ -213,7 +216,7 @@ struct SweepArgs {
     double *q;
     int64_t slab;
     int nx, ny, nz;
-    double lambda;
+    DevScalar lambda;
 };
 
 // ------------------------------------------------------------------------------------------
@@ -241,7 +244,8 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
     const int64_t row = blockIdx.x;
     double *q = a.q + row * n;
     const int64_t S = a.slab;
-    const double lambda = a.lambda;
+    if (a.lambda.off()) return;  // a device timestep of 0: after the end time
+    const double lambda = a.lambda.get();
 
     double u0[CPT][5], u1[CPT][5];
     V5<FT> keep[CPT];  // right faces, later fluxes
@@ -362,7 +366,7 @@ struct PipeArgs {
     int bh;             // rows per TMA box along the pencil (n, or n / 2 for pencils above 256)
     int nh;             // boxes per pencil and slab (1 or 2)
     int64_t nblocks;    // pencil blocks in the grid
-    double lambda;
+    DevScalar lambda;
     unsigned int *err;  // set to 1 when a TMA wait ran out
     uint32_t spin;      // poll limit of the tile waits
 };
@@ -425,7 +429,8 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
         ir[m] = (ci[m] == n - 1) ? 0 : ci[m] + 1;
     }
     auto SI = [&](int k, int j) { return (k * n + j) * W + col; };
-    const double lambda = a.lambda;
+    if (a.lambda.off()) return;  // a device timestep of 0: after the end time
+    const double lambda = a.lambda.get();
     const int64_t step = gridDim.x;
     const bool leader = threadIdx.x == 0;
 
@@ -590,20 +595,22 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
 // Dynamic shared memory: the box (pipe_tile_bytes(n, 2)), 2 planes of 5 n elements of FT and
 // 5 n doubles for the SSPRK sum.
 // ------------------------------------------------------------------------------------------
-__host__ __device__ __forceinline__ size_t pair_smem_bytes(int n, int ftsize)
+__host__ __device__ __forceinline__ size_t pair_smem_bytes(int n, int ftsize, int wc)
 {
-    return pipe_tile_bytes(n, 2) + (size_t)10 * n * ftsize + (size_t)40 * n;
+    return pipe_tile_bytes(n, wc) + (size_t)10 * n * ftsize + (size_t)40 * n;
 }
 
-template <int METHOD, int SLOPE, typename FT, int DIR, int NFIX = 0, int NS = 1>
-__global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
+// WC: pencils per box (2; 4 for z sweeps of x-y planes above 1 MB, whose 16-byte rows a plane
+// apart the memory system serves poorly: 32-byte rows, three CTAs per SM)
+template <int METHOD, int SLOPE, typename FT, int DIR, int NFIX = 0, int NS = 1, int WC = 2>
+__global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : (WC == 4 ? 3 : 4))
     sweep_pair_kernel(const __grid_constant__ CUtensorMap tm, PipeArgs a, FluidConsts<FT> c)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full;
     const int n = NFIX ? NFIX : a.n;
     double *T = reinterpret_cast<double *>(smem_raw);  // the box: [slab][cell][column]
-    FT *SA = reinterpret_cast<FT *>(smem_raw + pipe_tile_bytes(n, 2));
+    FT *SA = reinterpret_cast<FT *>(smem_raw + pipe_tile_bytes(n, WC));
     FT *SB = SA + 5 * n;
     double *SS = reinterpret_cast<double *>(SB + 5 * n);
     constexpr int s0 = slot_of<METHOD, DIR>(0), s1 = slot_of<METHOD, DIR>(1), s2 = slot_of<METHOD, DIR>(2),
@@ -613,13 +620,14 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
     const int i = threadIdx.x;
     const bool act = i < n;
     const int il = (i == 0) ? n - 1 : i - 1, ir = (i == n - 1) ? 0 : i + 1;
-    const double lambda = a.lambda;
+    if (a.lambda.off()) return;  // a device timestep of 0: after the end time
+    const double lambda = a.lambda.get();
     const bool leader = threadIdx.x == 0;
     if (leader) {
         mbar_init(&full, 1);
         fence_mbar_init();
-        mbar_arrive_expect_tx(&full, (uint32_t)(80 * n));
-        pipe_load<DIR>(T, &tm, b, a, 2, &full);
+        mbar_arrive_expect_tx(&full, (uint32_t)(40 * WC * n));
+        pipe_load<DIR>(T, &tm, b, a, WC, &full);
     }
     const bool ok = mbar_wait_cta(&full, 0, a.spin);  // uniform across the CTA
     if (!ok) {
@@ -630,8 +638,8 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
         return;
     }
 #pragma unroll 1
-    for (int col = 0; col < 2; col++) {
-        auto TI = [&](int k) { return (k * n + i) * 2 + col; };
+    for (int col = 0; col < WC; col++) {
+        auto TI = [&](int k) { return (k * n + i) * WC + col; };
         double u0[5], u1[5];
         V5<FT> keep;
 #pragma unroll
@@ -698,7 +706,7 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
     fence_proxy_async_smem();
     __syncthreads();
     if (leader) {
-        pipe_store<DIR>(&tm, T, b, a, 2);
+        pipe_store<DIR>(&tm, T, b, a, WC);
         bulk_commit();
         bulk_wait_all();
     }
@@ -738,7 +746,8 @@ __global__ void __launch_bounds__(512, 1)
         ir[m] = (ci[m] == n - 1) ? 0 : ci[m] + 1;
     }
     auto SI = [&](int k, int j) { return (k * n + j) * W + col; };
-    const double lambda = a.lambda;
+    if (a.lambda.off()) return;  // a device timestep of 0: after the end time
+    const double lambda = a.lambda.get();
     const int64_t step = gridDim.x;
     const bool leader = threadIdx.x == 0;
 
@@ -902,7 +911,7 @@ struct ChunkArgs {
     int C;               // chunks per pencil: ceil(n / L)
     int npw;             // pencil blocks per line of x (nx / W; 1 for x sweeps)
     int64_t ngroups;     // pencil blocks in the grid
-    double lambda;
+    DevScalar lambda;
     unsigned int *err;   // set to 1 when a TMA wait ran out
     uint32_t spin;       // poll limit of the tile waits
 };
@@ -973,7 +982,8 @@ __global__ void __launch_bounds__(512, 2)
     const int il = (r > 0) ? r - 1 : 0, ir = (r < R - 1) ? r + 1 : R - 1;  // edge rows: unused results
     auto SI = [&](int k, int j) { return (k * R + j) * W + col; };
     const int n = a.n, C = a.C;
-    const double lambda = a.lambda;
+    if (a.lambda.off()) return;  // a device timestep of 0: after the end time
+    const double lambda = a.lambda.get();
     const bool leader = threadIdx.x == 0;
     const int64_t njobs_all = a.ngroups * C;
     const int64_t step = gridDim.x;
@@ -1124,25 +1134,70 @@ struct TileArgs {
     int n;            // pencil length
     int64_t npencil;
     int Lc;           // chunk length
-    double lambda;
+    DevScalar lambda;
+    CylPencil cyl;    // cylindrical sweeps (GEO != CYL_NONE): radial rin, dr or the theta radius rule
 };
 
-template <int W>
+// GEO == CYL_RADIAL adds one double per tile row and column: the HLL stage input's pressure
+template <int W, int GEO = CYL_NONE>
 __host__ __device__ __forceinline__ size_t tile_smem_bytes(int Lc, size_t ft)
 {
     const size_t TR = Lc + 8, TR1 = Lc + 4;
-    return sizeof(double) * (5 * TR * W + 5 * TR1 * W + 2 * 5 * 4 * W) + ft * 3 * 5 * TR * W;
+    return sizeof(double) * (5 * TR * W + 5 * TR1 * W + 2 * 5 * 4 * W) + ft * 3 * 5 * TR * W +
+           (GEO == CYL_RADIAL ? sizeof(double) * TR * W : 0);
+}
+
+// lambda times the flux difference of one cell in cylindrical geometry, component by component
+// (local order rho, E, p_n, p_t1, p_t2; p_n = p_r in a radial sweep).  fR / fL: fluxes through the
+// cell's outer / inner face.  Radial: rc = the cell centre radius; HLLC weights the faces by
+// (rc +- dr/2) / rc and subtracts dr / (2 rc) times the cell's two face pressures from p_r's
+// difference (cudaFluidStep.cu:1164-1171, 1488-1495); HLL folds lambda into those factors and
+// subtracts the stage input's pressure (adiabatic) or rho c_iso^2 with rho the predicted density
+// (isothermal) times lambda dr / rc (1837-1842, 2270-2290, 2371-2391).  CYL_THETA_DIV divides by
+// the pencil radius; CYL_THETA_LAM gets lambda already divided by it.
+template <int METHOD, int GEO>
+__device__ __forceinline__ double cyl_dflux(int k, double fR, double fL, double lam, double rc, double dr,
+                                            double rpen, double psum, double p_hll, double rho1,
+                                            const FluidConsts<double> &c)
+{
+    if constexpr (GEO == CYL_RADIAL) {
+        if constexpr (METHOD == IB_METHOD_HLLC) {
+            const double cA = (rc - .5 * dr) / (rc);
+            const double cB = (rc + .5 * dr) / (rc);
+            const double cC = 0.5 * dr / rc;
+            double d = cB * fR - cA * fL;
+            if (k == 2) d = d - cC * psum;
+            return lam * d;
+        } else {
+            const double cA = lam * (rc - .5 * dr) / (rc);
+            const double cB = lam * (rc + .5 * dr) / (rc);
+            const double cC = lam * dr / rc;
+            double d = cB * fR - cA * fL;
+            if (k == 2) {
+                if (c.isotemp == -1) d = d - p_hll * cC;
+                else d = d - rho1 * c.isotempsq * cC;
+            }
+            return d;
+        }
+    } else if constexpr (GEO == CYL_THETA_DIV) {
+        return lam * (fR - fL) / rpen;
+    } else {
+        return lam * (fR - fL);
+    }
 }
 
 // One sweep of W pencils by one CTA.  colbase[c] = offset of pencil c's first cell, colok[c] =
 // whether pencil c exists, stride = distance between consecutive cells of a pencil, n = pencil
 // length, S = slab pitch.  tsm = dynamic shared memory of tile_smem_bytes<W>(Lc).  Must be
 // called by all threads of the CTA.
-template <int METHOD, int SLOPE, typename FT, int DIR, int W>
+template <int METHOD, int SLOPE, typename FT, int DIR, int W, int GEO = CYL_NONE>
 __device__ __forceinline__ void tile_sweep(double *qbase, int64_t S, const int64_t *colbase, const bool *colok,
                                            int64_t stride, int n, int Lc, double lambda, const FluidConsts<FT> &c,
-                                           double *tsm)
+                                           double *tsm, const double *colr = nullptr, double crin = 0.0,
+                                           double cdr = 0.0)
 {
+    static_assert(GEO == CYL_NONE || std::is_same<FT, double>::value, "cylindrical sweeps are FP64");
+    static_assert(GEO != CYL_RADIAL || DIR == 1, "radial sweeps run along x");
     const int TR = Lc + 8, TR1 = Lc + 4;
     double *U0t = tsm;                       // [5][TR][W]
     double *U1t = U0t + 5 * TR * W;          // [5][TR1][W]
@@ -1151,6 +1206,7 @@ __device__ __forceinline__ void tile_sweep(double *qbase, int64_t S, const int64
     FT *PA = reinterpret_cast<FT *>(first + 5 * 4 * W);  // [5][TR][W]
     FT *PB = PA + 5 * TR * W;
     FT *PC = PB + 5 * TR * W;
+    double *PP = reinterpret_cast<double *>(PC + 5 * TR * W);  // [TR][W], GEO == CYL_RADIAL only
     constexpr int s0 = slot_of<METHOD, DIR>(0), s1 = slot_of<METHOD, DIR>(1), s2 = slot_of<METHOD, DIR>(2),
                   s3 = slot_of<METHOD, DIR>(3), s4 = slot_of<METHOD, DIR>(4);
     const int slots[5] = {s0, s1, s2, s3, s4};
@@ -1192,6 +1248,7 @@ __device__ __forceinline__ void tile_sweep(double *qbase, int64_t S, const int64
             if (METHOD == IB_METHOD_HLL) {
 #pragma unroll
                 for (int k = 0; k < 5; k++) U0t[IDX(k, r, col, TR)] = u[k];
+                if constexpr (GEO == CYL_RADIAL) PP[r * W + col] = (double)w.a[2];  // the solver's P
             }
 #pragma unroll
             for (int k = 0; k < 5; k++) PA[IDX(k, r, col, TR)] = w.a[k];
@@ -1223,10 +1280,25 @@ __device__ __forceinline__ void tile_sweep(double *qbase, int64_t S, const int64
         __syncthreads();
         for (int it = threadIdx.x; it < tr1 * W; it += blockDim.x) {  // U1 for tile rows 2..tr-3
             const int r1 = it / W, col = it - r1 * W, r = r1 + 2;
+            if constexpr (GEO == CYL_NONE) {
 #pragma unroll
-            for (int k = 0; k < 5; k++)
-                U1t[IDX(k, r1, col, TR1)] = U0t[IDX(k, r, col, TR)] -
-                                            lambda * ((double)PA[IDX(k, r, col, TR)] - (double)PA[IDX(k, r - 1, col, TR)]);
+                for (int k = 0; k < 5; k++)
+                    U1t[IDX(k, r1, col, TR1)] = U0t[IDX(k, r, col, TR)] -
+                                                lambda * ((double)PA[IDX(k, r, col, TR)] - (double)PA[IDX(k, r - 1, col, TR)]);
+            } else {
+                const double rc = (GEO == CYL_RADIAL) ? crin + mod_n(cb - 2 + r1, n) * cdr : 0.0;
+                const double rp = (GEO == CYL_RADIAL) ? 0.0 : colr[col];
+                const double lam = (GEO == CYL_THETA_LAM) ? lambda / rp : lambda;
+                const double psum = (GEO == CYL_RADIAL && METHOD == IB_METHOD_HLLC)
+                                        ? (double)PB[IDX(1, r, col, TR)] + (double)PC[IDX(1, r, col, TR)] : 0.0;
+                const double php = (GEO == CYL_RADIAL && METHOD == IB_METHOD_HLL) ? PP[r * W + col] : 0.0;
+#pragma unroll
+                for (int k = 0; k < 5; k++)
+                    U1t[IDX(k, r1, col, TR1)] =
+                        U0t[IDX(k, r, col, TR)] -
+                        cyl_dflux<METHOD, GEO>(k, (double)PA[IDX(k, r, col, TR)], (double)PA[IDX(k, r - 1, col, TR)], lam,
+                                               rc, cdr, rp, psum, php, U1t[IDX(0, r1, col, TR1)], c);
+            }
         }
         __syncthreads();
         // ---- stage B (rows of U1t; U1t row r1 is cell cb-2+r1) ----
@@ -1239,6 +1311,7 @@ __device__ __forceinline__ void tile_sweep(double *qbase, int64_t S, const int64
             if (METHOD == IB_METHOD_HLL) {
 #pragma unroll
                 for (int k = 0; k < 5; k++) U1t[IDX(k, r1, col, TR1)] = u[k];
+                if constexpr (GEO == CYL_RADIAL) PP[r1 * W + col] = (double)w.a[2];
             }
 #pragma unroll
             for (int k = 0; k < 5; k++) PA[IDX(k, r1, col, TR)] = w.a[k];
@@ -1271,10 +1344,26 @@ __device__ __forceinline__ void tile_sweep(double *qbase, int64_t S, const int64
         for (int it = threadIdx.x; it < len * W; it += blockDim.x) {  // outputs: U1t rows 2..len+1
             const int m = it / W, col = it - m * W, r1 = m + 2;
             double out[5];
+            if constexpr (GEO == CYL_NONE) {
 #pragma unroll
-            for (int k = 0; k < 5; k++)
-                out[k] = .5 * (U1t[IDX(k, r1, col, TR1)] + U0t[IDX(k, r1 + 2, col, TR)] -
-                               lambda * ((double)PA[IDX(k, r1, col, TR)] - (double)PA[IDX(k, r1 - 1, col, TR)]));
+                for (int k = 0; k < 5; k++)
+                    out[k] = .5 * (U1t[IDX(k, r1, col, TR1)] + U0t[IDX(k, r1 + 2, col, TR)] -
+                                   lambda * ((double)PA[IDX(k, r1, col, TR)] - (double)PA[IDX(k, r1 - 1, col, TR)]));
+            } else {
+                const double rc = (GEO == CYL_RADIAL) ? crin + (cb + m) * cdr : 0.0;
+                const double rp = (GEO == CYL_RADIAL) ? 0.0 : colr[col];
+                const double lam = (GEO == CYL_THETA_LAM) ? lambda / rp : lambda;
+                const double psum = (GEO == CYL_RADIAL && METHOD == IB_METHOD_HLLC)
+                                        ? (double)PB[IDX(1, r1, col, TR)] + (double)PC[IDX(1, r1, col, TR)] : 0.0;
+                const double php = (GEO == CYL_RADIAL && METHOD == IB_METHOD_HLL) ? PP[r1 * W + col] : 0.0;
+                const double rho1 = U1t[IDX(0, r1, col, TR1)];
+#pragma unroll
+                for (int k = 0; k < 5; k++)
+                    out[k] = .5 * (U1t[IDX(k, r1, col, TR1)] + U0t[IDX(k, r1 + 2, col, TR)] -
+                                   cyl_dflux<METHOD, GEO>(k, (double)PA[IDX(k, r1, col, TR)],
+                                                          (double)PA[IDX(k, r1 - 1, col, TR)], lam, rc, cdr, rp, psum,
+                                                          php, rho1, c));
+            }
             const int cell = cb + m;
             if (!single && ch == 0 && m < 4) {
 #pragma unroll
@@ -1308,12 +1397,14 @@ __device__ __forceinline__ void tile_sweep(double *qbase, int64_t S, const int64
     __syncthreads();
 }
 
-template <int METHOD, int SLOPE, typename FT, int DIR, int W>
+template <int METHOD, int SLOPE, typename FT, int DIR, int W, int GEO = CYL_NONE>
 __global__ void __launch_bounds__(256, 4) sweep_tile_kernel(TileArgs a, FluidConsts<FT> c)
 {
     extern __shared__ __align__(16) double tsm[];
     __shared__ int64_t colbase[W];
     __shared__ bool colok[W];
+    __shared__ double colr[W];
+    if (a.lambda.off()) return;  // a device timestep of 0: after the end time
     int64_t stride;
     if (DIR == 1) stride = 1;
     else if (DIR == 2) stride = a.nx;
@@ -1327,9 +1418,13 @@ __global__ void __launch_bounds__(256, 4) sweep_tile_kernel(TileArgs a, FluidCon
         else if (DIR == 2) b = (p % a.nx) + (int64_t)a.nx * a.ny * (p / a.nx);
         else b = p;
         colbase[threadIdx.x] = b;
+        // theta pencils (DIR 2): radial index p mod nx, z index p / nx
+        if (GEO == CYL_THETA_DIV || GEO == CYL_THETA_LAM)
+            colr[threadIdx.x] = theta_radius(a.cyl, (int)(p % a.nx), (int)(p / a.nx));
     }
     __syncthreads();
-    tile_sweep<METHOD, SLOPE, FT, DIR, W>(a.q, a.slab, colbase, colok, stride, a.n, a.Lc, a.lambda, c, tsm);
+    tile_sweep<METHOD, SLOPE, FT, DIR, W, GEO>(a.q, a.slab, colbase, colok, stride, a.n, a.Lc, a.lambda.get(), c, tsm,
+                                               colr, a.cyl.rin, a.cyl.dr);
 }
 
 }  // namespace ib

@@ -2,7 +2,7 @@
 #include "ib_sweep_launch.cuh"
 
 namespace ib {
-int launch_hllc64(int slope, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
+int launch_hllc64(int slope, int dir, double *q, int64_t slab, const int grid[3], DevScalar lambda, double gamma,
               double rho_min, double c_iso, cudaStream_t st, int nsweep)
 {
     return launch_sweep_slope<IB_METHOD_HLLC, double>(slope, dir, q, slab, grid, lambda, gamma, rho_min, c_iso, st, nsweep);

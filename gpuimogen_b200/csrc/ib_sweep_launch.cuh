@@ -10,9 +10,9 @@
 namespace ib {
 
 // Tile-march launch: W pencils per CTA, chunks of ~TARGET cells, every chunk >= 8 cells.
-template <int METHOD, int SLOPE, typename FT, int DIR, int W>
-int launch_tile_dw(double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c,
-                   cudaStream_t st, int target)
+template <int METHOD, int SLOPE, typename FT, int DIR, int W, int GEO = CYL_NONE>
+int launch_tile_dw(double *q, int64_t slab, const int grid[3], DevScalar lambda, const FluidConsts<FT> &c,
+                   cudaStream_t st, int target, CylPencil cyl = CylPencil{0.0, 0.0, 0, 0})
 {
     const int n = grid[DIR - 1];
     const int64_t npencil = (int64_t)grid[0] * grid[1] * grid[2] / n;
@@ -26,19 +26,19 @@ int launch_tile_dw(double *q, int64_t slab, const int grid[3], double lambda, co
         Lc = (n + nc - 1) / nc;
     }
     if (Lc > lc_max) return IB_ERROR_NOIMPLEMENT;  // pencil too short to split into valid chunks
-    TileArgs a{q, slab, grid[0], grid[1], grid[2], n, npencil, Lc, lambda};
-    const size_t shm = tile_smem_bytes<W>(Lc, sizeof(FT));
+    TileArgs a{q, slab, grid[0], grid[1], grid[2], n, npencil, Lc, lambda, cyl};
+    const size_t shm = tile_smem_bytes<W, GEO>(Lc, sizeof(FT));
     static int attr_bytes = 0;
     // opt in whenever the size grows: without it the limit is 48 KB including the static
     // shared memory and the 1 KB the driver reserves per block (48640 B at 256-cell pencils fails)
     if ((int)shm > attr_bytes) {
-        int rc = check_cuda(cudaFuncSetAttribute(sweep_tile_kernel<METHOD, SLOPE, FT, DIR, W>,
+        int rc = check_cuda(cudaFuncSetAttribute(sweep_tile_kernel<METHOD, SLOPE, FT, DIR, W, GEO>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
         if (rc) return rc;
         attr_bytes = (int)shm;
     }
     const unsigned nblk = (unsigned)((npencil + W - 1) / W);
-    sweep_tile_kernel<METHOD, SLOPE, FT, DIR, W><<<nblk, 256, shm, st>>>(a, c);
+    sweep_tile_kernel<METHOD, SLOPE, FT, DIR, W, GEO><<<nblk, 256, shm, st>>>(a, c);
     return check_launch();
 }
 
@@ -50,7 +50,7 @@ int launch_tile_dw(double *q, int64_t slab, const int grid[3], double lambda, co
 // G > 1 selects sweep_pipe_wide_kernel: blocks of W*G columns (one TMA box), computed W at a time,
 // results stored from the input tile; pencils up to 256 cells, y/z sweeps only.
 template <int METHOD, int SLOPE, typename FT, int DIR, int W, int CPT, int NFIX = 0, int G = 1>
-int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c, cudaStream_t st,
+int launch_pipe(double *q, int64_t slab, const int grid[3], DevScalar lambda, const FluidConsts<FT> &c, cudaStream_t st,
                 int nsweep)
 {
     const int nx = grid[0], ny = grid[1], nz = grid[2];
@@ -123,14 +123,15 @@ int launch_pipe(double *q, int64_t slab, const int grid[3], double lambda, const
 // Pencil-pair kernel (sweep_pair_kernel): y/z pencils of at most 256 cells or of 512 (the box
 // arrives as two rows of 256), x even; one CTA per block of two adjacent pencils.  Returns
 // IB_ERROR_NOIMPLEMENT (caller falls back) otherwise.
-template <int METHOD, int SLOPE, typename FT, int DIR, int NFIX = 0>
-int launch_pair(double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c, cudaStream_t st,
+template <int METHOD, int SLOPE, typename FT, int DIR, int NFIX = 0, int WC = 2>
+int launch_pair(double *q, int64_t slab, const int grid[3], DevScalar lambda, const FluidConsts<FT> &c, cudaStream_t st,
                 int nsweep)
 {
     static_assert(DIR != 1, "x rows take the row kernel");
+    static_assert(WC == 2 || (WC == 4 && NFIX != 512), "boxes of 2 pencils, or 4 of at most 256 cells");
     const int nx = grid[0], ny = grid[1], nz = grid[2];
     const int n = grid[DIR - 1];
-    if ((n > 256 && !(NFIX == 512 && n == 512)) || (nx & 1)) return IB_ERROR_NOIMPLEMENT;
+    if ((n > 256 && !(NFIX == 512 && n == 512)) || (nx % WC)) return IB_ERROR_NOIMPLEMENT;
     if (NFIX && n != NFIX) return IB_ERROR_NOIMPLEMENT;
     if (((uintptr_t)q & 15) || (slab * 8) % 16) return IB_ERROR_NOIMPLEMENT;
     const uint64_t other = (DIR == 2) ? nz : ny;
@@ -140,8 +141,8 @@ int launch_pair(double *q, int64_t slab, const int grid[3], double lambda, const
     const int bh = (n > 256) ? n / 2 : n, nh = (n > 256) ? 2 : 1;
     uint64_t dims[5] = {(uint64_t)nx, (uint64_t)bh, (uint64_t)nh, other, 5};
     uint64_t strides[4] = {rs, rs * bh, os, (uint64_t)slab * 8};
-    uint32_t box[5] = {2, (uint32_t)bh, (uint32_t)nh, 1, 5};
-    const int npw = nx / 2;
+    uint32_t box[5] = {WC, (uint32_t)bh, (uint32_t)nh, 1, 5};
+    const int npw = nx / WC;
     const int64_t nblocks = (int64_t)npw * other;
     if (nblocks >= (int64_t)1 << 31) return IB_ERROR_NOIMPLEMENT;
     CUtensorMap tm;
@@ -150,10 +151,10 @@ int launch_pair(double *q, int64_t slab, const int grid[3], double lambda, const
     unsigned int *err = scratch().wait_flag();
     if (!err) return IB_ERROR_NOMEM;
     const int nt = (n + 31) / 32 * 32;
-    const size_t shm = pair_smem_bytes(n, (int)sizeof(FT));
+    const size_t shm = pair_smem_bytes(n, (int)sizeof(FT), WC);
     const int ns = (nsweep == 2) ? 2 : 1;
-    auto kern = ns == 2 ? &sweep_pair_kernel<METHOD, SLOPE, FT, DIR, NFIX, 2>
-                        : &sweep_pair_kernel<METHOD, SLOPE, FT, DIR, NFIX, 1>;
+    auto kern = ns == 2 ? &sweep_pair_kernel<METHOD, SLOPE, FT, DIR, NFIX, 2, WC>
+                        : &sweep_pair_kernel<METHOD, SLOPE, FT, DIR, NFIX, 1, WC>;
     static int attr_bytes[2] = {0, 0};
     if ((int)shm > attr_bytes[ns - 1]) {
         rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
@@ -170,7 +171,7 @@ int launch_pair(double *q, int64_t slab, const int grid[3], double lambda, const
 // chunk boundaries to scratch memory.  Returns IB_ERROR_NOIMPLEMENT (caller falls back) when the
 // grid does not meet TMA's rules: x rows of even length; y/z with W dividing nx.
 template <int METHOD, int SLOPE, typename FT, int DIR, int W, int R>
-int launch_chunk(double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c, cudaStream_t st)
+int launch_chunk(double *q, int64_t slab, const int grid[3], DevScalar lambda, const FluidConsts<FT> &c, cudaStream_t st)
 {
     constexpr int L = R - 8;
     const int nx = grid[0], ny = grid[1], nz = grid[2];
@@ -244,7 +245,7 @@ int launch_chunk(double *q, int64_t slab, const int grid[3], double lambda, cons
 }
 
 template <int METHOD, int SLOPE, typename FT>
-int launch_tile_t(int dir, double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c,
+int launch_tile_t(int dir, double *q, int64_t slab, const int grid[3], DevScalar lambda, const FluidConsts<FT> &c,
                   cudaStream_t st)
 {
     if (dir == 1) return launch_tile_dw<METHOD, SLOPE, FT, 1, 1>(q, slab, grid, lambda, c, st, 248);
@@ -256,7 +257,7 @@ int launch_tile_t(int dir, double *q, int64_t slab, const int grid[3], double la
 // sweeps in the middle of an iteration).  The row and pipeline kernels apply both to a block
 // while it is on chip; the chunked pipeline and the tile kernel are launched once per sweep.
 template <int METHOD, int SLOPE, typename FT>
-int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double lambda, const FluidConsts<FT> &c,
+int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], DevScalar lambda, const FluidConsts<FT> &c,
                    cudaStream_t st, int nsweep = 1)
 {
     const int nx = grid[0], ny = grid[1], nz = grid[2];
@@ -284,6 +285,10 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
         // 0.52 -> 0.44 ms; 512-cell y pencils 4.01 -> 3.60 ms at 512 x 512 x 256) rather than the
         // persistent pipeline, which remains for other lengths when the pair kernel declines
         constexpr bool pair = true, pair512 = true;
+        // z of x-y planes above 1 MB, FP64: 4-pencil boxes through the pencil-pair kernel (512 x 512
+        // x 256: z 3.96 -> 3.58 ms); FP32 flux keeps its 8-column wide blocks (2.43 ms against 2.77
+        // for the 4-pencil boxes)
+        constexpr bool wide4 = sizeof(FT) == 8;
         static const int wide8 = [] {
             const char *e = getenv("IMOGEN_B200_WIDE8");  // 0 = 4-column blocks for wide z planes
             return (e && e[0] == '0') ? 0 : 1;
@@ -312,16 +317,21 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
                 else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1>(q, slab, grid, lambda, c, st, nsweep);
             }
         } else if (n == 256) {
-            // FP32 flux: 8-column blocks (64-byte rows) computed 4 columns at a time (3.48 -> 2.52
-            // ms at 512 x 512 x 256).  FP64 is bound by its arithmetic there and keeps 4 columns:
-            // its planes leave room for only 2 columns per group, which is slower.
+            // z of x-y planes above 1 MB: FP64 takes 4-pencil boxes (32-byte rows) through the
+            // pencil-pair kernel; the FP32 flux takes 8-column wide blocks (64-byte rows) computed 4
+            // columns at a time (3.48 -> 2.52 ms at 512 x 512 x 256); the 4-column pipeline blocks
+            // remain where neither applies.
+            if (wide4) rc = launch_pair<METHOD, SLOPE, FT, 3, 256, 4>(q, slab, grid, lambda, c, st, nsweep);
             if constexpr (sizeof(FT) == 4) {
-                if (wide8 == 1) rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2, 256, 2>(q, slab, grid, lambda, c, st, nsweep);
+                if (rc == IB_ERROR_NOIMPLEMENT && wide8 == 1)
+                    rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2, 256, 2>(q, slab, grid, lambda, c, st, nsweep);
             }
             if (rc == IB_ERROR_NOIMPLEMENT) rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2, 256>(q, slab, grid, lambda, c, st, nsweep);
         } else if (n <= 256) {
+            if (wide4) rc = launch_pair<METHOD, SLOPE, FT, 3, 0, 4>(q, slab, grid, lambda, c, st, nsweep);
             if constexpr (sizeof(FT) == 4) {
-                if (wide8 == 1) rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2, 0, 2>(q, slab, grid, lambda, c, st, nsweep);
+                if (rc == IB_ERROR_NOIMPLEMENT && wide8 == 1)
+                    rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2, 0, 2>(q, slab, grid, lambda, c, st, nsweep);
             }
             if (rc == IB_ERROR_NOIMPLEMENT) rc = launch_pipe<METHOD, SLOPE, FT, 3, 4, 2>(q, slab, grid, lambda, c, st, nsweep);
         } else if (n == 512) {
@@ -415,7 +425,7 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], double l
 }
 
 template <int METHOD, typename FT>
-int launch_sweep_slope(int slope, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
+int launch_sweep_slope(int slope, int dir, double *q, int64_t slab, const int grid[3], DevScalar lambda, double gamma,
                        double rho_min, double c_iso, cudaStream_t st, int nsweep)
 {
     FluidConsts<FT> c = make_consts<FT>(gamma, rho_min, c_iso);
@@ -431,11 +441,44 @@ int launch_sweep_slope(int slope, int dir, double *q, int64_t slab, const int gr
     }
 }
 
-int launch_hllc64(int slope, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
+// Cylindrical sweeps (radial x, theta y) run in the tile kernel with the geometry's update, FP64
+template <int METHOD, int SLOPE>
+int launch_sweep_cyl_t(double *q, int64_t slab, const int grid[3], DevScalar lambda, const FluidConsts<double> &c,
+                       cudaStream_t st, const CylSweep &cs)
+{
+    switch (cs.kind) {
+    case CYL_RADIAL:
+        return launch_tile_dw<METHOD, SLOPE, double, 1, 1, CYL_RADIAL>(q, slab, grid, lambda, c, st, 248, cs.pencil);
+    case CYL_THETA_DIV:
+        return launch_tile_dw<METHOD, SLOPE, double, 2, 4, CYL_THETA_DIV>(q, slab, grid, lambda, c, st, 56, cs.pencil);
+    case CYL_THETA_LAM:
+        return launch_tile_dw<METHOD, SLOPE, double, 2, 4, CYL_THETA_LAM>(q, slab, grid, lambda, c, st, 56, cs.pencil);
+    default: return IB_ERROR_INVALID_ARGS;
+    }
+}
+
+template <int METHOD>
+int launch_sweep_cyl_slope(int slope, double *q, int64_t slab, const int grid[3], DevScalar lambda, double gamma,
+                           double rho_min, double c_iso, cudaStream_t st, const CylSweep &cs)
+{
+    FluidConsts<double> c = make_consts<double>(gamma, rho_min, c_iso);
+    switch (slope) {
+    case IB_SLOPE_OSPRE: return launch_sweep_cyl_t<METHOD, IB_SLOPE_OSPRE>(q, slab, grid, lambda, c, st, cs);
+    case IB_SLOPE_MC: return launch_sweep_cyl_t<METHOD, IB_SLOPE_MC>(q, slab, grid, lambda, c, st, cs);
+    case IB_SLOPE_VANLEER: return launch_sweep_cyl_t<METHOD, IB_SLOPE_VANLEER>(q, slab, grid, lambda, c, st, cs);
+    case IB_SLOPE_MINMOD: return launch_sweep_cyl_t<METHOD, IB_SLOPE_MINMOD>(q, slab, grid, lambda, c, st, cs);
+    case IB_SLOPE_SUPERBEE: return launch_sweep_cyl_t<METHOD, IB_SLOPE_SUPERBEE>(q, slab, grid, lambda, c, st, cs);
+    case IB_SLOPE_VANALBADA: return launch_sweep_cyl_t<METHOD, IB_SLOPE_VANALBADA>(q, slab, grid, lambda, c, st, cs);
+    case IB_SLOPE_ZERO: return launch_sweep_cyl_t<METHOD, IB_SLOPE_ZERO>(q, slab, grid, lambda, c, st, cs);
+    default: return IB_ERROR_INVALID_ARGS;
+    }
+}
+
+int launch_hllc64(int slope, int dir, double *q, int64_t slab, const int grid[3], DevScalar lambda, double gamma,
                   double rho_min, double c_iso, cudaStream_t st, int nsweep);
-int launch_hllc32(int slope, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
+int launch_hllc32(int slope, int dir, double *q, int64_t slab, const int grid[3], DevScalar lambda, double gamma,
                   double rho_min, double c_iso, cudaStream_t st, int nsweep);
-int launch_hll64(int slope, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
+int launch_hll64(int slope, int dir, double *q, int64_t slab, const int grid[3], DevScalar lambda, double gamma,
                  double rho_min, double c_iso, cudaStream_t st, int nsweep);
 
 }  // namespace ib

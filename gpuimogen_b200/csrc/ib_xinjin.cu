@@ -100,10 +100,18 @@ __device__ __forceinline__ void flux_limit_pair(double A1, double B1, double A2,
 // barriers.  RELOAD (x rows): the corrector re-reads its base state from memory, coalesced and
 // L2-resident, rather than keep it in registers; fewer spills made x 0.85 -> 0.82 ms at 256^3 and
 // 0.30 -> 0.27 ms at 2048^2, while the strided y/z loads measured slower that way.
-template <int FLIM, int W, int CPT, bool RELOAD>
+//
+// Cylindrical geometry (GEO, ib_cyl.cuh): radial x sweeps weight the relaxation fluxes by the face
+// radii and add 2 dr / r_c times the stage input's pressure to p_r, the factor 2 compensating the
+// halved lambda (cudaFluidStep.cu:2463-2470, 2576-2581, 2603-2607); theta y sweeps divide the
+// update by the pencil radius or lambda by it first (2478-2480, 2582-2585, 2608-2611).
+template <int FLIM, int W, int CPT, bool RELOAD, int GEO = CYL_NONE>
 __global__ void __launch_bounds__(1024) xj_pencil_kernel(double *q, int64_t slab, int nx, int ny, int nz, int dir,
-                                                         double lambda, double gamma, double minmass, double mintemp)
+                                                         DevScalar lam_in, double gamma, double minmass, double mintemp,
+                                                         CylPencil cyl)
 {
+    if (lam_in.off()) return;  // a device timestep of 0: after the end time
+    const double lambda = lam_in.get();
     extern __shared__ __align__(16) double sm[];
     __shared__ double red[32 * W];
     const int n = (dir == 1) ? nx : (dir == 2 ? ny : nz);
@@ -121,6 +129,10 @@ __global__ void __launch_bounds__(1024) xj_pencil_kernel(double *q, int64_t slab
     else { base = p; stride = (int64_t)nx * ny; }
     const int nslot = 1 + dir;
     const double gm1 = gamma - 1.0;
+    // theta pencils: the radius of this column's pencil (radial index p mod nx, z index p / nx)
+    const double rpen = (GEO == CYL_THETA_DIV || GEO == CYL_THETA_LAM)
+                            ? theta_radius(cyl, (int)(p % nx), (int)(p / nx)) : 1.0;
+    double pcell[GEO == CYL_RADIAL ? CPT : 1];  // radial: each cell's stage-input pressure
 
     double u0[CPT][5], u1[CPT][5];
     // 1 / density of each cell's current stage input: the product build computes it once per stage
@@ -170,6 +182,7 @@ __global__ void __launch_bounds__(1024) xj_pencil_kernel(double *q, int64_t slab
                 const double Pv = gm1 * (q1 - .5 * (q4 * q4 + q3 * q3 + q2 * q2) * ir);
                 const double Vx = Q[nslot] * ir;
 #endif
+                if constexpr (GEO == CYL_RADIAL) pcell[m] = Pv;
 #pragma unroll
                 for (int k = 0; k < 5; k++) {
                     const double qk = Q[k];
@@ -227,7 +240,21 @@ __global__ void __launch_bounds__(1024) xj_pencil_kernel(double *q, int64_t slab
                 for (int k = 0; k < 5; k++) {
                     // the block's own pencils are unchanged in memory until the final store
                     const double b = (RELOAD && stage == 1) ? q[k * slab + base + i * stride] : u0[m][k];
-                    pr[k] = b - lam * (Rb[IX(k, i)] - Rb[IX(k, il)] - Lb[IX(k, ir)] + Lb[IX(k, i)]);
+                    if constexpr (GEO == CYL_NONE) {
+                        pr[k] = b - lam * (Rb[IX(k, i)] - Rb[IX(k, il)] - Lb[IX(k, ir)] + Lb[IX(k, i)]);
+                    } else if constexpr (GEO == CYL_THETA_DIV) {
+                        pr[k] = b - lam * (Rb[IX(k, i)] - Rb[IX(k, il)] - Lb[IX(k, ir)] + Lb[IX(k, i)]) / rpen;
+                    } else if constexpr (GEO == CYL_THETA_LAM) {
+                        const double lr = lam / rpen;
+                        pr[k] = b - lr * (Rb[IX(k, i)] - Rb[IX(k, il)] - Lb[IX(k, ir)] + Lb[IX(k, i)]);
+                    } else {
+                        const double rc = cyl.rin + i * cyl.dr;
+                        const double cA = (rc - .5 * cyl.dr) / (rc);
+                        const double cB = (rc + .5 * cyl.dr) / (rc);
+                        const double cC = 2.0 * cyl.dr / rc;
+                        pr[k] = b - lam * (cB * Rb[IX(k, i)] - cA * Rb[IX(k, il)] - cB * Lb[IX(k, ir)] + cA * Lb[IX(k, i)]);
+                        if (k == 2) pr[k] += lam * cC * pcell[m];
+                    }
                 }
                 double p0 = pr[0], p1 = pr[1];
                 const double p2 = pr[2], p3 = pr[3], p4 = pr[4];
@@ -253,9 +280,13 @@ __global__ void __launch_bounds__(1024) xj_pencil_kernel(double *q, int64_t slab
     }
 }
 
-int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3], double lambda, double gamma,
-                    double rho_min, cudaStream_t st)
+int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3], DevScalar lambda, double gamma,
+                    double rho_min, cudaStream_t st, const CylSweep *cyl)
 {
+    const int geo = cyl ? cyl->kind : CYL_NONE;
+    const CylPencil cp = cyl ? cyl->pencil : CylPencil{0.0, 0.0, 0, 0};
+    if ((geo == CYL_RADIAL && dir != 1) || ((geo == CYL_THETA_DIV || geo == CYL_THETA_LAM) && dir != 2))
+        return IB_ERROR_INVALID_ARGS;
     const int n = grid[dir - 1];
     const int64_t N = (int64_t)grid[0] * grid[1] * grid[2];
     if (n > 2048) return IB_ERROR_NOIMPLEMENT;  // 1024 threads x 2 cells per pencil block
@@ -270,7 +301,7 @@ int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3
     // blocks of wider runs (256^3: y 1.33 ms at W = 2 against 1.39 at W = 4; 128^3: W = 4 0.146 ms,
     // W = 8 0.171); W = 2 in a 1024-thread block still beats W = 1 (512 x 512 x 64, y: 1.55 / 1.78).
     int W = 1;
-    if (dir > 1) {
+    if (dir > 1 && geo == CYL_NONE) {  // cylindrical theta sweeps: one pencil per block
         for (int w = 4; w >= 2; w >>= 1)
             if (w <= xjw && grid[0] % w == 0 && n * w <= 512) { W = w; break; }
         // pencils of 257-512 cells: 4 pencils of 2 cells a thread (full 32-byte runs) rather than 2
@@ -286,27 +317,37 @@ int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3
     const size_t shm_cap = 227 * 1024 - 2048;  // opt-in limit minus the kernel's static shared memory
     if (shm > shm_cap) return IB_ERROR_NOIMPLEMENT;
     const unsigned nblk = (unsigned)(np / W);
-#define IB_XJ(F, WW, CC, RR)                                                                                  \
+#define IB_XJ_G(F, WW, CC, RR, GG)                                                                            \
     do {                                                                                                      \
         static bool attr_set = false;                                                                         \
         if (!attr_set) {                                                                                      \
-            int rc_ = check_cuda(cudaFuncSetAttribute(xj_pencil_kernel<F, WW, CC, RR>,                        \
+            int rc_ = check_cuda(cudaFuncSetAttribute(xj_pencil_kernel<F, WW, CC, RR, GG>,                    \
                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm_cap)); \
             if (rc_) return rc_;                                                                              \
             attr_set = true;                                                                                  \
         }                                                                                                     \
-        xj_pencil_kernel<F, WW, CC, RR><<<nblk, nt, shm, st>>>(q, slab, grid[0], grid[1], grid[2], dir,       \
-                                                               lambda, gamma, rho_min, mintemp);              \
+        xj_pencil_kernel<F, WW, CC, RR, GG><<<nblk, nt, shm, st>>>(q, slab, grid[0], grid[1], grid[2], dir,   \
+                                                                   lambda, gamma, rho_min, mintemp, cp);      \
     } while (0)
-#define IB_XJ_W(F)                                            \
-    do {                                                      \
-        if (W == 4 && CPT == 2) IB_XJ(F, 4, 2, true);         \
-        else if (W == 4) IB_XJ(F, 4, 1, false);               \
-        else if (W == 2) IB_XJ(F, 2, 1, false);               \
-        else if (CPT == 2 && dir == 1) IB_XJ(F, 1, 2, true);  \
-        else if (CPT == 2) IB_XJ(F, 1, 2, false);             \
-        else if (dir == 1) IB_XJ(F, 1, 1, true);              \
-        else IB_XJ(F, 1, 1, false);                           \
+#define IB_XJ(F, WW, CC, RR) IB_XJ_G(F, WW, CC, RR, CYL_NONE)
+#define IB_XJ_W(F)                                                                    \
+    do {                                                                              \
+        if (geo == CYL_RADIAL) {                                                      \
+            if (CPT == 2) IB_XJ_G(F, 1, 2, true, CYL_RADIAL);                         \
+            else IB_XJ_G(F, 1, 1, true, CYL_RADIAL);                                  \
+        } else if (geo == CYL_THETA_DIV) {                                            \
+            if (CPT == 2) IB_XJ_G(F, 1, 2, false, CYL_THETA_DIV);                     \
+            else IB_XJ_G(F, 1, 1, false, CYL_THETA_DIV);                              \
+        } else if (geo == CYL_THETA_LAM) {                                            \
+            if (CPT == 2) IB_XJ_G(F, 1, 2, false, CYL_THETA_LAM);                     \
+            else IB_XJ_G(F, 1, 1, false, CYL_THETA_LAM);                              \
+        } else if (W == 4 && CPT == 2) IB_XJ(F, 4, 2, true);                          \
+        else if (W == 4) IB_XJ(F, 4, 1, false);                                       \
+        else if (W == 2) IB_XJ(F, 2, 1, false);                                       \
+        else if (CPT == 2 && dir == 1) IB_XJ(F, 1, 2, true);                          \
+        else if (CPT == 2) IB_XJ(F, 1, 2, false);                                     \
+        else if (dir == 1) IB_XJ(F, 1, 1, true);                                      \
+        else IB_XJ(F, 1, 1, false);                                                   \
     } while (0)
     switch (flim) {
     case IB_FLUX_OSPRE: IB_XJ_W(IB_FLUX_OSPRE); break;
@@ -317,6 +358,7 @@ int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3
     }
 #undef IB_XJ_W
 #undef IB_XJ
+#undef IB_XJ_G
     return check_launch();
 }
 

@@ -72,7 +72,7 @@ class IbGeometry(ctypes.Structure):
 
 class IbNumerics(ctypes.Structure):
     _fields_ = [("slope_limiter", ctypes.c_int32), ("flux_limiter", ctypes.c_int32),
-                ("precision", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("precision", ctypes.c_int32), ("flags", ctypes.c_int32)]
 
 
 class IbThermo(ctypes.Structure):
@@ -85,6 +85,12 @@ class IbThermo(ctypes.Structure):
 class IbDragSource(ctypes.Structure):
     _fields_ = [("thermo_gas", IbThermo), ("thermo_dust", IbThermo), ("method", ctypes.c_int32),
                 ("reserved", ctypes.c_int32)]
+
+
+class IbTimeState(ctypes.Structure):
+    _fields_ = [("tau", ctypes.c_double * 4), ("dt", ctypes.c_double), ("time", ctypes.c_double),
+                ("kahan", ctypes.c_double), ("cfl", ctypes.c_double), ("tmax", ctypes.c_double),
+                ("iteration", ctypes.c_int64), ("nfluids", ctypes.c_int32), ("status", ctypes.c_int32)]
 
 
 class IbDragModel(ctypes.Structure):
@@ -125,6 +131,13 @@ EXPORTS = {
                                            ctypes.POINTER(IbGeometry), ctypes.POINTER(ctypes.c_double),
                                            ctypes.c_int, ctypes.POINTER(IbNumerics), ctypes.POINTER(IbDragSource),
                                            ctypes.c_void_p]),
+    "ib_completeTimestepDeviceDt": (ctypes.c_int, [ctypes.POINTER(IbFluid), ctypes.POINTER(IbFluidThermo),
+                                                   ctypes.c_int, ctypes.POINTER(IbGeometry), ctypes.c_void_p,
+                                                   ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                                                   ctypes.POINTER(IbNumerics), ctypes.POINTER(IbDragSource),
+                                                   ctypes.c_void_p]),
+    "ib_timeUpdate": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "ib_timeAdvance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "ib_cudaSoundspeed": (ctypes.c_int, [ctypes.POINTER(IbFluid), ctypes.c_double, ctypes.c_void_p,
                                          ctypes.c_void_p]),
     "ib_cflTimestep": (ctypes.c_int, [ctypes.POINTER(IbFluid), ctypes.c_void_p, ctypes.POINTER(IbGeometry),
@@ -312,28 +325,40 @@ class Fluid:
 
 
 class Geometry:
-    """GeometryManager subset: cell sizes, shape (square only) and global resolution."""
+    """GeometryManager subset: cell sizes, shape and global resolution.
 
-    def __init__(self, shape, h=None):
+    Square (default): h = [dx, dy, dz].  Cylindrical (geometryCylindrical, GeometryManager.m:
+    300-311): x = r, y = theta, z = z, h = [dr, dtheta, dz] and r_inner = the radius of the centre
+    of radial cell 0."""
+
+    def __init__(self, shape, h=None, cylindrical=False, r_inner=0.0):
         self.shape = tuple(int(s) for s in shape)
         if h is None:
             h = [1.0 / s for s in self.shape]
         self.h = [float(x) for x in h]
+        self.cylindrical = bool(cylindrical)
+        self.r_inner = float(r_inner)
 
     def c_struct(self):
         g = IbGeometry()
         for i in range(3):
             g.h[i] = self.h[i]
             g.global_rez[i] = self.shape[i]
-        g.r_inner = 0.0
-        g.shape = 0
+        g.r_inner = self.r_inner
+        g.shape = 1 if self.cylindrical else 0
         return g
 
 
-def numerics(slope="ospre", fluxlim="ospre", precision="fp64"):
+FLAG_CYL_GEOMETRIC_RADIUS = 1
+
+
+def numerics(slope="ospre", fluxlim="ospre", precision="fp64", geometric_radius=False):
+    """Numerical switches; geometric_radius: cylindrical theta sweeps use the cell centre radius
+    instead of the reference's radius arithmetic."""
     return IbNumerics(SLOPE[slope] if isinstance(slope, str) else slope,
                       FLUXLIM[fluxlim] if isinstance(fluxlim, str) else fluxlim,
-                      PRECISION[precision] if isinstance(precision, str) else precision, 0)
+                      PRECISION[precision] if isinstance(precision, str) else precision,
+                      FLAG_CYL_GEOMETRIC_RADIUS if geometric_radius else 0)
 
 
 def _dvec(params):
@@ -384,6 +409,38 @@ def completeTimestep(fluids, geometry, params, num=None, drag=None):
                                        DRAG[method] if isinstance(method, str) else int(method), 0))
     _check("ib_completeTimestep", _lib().ib_completeTimestep(fs, th, len(fluids), ctypes.byref(g), p, n, nm, ds,
                                                              _stream()))
+
+
+def _drag_struct(drag):
+    if drag is None:
+        return None
+    tg, td, method = drag
+    return IbDragSource(thermo_struct(tg), thermo_struct(td), DRAG[method] if isinstance(method, str) else int(method),
+                        0)
+
+
+def completeTimestepDeviceDt(fluids, geometry, dt_device, params, num=None, drag=None):
+    """completeTimestep with the timestep read by the kernels from device memory (dt_device: a
+    device address, e.g. of an ib_time_state's dt); params = [purehydro, iteration, method]."""
+    if isinstance(fluids, Fluid):
+        fluids = [fluids]
+    fs = (IbFluid * len(fluids))(*[f.c_struct() for f in fluids])
+    th = (IbFluidThermo * len(fluids))(*[f.thermo() for f in fluids])
+    g = geometry.c_struct()
+    p, n = _dvec(params)
+    nm = ctypes.byref(num) if num is not None else None
+    ds = _drag_struct(drag)
+    _check("ib_completeTimestepDeviceDt", _lib().ib_completeTimestepDeviceDt(
+        fs, th, len(fluids), ctypes.byref(g), ctypes.c_void_p(int(dt_device)), p, n, nm,
+        ctypes.byref(ds) if ds is not None else None, _stream()))
+
+
+def timeUpdate(ts_device):
+    _check("ib_timeUpdate", _lib().ib_timeUpdate(ctypes.c_void_p(int(ts_device)), _stream()))
+
+
+def timeAdvance(ts_device):
+    _check("ib_timeAdvance", _lib().ib_timeAdvance(ctypes.c_void_p(int(ts_device)), _stream()))
 
 
 def cudaSoundspeed(fluid, gamma):

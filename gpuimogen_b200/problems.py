@@ -90,3 +90,30 @@ def random_jumpy(shape, gamma=1.4, seed=11):
     vx, vy, vz = blocks(-1.5, 1.5), blocks(-1.0, 1.0), blocks(-1.0, 1.0)
     E = P / (gamma - 1) + 0.5 * rho * (vx * vx + vy * vy + vz * vz)
     return pack(shape, rho, E, rho * vx, rho * vy, rho * vz)
+
+
+def rotating_annulus(shape, r_inner=1.0, dr=0.05, gamma=1.4, seed=31, amp=0.05):
+    """Cylindrical test state (x = r, y = theta, z = z): a rotating annulus with v_theta = r^-1/2,
+    a radial pressure gradient and seeded smooth perturbations of every field, for the cylindrical
+    parity tests.  The radial cell i has its centre at r_inner + i dr."""
+    nx, ny, nz = shape
+    rng = np.random.Generator(np.random.Philox(seed))
+    r = (r_inner + dr * np.arange(nx))[None, None, :]
+    th = (np.arange(ny) / ny)[None, :, None]
+    z = (np.arange(nz) / nz)[:, None, None]
+
+    def noise():
+        f = np.zeros((nz, ny, nx))
+        for _ in range(3):
+            k, m, l = rng.integers(1, 4), rng.integers(0, 3), rng.integers(0, 2)
+            ph = rng.uniform(0, 2 * np.pi)
+            f = f + rng.uniform(-1, 1) * np.cos(2 * np.pi * (k * (r - r_inner) / (dr * nx) + m * th + l * z) + ph)
+        return f
+
+    rho = (1.0 + 0.5 * (r - r_inner)) * (1.0 + amp * noise())
+    P = 1.0 / r * (1.0 + amp * noise())
+    vr = amp * noise()
+    vth = r ** -0.5 * (1.0 + amp * noise())
+    vz = amp * noise()
+    E = P / (gamma - 1) + 0.5 * rho * (vr * vr + vth * vth + vz * vz)
+    return pack(shape, rho, E, rho * vr, rho * vth, rho * vz)

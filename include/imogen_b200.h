@@ -122,8 +122,12 @@ typedef struct ib_fluid_thermo {
 } ib_fluid_thermo;
 
 /* Geometry (GeometryParams, cudaCommon.h; accessMatlabGeometryClass, cudaCommonML.cu:453-481).
- * Only shape 0 = SQUARE is implemented. global_rez gives the dimensionality for the CFL
- * (globalDomainRez, cflTimestep.cu:85-87). */
+ * shape: IB_GEOMETRY_SQUARE (h = dx, dy, dz) or IB_GEOMETRY_CYLINDRICAL (x = r, y = theta,
+ * z = z; h = dr, dtheta, dz; r_inner = radius of the centre of radial cell 0, pInnerRadius,
+ * GeometryManager.m:300-311).  global_rez gives the dimensionality for the CFL
+ * (globalDomainRez, cflTimestep.cu:85-87).  The RZ layout (ny = 1) of the reference's
+ * RZCYLINDRICAL is not a separate shape here: a cylindrical grid with ny = 1 sweeps r and z. */
+enum { IB_GEOMETRY_SQUARE = 0, IB_GEOMETRY_CYLINDRICAL = 1 };
 typedef struct ib_geometry {
     double h[3];
     double r_inner;
@@ -132,12 +136,17 @@ typedef struct ib_geometry {
 } ib_geometry;
 
 /* Numerical switches that the reference fixes at compile time; NULL = reference defaults
- * (Ospre slope limiter, Ospre flux limiter, FP64). */
+ * (Ospre slope limiter, Ospre flux limiter, FP64, the reference's cylindrical arithmetic).
+ * flags: IB_FLAG_CYL_GEOMETRIC_RADIUS makes cylindrical theta sweeps use the cell centre radius
+ * r_inner + i dr; without it they compute the radius as the reference's kernels do, with the theta
+ * cell size as the radial step (cudaFluidStep.cu:305-307, 340, 848-855) and, for the sweeps whose
+ * memory layout is theta,z,r on a 2-D grid, r_inner for every radius. */
+enum { IB_FLAG_CYL_GEOMETRIC_RADIUS = 1 };
 typedef struct ib_numerics {
     int32_t slope_limiter;
     int32_t flux_limiter;
     int32_t precision;
-    int32_t reserved;
+    int32_t flags;
 } ib_numerics;
 
 /* Microphysics of one fluid for the drag source (ThermoDetails, cudaCommon.h;
@@ -222,7 +231,11 @@ IB_API int ib_setTileWaitLimit(long long polls);
 /* Replaces the cudaFluidStep mex (gpuclass/cudaFluidStep.cu:161-227): one SSPRK2 directional
  * sweep of one fluid, in place, without boundary fill.
  * params = [dt, purehydro, gamma, rho_min, method (1 HLL | 2 HLLC | 3 XJ), direction (1..3)
- *           (, c_isothermal)], nparams 6 or 7; with 7 the fluid is isothermal and gamma := 2. */
+ *           (, c_isothermal (, theta_layout))], nparams 6, 7 or 8; c_isothermal != -1 makes the
+ * fluid isothermal and gamma := 2.  In cylindrical geometry direction 1 is r and 2 theta; the
+ * reference takes a theta sweep's form from the arrays' memory permutation, which this API's
+ * XYZ-ordered arrays do not carry: theta_layout 0 (default) = the form of layout theta,r,z
+ * (FLUX_THETA_213), 1 = theta,z,r (FLUX_THETA_231).  Cylindrical sweeps are FP64 only. */
 IB_API int ib_cudaFluidStep(ib_fluid *fluid, const ib_geometry *geo, const double *params, int nparams,
                      const ib_numerics *num, void *stream);
 
@@ -255,6 +268,45 @@ typedef struct ib_drag_source {
 IB_API int ib_completeTimestep(ib_fluid *fluids, const ib_fluid_thermo *thermo, int nfluids,
                                const ib_geometry *geo, const double *params, int nparams,
                                const ib_numerics *num, const ib_drag_source *drag, void *stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * The main loop with its timestep on the device (no reference counterpart: the reference reads
+ * tau back to the host every iteration, TimeManager.m:124-186).  A loop that keeps dt on the
+ * device can capture a whole iteration -- CFL of every fluid, ib_timeUpdate,
+ * ib_completeTimestepDeviceDt, ib_timeAdvance -- in a CUDA graph and replay it without host
+ * reads between iterations (one graph per iteration index modulo 6, which fixes the sweep
+ * order).  After the end time dt is 0 and every kernel that reads it returns at once, so
+ * iterations replayed past the end change nothing.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct ib_time_state {  /* device memory */
+    double tau[4];      /* CFL time of each fluid, written by ib_cflTimestepFused(..., tau_device = &tau[k]) */
+    double dt;          /* this iteration's timestep; 0 once time has reached tmax */
+    double time;        /* simulated time */
+    double kahan;       /* compensation of the time sum */
+    double cfl;         /* CFL number */
+    double tmax;        /* end time (INFINITY: none) */
+    int64_t iteration;  /* iterations taken */
+    int32_t nfluids;    /* tau entries in use, 1..4 */
+    int32_t status;     /* 1 once a non-finite CFL time stopped the loop (dt stays 0) */
+} ib_time_state;
+
+/* TimeManager.update (time/TimeManager.m:124-186) on the device: dt = cfl * min(tau[0..nfluids)),
+ * clipped so that time + 2 dt <= tmax; dt = 0 once time >= tmax (1 - 1e-14) or status != 0. */
+IB_API int ib_timeUpdate(ib_time_state *ts, void *stream);
+
+/* TimeManager.step (:270-277) on the device: iteration += 1 and time += 2 dt (compensated), when
+ * dt > 0. */
+IB_API int ib_timeAdvance(ib_time_state *ts, void *stream);
+
+/* ib_completeTimestep with the timestep read from device memory (*dt_device) by every kernel
+ * (lambda = *dt_device / h in the sweeps, computed as the host form computes it, so both give
+ * the same bits); params = [purehydro, iteration, method].  No host value depends on dt, so the
+ * call can be captured in a CUDA graph after a first, uncaptured call of the same shape has set
+ * up the library's scratch memory and kernel attributes. */
+IB_API int ib_completeTimestepDeviceDt(ib_fluid *fluids, const ib_fluid_thermo *thermo, int nfluids,
+                                       const ib_geometry *geo, const double *dt_device, const double *params,
+                                       int nparams, const ib_numerics *num, const ib_drag_source *drag,
+                                       void *stream);
 
 /* Replaces the cudaSoundspeed mex for hydro (gpuclass/cudaSoundspeed.cu:54-105,
  * calculateSoundspeed :107-150): cs_out[N] = sqrt(max(0, gamma(gamma-1) e_int / rho)). */

@@ -220,6 +220,29 @@ static void rowbuf_free(rowbuf *r) { free(r->u[0]); }
 
 static inline int wrap(int i, int n) { return (i < 0) ? i + n : ((i >= n) ? i - n : i); }
 
+/* Cylindrical geometry of one pencil.  kind: 0 square (or the z sweep), 1 radial sweep (the
+ * face-area factors and the geometric pressure term), 2 theta sweep with the flux difference
+ * divided by r (FLUX_THETA_213), 3 theta sweep with lambda divided by r first (FLUX_THETA_231).
+ * Radial cell i has its centre at rin + i dr; r is a theta pencil's radius. */
+typedef struct {
+    int kind;
+    double rin, dr;
+    double r;
+} rowgeo;
+
+static const rowgeo ROWGEO_SQUARE = {0, 0.0, 0.0, 0.0};
+
+/* Radius the reference's theta kernels compute for the pencil at radial index j (layout
+ * theta,r,z): thread row ty = j mod 4 starts at ty dr + rin and every pass of the block's row
+ * loop adds 4 dr (YBLOCKS = 4; cudaFluidStep.cu:848-850, 1112-1116, 1844-1846, 2462-2464). */
+static double theta_radius_213(int j, double rin, double dr)
+{
+    double r = (double)(j % 4) * dr + rin;
+    int m;
+    for (m = 0; m < j / 4; m++) r = r + 4.0 * dr;
+    return r;
+}
+
 /* ------------------------------------------------------------------------------------------
  * HLLC, 2nd order MUSCL (cukern_HLLC_2ndorder, cudaFluidStep.cu:1124-1463), one stage.
  * in[5]: conserved state of the row (local order).  flux[k][i] = flux through face i+1/2.
@@ -335,19 +358,41 @@ static void hllc_row_flux(rowbuf *r, double *const in[5], const fconst *c, int s
     }
 }
 
+/* lambda times the flux difference of cell i, component k, after hllc_row_flux.  Radial
+ * sweeps weight the faces by their radii and add the cell's mean face pressure to the radial
+ * momentum (cylgeomA/B/C, cudaFluidStep.cu:1164-1171, 1488-1495); theta sweeps divide by r
+ * (1499-1505) or use lambda / r (1506-1512). */
+static double hllc_dflux(const rowbuf *r, const rowgeo *G, double lam, int k, int i)
+{
+    const int il = wrap(i - 1, r->n);
+    const double fr = r->flux[k][i], fl = r->flux[k][il];
+    if (G->kind == 1) {
+        double R = G->rin + i * G->dr;
+        double cA = (R - .5 * G->dr) / (R);
+        double cB = (R + .5 * G->dr) / (R);
+        double cC = 0.5 * G->dr / R;
+        double d = cB * fr - cA * fl;
+        if (k == 2) d = d - cC * (r->edge[2][i] + r->edge[3][i]);
+        return lam * d;
+    }
+    if (G->kind == 2) return lam * (fr - fl) / G->r;
+    return lam * (fr - fl);
+}
+
 /* SSPRK2 with HLLC (cudaFluidStep.cu:1510-1559 stage A, 1560-1600 stage B) */
-static void hllc_row_sweep(rowbuf *r, const fconst *c, int slope, double lambda)
+static void hllc_row_sweep(rowbuf *r, const fconst *c, int slope, double lambda, const rowgeo *G)
 {
     int n = r->n, i, k;
+    double lam = lambda;
+    if (G->kind == 3) lam /= G->r;
     hllc_row_flux(r, r->u, c, slope);
     for (k = 0; k < 5; k++)
         for (i = 0; i < n; i++)
-            r->tmp[k][i] = r->u[k][i] - lambda * (r->flux[k][i] - r->flux[k][wrap(i - 1, n)]);
+            r->tmp[k][i] = r->u[k][i] - hllc_dflux(r, G, lam, k, i);
     hllc_row_flux(r, r->tmp, c, slope);
     for (k = 0; k < 5; k++)
         for (i = 0; i < n; i++)
-            r->u[k][i] = .5 * (r->tmp[k][i] + r->u[k][i] -
-                               lambda * (r->flux[k][i] - r->flux[k][wrap(i - 1, n)]));
+            r->u[k][i] = .5 * (r->tmp[k][i] + r->u[k][i] - hllc_dflux(r, G, lam, k, i));
 }
 
 /* ------------------------------------------------------------------------------------------
@@ -503,29 +548,56 @@ static void hll_row_flux(rowbuf *r, double *const in[5], const double *P, const 
     }
 }
 
+/* The flux difference of cell i, component k, after hll_row_flux, as the HLL kernel subtracts
+ * it.  Radial sweeps take the radius factors with lambda folded in (cudaFluidStep.cu:1837-1842)
+ * and add the geometric pressure term to the radial momentum: the stage input's pressure from
+ * the pressure solver, or for an isothermal fluid rho c^2 with rho the density of the predicted
+ * state (Qstore[0], which the predictor has just written; 2270-2290, 2371-2391).  Theta sweeps
+ * divide by r or use lambda / r (2293-2305, 2255-2268). */
+static double hll_dflux(const rowbuf *r, const rowgeo *G, const fconst *c, double lam, const double *P,
+                        double *const U1[5], int k, int i)
+{
+    const int il = wrap(i - 1, r->n);
+    const double fr = r->flux[k][i], fl = r->flux[k][il];
+    if (G->kind == 1) {
+        double Fa = G->rin + i * G->dr;
+        double cA = lam * (Fa - .5 * G->dr) / (Fa);
+        double cB = lam * (Fa + .5 * G->dr) / (Fa);
+        double cC = lam * G->dr / Fa;
+        double d = cB * fr - cA * fl;
+        if (k == 2) {
+            if (c->isotemp == -1) d = d - P[i] * cC;
+            else d = d - U1[0][i] * c->isotempsq * cC;
+        }
+        return d;
+    }
+    if (G->kind == 2) return lam * (fr - fl) / G->r;
+    return lam * (fr - fl);
+}
+
 static void hll_row_sweep(rowbuf *r, const fconst *c, int slope, double lambda,
-                          const int mom_order[3])
+                          const int mom_order[3], const rowgeo *G)
 {
     int n = r->n, i, k;
-    double *P = r->tmp[0];  /* reuse: the pressure row is consumed before tmp is written */
     double *Pcopy = (double *)malloc(sizeof(double) * (size_t)n);
     double *U1[5];
     double *blk = (double *)malloc(sizeof(double) * (size_t)n * 5);
+    double lam = lambda;
+    if (G->kind == 3) lam /= G->r;
     for (k = 0; k < 5; k++) U1[k] = blk + (size_t)n * k;
-    (void)P;
-    /* pressure + floors on the fluid, predictor (PCswitch RK_PREDICT, SSPRK) */
+    /* pressure + floors on the fluid, predictor (PCswitch RK_PREDICT, SSPRK); the density
+     * (k = 0) is written first, as the isothermal radial term reads it */
     hll_pressure_row(r->u, Pcopy, n, c, mom_order);
     hll_row_flux(r, r->u, Pcopy, c, slope);
     for (k = 0; k < 5; k++)
         for (i = 0; i < n; i++)
-            U1[k][i] = r->u[k][i] - lambda * (r->flux[k][i] - r->flux[k][wrap(i - 1, n)]);
+            U1[k][i] = r->u[k][i] - hll_dflux(r, G, c, lam, Pcopy, U1, k, i);
     /* pressure + floors on the predicted state, corrector */
     hll_pressure_row(U1, Pcopy, n, c, mom_order);
     hll_row_flux(r, U1, Pcopy, c, slope);
     for (k = 0; k < 5; k++)
         for (i = 0; i < n; i++)
-            r->u[k][i] = .5 * (r->u[k][i] + U1[k][i] -
-                               lambda * (r->flux[k][i] - r->flux[k][wrap(i - 1, n)]));
+            r->u[k][i] = .5 * (r->u[k][i] + U1[k][i] - hll_dflux(r, G, c, lam, Pcopy, U1, k, i));
     free(blk);
     free(Pcopy);
 }
@@ -559,7 +631,7 @@ static double xj_freeze(double *const s[5], int n, const fconst *c, const int me
 
 static void xj_stage(double *const Qin[5], double *const Qbase[5], double *const Qout[5],
                      int n, const fconst *c, double Cf, double lambda, int corrector,
-                     int nslot, int flim, rowbuf *r)
+                     int nslot, int flim, rowbuf *r, const rowgeo *G)
 {
     /* Qin: state the fluxes are built from; Qbase: state that is updated (corrector) */
     int i, k;
@@ -599,7 +671,20 @@ static void xj_stage(double *const Qin[5], double *const Qbase[5], double *const
         for (i = 0; i < n; i++) {
             int il = wrap(i - 1, n), ir = wrap(i + 1, n);
             double base = corrector ? Qbase[k][i] : Qin[k][i];
-            prop[k][i] = base - lambda * (R[i] - R[il] - L[ir] + L[i]);
+            if (G->kind == 1) {
+                /* radial: face radii, and 2 dr / r times the cell pressure on p_r, the 2
+                 * undoing the halved lambda (cudaFluidStep.cu:2463-2470, 2576-2581, 2603-2607) */
+                double Rc = G->rin + i * G->dr;
+                double cA = (Rc - .5 * G->dr) / (Rc);
+                double cB = (Rc + .5 * G->dr) / (Rc);
+                double cC = 2.0 * G->dr / Rc;
+                prop[k][i] = base - lambda * (cB * R[i] - cA * R[il] - cB * L[ir] + cA * L[i]);
+                if (k == 2) prop[k][i] += lambda * cC * P[i];
+            } else if (G->kind == 2) {
+                prop[k][i] = base - lambda * (R[i] - R[il] - L[ir] + L[i]) / G->r;
+            } else {
+                prop[k][i] = base - lambda * (R[i] - R[il] - L[ir] + L[i]);
+            }
         }
     }
     for (i = 0; i < n; i++) {
@@ -612,20 +697,25 @@ static void xj_stage(double *const Qin[5], double *const Qbase[5], double *const
     }
 }
 
-static void xj_row_sweep(rowbuf *r, const fconst *c, int flim, double lambda, int dir)
+static void xj_row_sweep(rowbuf *r, const fconst *c, int flim, double lambda, int dir, const rowgeo *G)
 {
-    /* r->u holds the row in memory slab order for XJ */
+    /* r->u holds the row in memory slab order for XJ; the theta form with lambda / r divides
+     * each stage's lambda (0.25 and 0.5 of the sweep's) by r (cudaFluidStep.cu:2478-2480) */
     int n = r->n, k;
     int mem[5] = {0, 1, 2, 3, 4};
     int nslot = 1 + dir;
     double *U1[5];
     double *blk = (double *)malloc(sizeof(double) * (size_t)n * 5);
-    double Cf;
+    double Cf, la = 0.25 * lambda, lb = 0.5 * lambda;
+    if (G->kind == 3) {
+        la /= G->r;
+        lb /= G->r;
+    }
     for (k = 0; k < 5; k++) U1[k] = blk + (size_t)n * k;
     Cf = xj_freeze(r->u, n, c, mem);
-    xj_stage(r->u, r->u, U1, n, c, Cf, 0.25 * lambda, 0, nslot, flim, r);
+    xj_stage(r->u, r->u, U1, n, c, Cf, la, 0, nslot, flim, r, G);
     Cf = xj_freeze(U1, n, c, mem);
-    xj_stage(U1, r->u, r->u, n, c, Cf, 0.5 * lambda, 1, nslot, flim, r);
+    xj_stage(U1, r->u, r->u, n, c, Cf, lb, 1, nslot, flim, r, G);
     free(blk);
 }
 
@@ -649,6 +739,39 @@ static long pencil_base(const or_grid *g, int dir, long p)
         return x + (long)g->nx * g->ny * z;
     }
     return p;  /* dir 3: pencils indexed by x + nx*y */
+}
+
+/* Geometry of pencil pp of a sweep along dir (see rowgeo).  Theta pencils: with
+ * OR_CYL_GEOMETRIC_RADIUS r = r_inner + i h[0] (i = radial index); otherwise the radius the
+ * reference's kernels compute, whose radial step is the sweep direction's cell size h[1]
+ * (gamHost[9], cudaFluidStep.cu:305-307, 340).  Layout theta,r,z: theta_radius_213 of the radial
+ * index, or of the z index when nx = 1 < nz (the launch then treats z as the second dimension,
+ * cudaFluidStep.cu:325-329).  Layout theta,z,r: i h[1] + r_inner from the block index, which is
+ * always 0 when nz = 1 (the same reshaping), so every such pencil gets r_inner. */
+static rowgeo pencil_rowgeo(const or_grid *g, const or_step *p, int dir, long pp)
+{
+    rowgeo G = ROWGEO_SQUARE;
+    if (p->geometry != OR_GEO_CYLINDRICAL || dir == 3) return G;
+    if (dir == 1) {
+        G.kind = 1;
+        G.rin = p->r_inner;
+        G.dr = p->h[0];
+        return G;
+    }
+    {
+        const int i = (int)(pp % g->nx), kz = (int)(pp / g->nx);
+        G.kind = (p->theta_form == OR_THETA_231) ? 3 : 2;
+        if (p->cyl_flags & OR_CYL_GEOMETRIC_RADIUS) G.r = p->r_inner + i * p->h[0];
+        else if (p->theta_form == OR_THETA_231) G.r = (g->nz == 1 ? 0 : i) * p->h[1] + p->r_inner;
+        else G.r = theta_radius_213((g->nx == 1 && g->nz > 1) ? kz : i, p->r_inner, p->h[1]);
+    }
+    return G;
+}
+
+int or_theta_form(int sweep_dir, int step_number)
+{
+    const int sweep = (step_number + 3 * (sweep_dir > 0)) % 6;
+    return (sweep == 0 || sweep == 5) ? OR_THETA_231 : OR_THETA_213;
 }
 
 int or_fluid_sweep(double *q, const or_grid *g, const or_step *p, int dir)
@@ -692,9 +815,10 @@ int or_fluid_sweep(double *q, const or_grid *g, const or_step *p, int dir)
                 const double *s = q + (long)map[k] * g->slab + b;
                 for (i = 0; i < n; i++) r.u[k][i] = s[(long)i * stride];
             }
-            if (p->method == 2) hllc_row_sweep(&r, &c, p->slope_limiter, lambda);
-            else if (p->method == 1) hll_row_sweep(&r, &c, p->slope_limiter, lambda, mom_order);
-            else xj_row_sweep(&r, &c, p->flux_limiter, lambda, dir);
+            rowgeo G = pencil_rowgeo(g, p, dir, pp);
+            if (p->method == 2) hllc_row_sweep(&r, &c, p->slope_limiter, lambda, &G);
+            else if (p->method == 1) hll_row_sweep(&r, &c, p->slope_limiter, lambda, mom_order, &G);
+            else xj_row_sweep(&r, &c, p->flux_limiter, lambda, dir, &G);
             for (k = 0; k < 5; k++) {
                 double *s = q + (long)map[k] * g->slab + b;
                 for (i = 0; i < n; i++) s[(long)i * stride] = r.u[k][i];
@@ -831,13 +955,16 @@ int or_fluid_boundary(double *q, const or_grid *g, const int32_t bc[6], int dir,
 /* ------------------------------------------------------------------------------------------
  * performFluidUpdate_3D (flux.cu:27-165)
  * ---------------------------------------------------------------------------------------- */
-int or_fluid_step_3d(double *q, const or_grid *g, const or_step *p, const int32_t bc[6],
+int or_fluid_step_3d(double *q, const or_grid *g, const or_step *p0, const int32_t bc[6],
                      int sweep_dir, int step_number)
 {
     static const int fluxcall[3][6] = {{1, 2, 1, 2, 3, 3}, {3, 1, 2, 3, 1, 2}, {2, 3, 3, 1, 2, 1}};
     int sweep = (step_number + 3 * (sweep_dir > 0)) % 6;
     int nstep, rc;
     int ext[3];
+    or_step pst = *p0;
+    const or_step *p = &pst;
+    pst.theta_form = or_theta_form(sweep_dir, step_number);
     ext[0] = g->nx; ext[1] = g->ny; ext[2] = g->nz;
     if (g->ny == 1 && g->nz == 1) {
         rc = or_fluid_sweep(q, g, p, 1);
@@ -877,6 +1004,12 @@ void or_soundspeed(const double *q, const or_grid *g, double gamma, double *cs)
 double or_cfl_timestep(const double *q, const double *cs, const or_grid *g, const double h[3],
                        const int32_t global_rez[3], int method)
 {
+    return or_cfl_timestep_geo(q, cs, g, h, global_rez, method, OR_GEO_SQUARE, 0.0);
+}
+
+double or_cfl_timestep_geo(const double *q, const double *cs, const or_grid *g, const double h[3],
+                           const int32_t global_rez[3], int method, int geometry, double r_inner)
+{
     long N = (long)g->nx * g->ny * g->nz, x;
     int spacedim = 0, sim;
     int algo_xj;
@@ -889,8 +1022,13 @@ double or_cfl_timestep(const double *q, const double *cs, const or_grid *g, cons
     /* ctype table (cflTimestep.cu:175-193): 1-D Xin-Jin uses the HLL/HLLC kernel */
     algo_xj = (method == 3) && (sim > 1);
     hmin = h[0];
-    if (sim > 1 && h[1] < hmin) hmin = h[1];
-    if (sim > 2 && h[2] < hmin) hmin = h[2];
+    if (geometry == OR_GEO_CYLINDRICAL) {
+        /* dr, and dz in 3-D; the theta extent is taken per cell (cflTimestep.cu:301-304) */
+        if (sim == 3) hmin = (hmin < h[2]) ? hmin : h[2];
+    } else {
+        if (sim > 1 && h[1] < hmin) hmin = h[1];
+        if (sim > 2 && h[2] < hmin) hmin = h[2];
+    }
 #pragma omp parallel for reduction(min : tmin) schedule(static)
     for (x = 0; x < N; x++) {
         double u, v;
@@ -910,11 +1048,21 @@ double or_cfl_timestep(const double *q, const double *cs, const or_grid *g, cons
                 p = sqrt(pp);
             }
             u = p / rho[x] + cs[x];
-            u = hmin / u;
+            if (geometry == OR_GEO_CYLINDRICAL) {
+                /* r dtheta of this cell's radius (cflTimestep.cu:316-320) */
+                double w = (r_inner + (x % g->nx) * h[0]) * h[1];
+                w = (w < hmin) ? w : hmin;
+                u = w / u;
+            } else {
+                u = hmin / u;
+            }
         } else {
             double r = rho[x];
             u = h[0] / (fabs(px[x]) / r + cs[x]);
-            v = h[1] / (fabs(py[x]) / r + cs[x]);
+            if (geometry == OR_GEO_CYLINDRICAL)
+                v = (r_inner + (x % g->nx) * h[0]) * h[1] / (fabs(py[x]) / r + cs[x]);
+            else
+                v = h[1] / (fabs(py[x]) / r + cs[x]);
             u = (u < v) ? u : v;
             if (sim > 2) {
                 v = h[2] / (fabs(pz[x]) / r + cs[x]);
@@ -926,6 +1074,62 @@ double or_cfl_timestep(const double *q, const double *cs, const or_grid *g, cons
     if (tmin > 1e37) tmin = 1e37;  /* per-thread initial value in the kernel */
     if (method == 1 || method == 2) tmin = tmin / 2;
     return tmin;
+}
+
+/* ------------------------------------------------------------------------------------------
+ * Cylindrical geometric source terms (cukern_SourceCylindricalTerms,
+ * cudaSourceCylindricalTerms.cu:119-222).  Per cell: v_r' = v_theta^2 / r, v_theta' = -v_r
+ * v_theta / r over dt by the two-stage Gauss-Legendre collocation method (the Butcher table of
+ * the fourth-order Gauss-Legendre method, with the reference's own decimal constants) and two
+ * fixed-point passes.  The stage updates are restated as the reference writes them, including
+ * the sign of the second stage's term in the first v_theta update and the second v_theta
+ * update's use of the old v_r of stage B in both terms; the kinetic-energy change goes into
+ * internal energy except that a non-positive pressure is reset.  Runs on the XYZ layout.
+ * ---------------------------------------------------------------------------------------- */
+#define GL4_A11 .25
+#define GL4_A12 -0.038675134594812865529
+#define GL4_A21 0.53867513459481286553
+#define GL4_A22 .25
+
+void or_cyl_source(double *q, const or_grid *g, double dt, double dr, double r_inner)
+{
+    const long nx = g->nx, N = (long)g->nx * g->ny * g->nz;
+    const long S = g->slab;
+    long x;
+#pragma omp parallel for schedule(static)
+    for (x = 0; x < N; x++) {
+        double *base = q + x;
+        double r = r_inner + (int)(x % nx) * dr;
+        double rho, u, v, w, E, newP, vrA, vphiA, vrB, vphiB, diffmom, diffmomB, scratch;
+        int it;
+        rho = base[0];
+        u = base[2 * S] / rho;
+        v = base[3 * S] / rho;
+        diffmom = dt * v / r;
+        vrA = u + GL4_A11 * v * diffmom;
+        vphiA = v - GL4_A11 * u * diffmom;
+        vrB = u + GL4_A12 * v * diffmom;
+        vphiB = v - GL4_A12 * u * diffmom;
+        for (it = 0; it < 2; it++) {
+            diffmom = dt * vphiA / r;
+            diffmomB = dt * vphiB / r;
+            scratch = vrA;
+            vrA = u + GL4_A11 * vphiA * diffmom + GL4_A12 * vphiB * diffmomB;
+            vphiA = v - GL4_A11 * scratch * diffmom + GL4_A12 * vrB * diffmomB;
+            diffmom = dt * vphiA / r;
+            scratch = vrB;
+            vrB = u + GL4_A21 * vphiA * diffmom + GL4_A22 * vphiB * diffmomB;
+            vphiB = v - GL4_A21 * scratch * diffmom + GL4_A22 * scratch * diffmomB;
+        }
+        u = rho * (u + .5 * dt * (vphiA * vphiA + vphiB * vphiB) / r);
+        v = rho * (v - .5 * dt * (vphiA * vrA + vphiB * vrB) / r);
+        E = base[S];
+        w = base[4 * S];
+        newP = E - .5 * (u * u + v * v + w * w) / rho;
+        if (newP <= 0.0) base[S] = .5 * (u * u + v * v + w * w) / rho + .00001 * rho;
+        base[2 * S] = u;
+        base[3 * S] = v;
+    }
 }
 
 /* ------------------------------------------------------------------------------------------

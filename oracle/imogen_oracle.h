@@ -38,8 +38,20 @@ typedef struct {
     int32_t method;        /* 1 HLL, 2 HLLC, 3 Xin-Jin */
     int32_t slope_limiter; /* OR_SLOPE_* (HLL / HLLC reconstruction) */
     int32_t flux_limiter;  /* OR_FLUX_*  (Xin-Jin TVD correction) */
-    int32_t pad_;
+    int32_t geometry;      /* OR_GEO_SQUARE or OR_GEO_CYLINDRICAL (x = r, y = theta, z = z) */
+    double r_inner;        /* cylindrical: radius of the centre of radial cell 0 (pInnerRadius) */
+    int32_t theta_form;    /* cylindrical theta sweeps: OR_THETA_213 or OR_THETA_231 */
+    int32_t cyl_flags;     /* OR_CYL_GEOMETRIC_RADIUS: theta sweeps take r = r_inner + i*h[0] */
 } or_step;
+
+enum { OR_GEO_SQUARE = 0, OR_GEO_CYLINDRICAL = 1 };
+/* The reference permutes memory so that the swept direction is fastest; for a theta sweep the
+ * radial direction is then either the second (layout theta,r,z: FLUX_THETA_213, the flux
+ * difference is divided by r) or the third (theta,z,r: FLUX_THETA_231, lambda is divided by r
+ * first), which rounds differently (cudaFluidStep.cu:264-278, 848-855, 1085-1106).  Which one a
+ * sweep of a fluid step gets follows from the sweep index (or_theta_form). */
+enum { OR_THETA_213 = 0, OR_THETA_231 = 1 };
+enum { OR_CYL_GEOMETRIC_RADIUS = 1 };
 
 enum { OR_SLOPE_OSPRE = 0, OR_SLOPE_MC = 1, OR_SLOPE_VANLEER = 2, OR_SLOPE_MINMOD = 3,
        OR_SLOPE_SUPERBEE = 4, OR_SLOPE_VANALBADA = 5, OR_SLOPE_ZERO = 6 };
@@ -72,6 +84,21 @@ void or_soundspeed(const double *q, const or_grid *g, double gamma, double *cs);
  * global_rez gives the dimensionality, h the cell sizes. */
 double or_cfl_timestep(const double *q, const double *cs, const or_grid *g, const double h[3],
                        const int32_t global_rez[3], int method);
+
+/* The same in cylindrical geometry (geometry = OR_GEO_CYLINDRICAL): the theta extent of a cell
+ * is (r_inner + i h[0]) h[1] for radial index i (cflTimestep.cu:301-333). */
+double or_cfl_timestep_geo(const double *q, const double *cs, const or_grid *g, const double h[3],
+                           const int32_t global_rez[3], int method, int geometry, double r_inner);
+
+/* Geometric source terms of cylindrical coordinates over dt (cukern_SourceCylindricalTerms,
+ * cudaSourceCylindricalTerms.cu:119-222): the centrifugal and Coriolis exchange between p_r and
+ * p_theta, integrated by a two-stage Gauss-Legendre step with two fixed-point iterations, with
+ * the reference's stage arithmetic as written; dr = h[0]. */
+void or_cyl_source(double *q, const or_grid *g, double dt, double dr, double r_inner);
+
+/* The theta form a theta sweep of a fluid step gets (sweep index (step_number + 3 [sweep_dir >
+ * 0]) mod 6, flux.cu:46-49, through the permutations of cudaArrayRotateB.cu:580-643). */
+int or_theta_form(int sweep_dir, int step_number);
 
 /* freezeAndPtot hydro (freezeAndPtot.cu:32-147, 229-290): writes Ptot[N], freeze[ny*nz]
  * and floors E in place where c_s < cs_min. */

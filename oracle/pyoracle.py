@@ -30,7 +30,13 @@ class Step(ctypes.Structure):
     _fields_ = [("dt", ctypes.c_double), ("h", ctypes.c_double * 3), ("gamma", ctypes.c_double),
                 ("rho_min", ctypes.c_double), ("c_iso", ctypes.c_double),
                 ("method", ctypes.c_int32), ("slope_limiter", ctypes.c_int32),
-                ("flux_limiter", ctypes.c_int32), ("pad_", ctypes.c_int32)]
+                ("flux_limiter", ctypes.c_int32), ("geometry", ctypes.c_int32),
+                ("r_inner", ctypes.c_double), ("theta_form", ctypes.c_int32),
+                ("cyl_flags", ctypes.c_int32)]
+
+GEO_SQUARE, GEO_CYLINDRICAL = 0, 1
+THETA_213, THETA_231 = 0, 1
+CYL_GEOMETRIC_RADIUS = 1
 
 
 def build():
@@ -54,6 +60,14 @@ def lib():
         L.or_cfl_timestep.argtypes = [dp, dp, ctypes.POINTER(Grid), dp,
                                       ctypes.POINTER(ctypes.c_int32), ctypes.c_int]
         L.or_cfl_timestep.restype = ctypes.c_double
+        L.or_cfl_timestep_geo.argtypes = [dp, dp, ctypes.POINTER(Grid), dp,
+                                          ctypes.POINTER(ctypes.c_int32), ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_double]
+        L.or_cfl_timestep_geo.restype = ctypes.c_double
+        L.or_cyl_source.argtypes = [dp, ctypes.POINTER(Grid), ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double]
+        L.or_theta_form.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.or_theta_form.restype = ctypes.c_int
         L.or_freeze_and_ptot.argtypes = [dp, ctypes.POINTER(Grid), ctypes.c_double,
                                          ctypes.c_double, dp, dp]
         L.or_array_boundary.argtypes = [dp, ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int,
@@ -78,9 +92,11 @@ def grid(shape, slab=None):
     return Grid(nx, ny, nz, 0, slab if slab is not None else nx * ny * nz)
 
 
-def step_params(dt, h, gamma, rho_min=1e-5, c_iso=-1.0, method=2, slope="ospre", fluxlim="ospre"):
+def step_params(dt, h, gamma, rho_min=1e-5, c_iso=-1.0, method=2, slope="ospre", fluxlim="ospre",
+                cylindrical=False, r_inner=0.0, theta_form=THETA_213, geometric_radius=False):
     return Step(dt, (ctypes.c_double * 3)(*h), gamma, rho_min, c_iso, method,
-                SLOPE[slope], FLUXLIM[fluxlim], 0)
+                SLOPE[slope], FLUXLIM[fluxlim], GEO_CYLINDRICAL if cylindrical else GEO_SQUARE,
+                r_inner, theta_form, CYL_GEOMETRIC_RADIUS if geometric_radius else 0)
 
 
 def _bcarr(bc):
@@ -117,13 +133,24 @@ def soundspeed(q, shape, gamma):
     return cs
 
 
-def cfl_timestep(q, shape, gamma, h, method, cs=None):
+def cfl_timestep(q, shape, gamma, h, method, cs=None, cylindrical=False, r_inner=0.0):
     if cs is None:
         cs = soundspeed(q, shape, gamma)
     g = grid(shape, q.shape[1])
     hh = np.ascontiguousarray(h, dtype=np.float64)
     rez = (ctypes.c_int32 * 3)(*shape)
-    return lib().or_cfl_timestep(_p(q), _p(cs), ctypes.byref(g), _p(hh), rez, method)
+    return lib().or_cfl_timestep_geo(_p(q), _p(cs), ctypes.byref(g), _p(hh), rez, method,
+                                     GEO_CYLINDRICAL if cylindrical else GEO_SQUARE, r_inner)
+
+
+def cyl_source(q, shape, dt, dr, r_inner):
+    """Cylindrical geometric source terms over dt, in place."""
+    g = grid(shape, q.shape[1])
+    lib().or_cyl_source(_p(q), ctypes.byref(g), dt, dr, r_inner)
+
+
+def theta_form(sweep_dir, step_number):
+    return lib().or_theta_form(sweep_dir, step_number)
 
 
 def freeze_and_ptot(q, shape, gamma, cs_min):

@@ -23,6 +23,7 @@
 #include "cudaSoundspeed.h"
 #include "cudaSource2FluidDrag.h"
 #include "cudaStatics.h"
+#include "cudaSourceCylindricalTerms.h"
 
 // One rank: the reference's halo exchange returns at once when its topology has a single rank
 // in the exchange direction (cudaHaloExchange.cu:157-158); its source pulls in HDF5, so this
@@ -331,6 +332,134 @@ int ref_time(double *hq, int nx, int ny, int nz, int64_t hslab, double gamma, in
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     *ms_out = ms;
+    MGA_delete(&holder);
+    return rc;
+}
+
+// ---- cylindrical geometry (x = r, y = theta, z = z) ----
+
+static GeometryParams make_cyl_geometry(int nx, int ny, int nz, const double h[3], double r_inner)
+{
+    GeometryParams g = make_geometry(nx, ny, nz, h);
+    g.shape = CYLINDRICAL;
+    g.Rinner = r_inner;
+    return g;
+}
+
+// One cylindrical sweep along dir with the reference's performFluidUpdate_1D.  A theta sweep
+// (dir 2) runs on the array permuted so that theta is fastest: form 0 = layout theta,r,z
+// (exchange X and Y, code 2), form 1 = theta,z,r (rotate left, code 5); the array is permuted
+// back afterwards.  No boundary fill.
+int ref_sweep_cyl(double *hq, int nx, int ny, int nz, int64_t hslab, double gamma, double rho_min, double c_iso,
+                  int method, const double *h, double r_inner, int dir, int form, double dt)
+{
+    MGArray holder, fl[5];
+    const int bc[6] = {0, 0, 0, 0, 0, 0};
+    int rc = make_fluid(&holder, fl, nx, ny, nz, bc, 4);
+    if (rc != SUCCESSFUL) return rc;
+    const int64_t n = (int64_t)nx * ny * nz;
+    upload(&holder, hq, hslab, n);
+    ParallelTopology topo;
+    make_topology(&topo);
+    cudaStream_t *streams = &topo.cudaStreamPtrs[0];
+    FluidStepParams fsp;
+    memset(&fsp, 0, sizeof(fsp));
+    fsp.onlyHydro = 1;
+    fsp.thermoGamma = (c_iso != -1) ? 2.0 : gamma;
+    fsp.Cisothermal = c_iso;
+    fsp.minimumRho = rho_min;
+    fsp.stepMethod = to_method(method);
+    fsp.geometry = make_cyl_geometry(nx, ny, nz, h, r_inner);
+    fsp.dt = dt;
+    fsp.stepDirection = dir;
+    const int pre = (dir == 2) ? (form == 0 ? 2 : 5) : 0;
+    const int post = (dir == 2) ? (form == 0 ? 2 : 6) : 0;
+    if (pre) rc = flipArrayIndices(&fl[0], (MGArray **)NULL, 5, pre, streams, (MGArray *)NULL);
+    if (rc == SUCCESSFUL) rc = performFluidUpdate_1D(&fl[0], fsp, &topo, (MGArray *)NULL);
+    if (rc == SUCCESSFUL && post) rc = flipArrayIndices(&fl[0], (MGArray **)NULL, 5, post, streams, (MGArray *)NULL);
+    cudaDeviceSynchronize();
+    download(&holder, hq, hslab, n);
+    MGA_delete(&holder);
+    return rc;
+}
+
+// The cylindrical source over dt on an XYZ-ordered fluid (sourcefunction_CylindricalTerms)
+int ref_cyl_source(double *hq, int nx, int ny, int nz, int64_t hslab, const double *h, double r_inner, double dt)
+{
+    MGArray holder, fl[5];
+    const int bc[6] = {0, 0, 0, 0, 0, 0};
+    int rc = make_fluid(&holder, fl, nx, ny, nz, bc, 4);
+    if (rc != SUCCESSFUL) return rc;
+    const int64_t n = (int64_t)nx * ny * nz;
+    upload(&holder, hq, hslab, n);
+    double hh[3] = {h[0], h[1], h[2]};
+    rc = sourcefunction_CylindricalTerms(&fl[0], dt, &hh[0], r_inner);
+    cudaDeviceSynchronize();
+    download(&holder, hq, hslab, n);
+    MGA_delete(&holder);
+    return rc;
+}
+
+// CFL timestep in cylindrical geometry
+int ref_cfl_cyl(const double *hq, int nx, int ny, int nz, int64_t hslab, double gamma, int method, const double *h,
+                double r_inner, double *tau_out)
+{
+    MGArray holder, fl[5];
+    const int bc[6] = {0, 0, 0, 0, 0, 0};
+    int rc = make_fluid(&holder, fl, nx, ny, nz, bc, 4);
+    if (rc != SUCCESSFUL) return rc;
+    upload(&holder, hq, hslab, (int64_t)nx * ny * nz);
+    GeometryParams geo = make_cyl_geometry(nx, ny, nz, h, r_inner);
+    rc = cfl_tau(fl, &geo, gamma, method, tau_out);
+    MGA_delete(&holder);
+    return rc;
+}
+
+// One-fluid main loop in cylindrical geometry, as performCompleteTimestep runs it with the
+// cylinder-only source (srcType 1, flux_multi.cu:161-250; srcC___, sourceStep.cu:498-518):
+// CFL, source dt/2, forward step, source dt, backward step, source dt/2, each source followed by
+// the boundary fill of directions 1, 2, 3 (setAllBoundaryConditions, sourceStep.cu:276-291).
+int ref_run_cyl(double *hq, int nx, int ny, int nz, int64_t hslab, double gamma, double rho_min, double c_iso,
+                int method, const double *h, double r_inner, const int *bc, double cfl, int niter, double *dts_out)
+{
+    MGArray holder, fl[5];
+    int rc = make_fluid(&holder, fl, nx, ny, nz, bc, 4);
+    if (rc != SUCCESSFUL) return rc;
+    const int64_t n = (int64_t)nx * ny * nz;
+    upload(&holder, hq, hslab, n);
+    ParallelTopology topo;
+    make_topology(&topo);
+    GeometryParams geo = make_cyl_geometry(nx, ny, nz, h, r_inner);
+    FluidStepParams fsp;
+    memset(&fsp, 0, sizeof(fsp));
+    fsp.onlyHydro = 1;
+    fsp.thermoGamma = (c_iso != -1) ? 2.0 : gamma;
+    fsp.Cisothermal = c_iso;
+    fsp.minimumRho = rho_min;
+    fsp.stepMethod = to_method(method);
+    fsp.geometry = geo;
+    auto source = [&](double dt) {
+        int r = sourcefunction_CylindricalTerms(&fl[0], dt, &geo.h[0], geo.Rinner);
+        for (int d = 1; d <= 3 && r == SUCCESSFUL; d++) r = setFluidBoundary(&fl[0], &geo, d);
+        return r;
+    };
+    for (int it = 0; it < niter && rc == SUCCESSFUL; it++) {
+        double tau = 0;
+        rc = cfl_tau(fl, &geo, gamma, method, &tau);
+        if (rc != SUCCESSFUL) break;
+        fsp.dt = cfl * tau;
+        fsp.stepNumber = it;
+        dts_out[it] = fsp.dt;
+        rc = source(0.5 * fsp.dt);
+        fsp.stepDirection = 1;
+        if (rc == SUCCESSFUL) rc = fluid_update_3d(&fl[0], &topo, fsp);
+        if (rc == SUCCESSFUL) rc = source(fsp.dt);
+        fsp.stepDirection = -1;
+        if (rc == SUCCESSFUL) rc = fluid_update_3d(&fl[0], &topo, fsp);
+        if (rc == SUCCESSFUL) rc = source(0.5 * fsp.dt);
+    }
+    cudaDeviceSynchronize();
+    download(&holder, hq, hslab, n);
     MGA_delete(&holder);
     return rc;
 }

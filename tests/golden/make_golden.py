@@ -14,7 +14,7 @@ Boundary conditions are limited to circular, const and mirror: the reference's o
 extrapolation kernels write outside their rows (cudaStatics.cu / boundaryConds.cu), so they are not
 run here.
 
-Usage: python tests/golden/make_golden.py OUTDIR [--etdrk2-only | --cases=name1,name2]
+Usage: python tests/golden/make_golden.py OUTDIR [--etdrk2-only | --cyl-only | --cases=name1,name2]
 """
 import ctypes
 import json
@@ -230,8 +230,104 @@ def main(outdir, only=None, cases=None):
         json.dump(index, f, indent=1)
 
 
+# ---- cylindrical geometry (x = r, y = theta, z = z) ----
+CYL_H = [0.05, 0.04, 0.1]   # dr, dtheta, dz: dtheta != dr shows which spacing the theta sweeps use
+CYL_RIN = 1.0
+# single sweeps: name, shape, method, c_iso; each along r (dir 1) and theta in both layouts
+CYL_SWEEP_CASES = [
+    ("hllc3d", (32, 32, 6), 2, -1.0),
+    ("hll3d", (32, 32, 6), 1, -1.0),
+    ("xj3d", (32, 32, 6), 3, -1.0),
+    ("hllc2d", (32, 24, 1), 2, -1.0),
+    ("hll2d", (32, 24, 1), 1, -1.0),
+    ("hlliso2d", (32, 24, 1), 1, 0.8),
+]
+CYL_SWEEPS = [(1, 0), (2, 0), (2, 1)]   # (dir, theta layout 0 = theta,r,z / 1 = theta,z,r)
+# main loops with the cylinder source: name, shape, method, gamma, c_iso, bc, cfl, niter.  Xin-Jin
+# runs at extents its launch covers (32; the z extent 3 is not swept), and never on a 2-D grid,
+# where its theta sweep in the theta,z,r layout indexes outside its arrays.
+CYL_RUN_CASES = [
+    ("cyl_hllc_3d", (24, 20, 6), 2, 1.4, -1.0, ["const", "const"] + ["circular"] * 4, 0.4, 6),
+    ("cyl_hll_2d", (24, 32, 1), 1, 1.4, -1.0, ["const", "const"] + ["circular"] * 4, 0.4, 6),
+    ("cyl_hllc_2d", (24, 32, 1), 2, 5 / 3.0, -1.0, ["mirror", "const"] + ["circular"] * 4, 0.4, 6),
+    ("cyl_hlliso_2d", (24, 32, 1), 1, 1.4, 0.8, ["const", "const"] + ["circular"] * 4, 0.4, 6),
+    ("cyl_xj_3d", (32, 32, 3), 3, 1.4, -1.0, ["const", "const"] + ["circular"] * 4, 0.3, 6),
+]
+
+
+def cyl_lib(strict):
+    L = lib("ospre", strict)
+    dp = ctypes.POINTER(ctypes.c_double)
+    i64, dbl, cint = ctypes.c_int64, ctypes.c_double, ctypes.c_int
+    L.ref_sweep_cyl.argtypes = [dp, cint, cint, cint, i64, dbl, dbl, dbl, cint, dp, dbl, cint, cint, dbl]
+    L.ref_cyl_source.argtypes = [dp, cint, cint, cint, i64, dp, dbl, dbl]
+    L.ref_cfl_cyl.argtypes = [dp, cint, cint, cint, i64, dbl, cint, dp, dbl, dp]
+    L.ref_run_cyl.argtypes = [dp, cint, cint, cint, i64, dbl, dbl, dbl, cint, dp, dbl,
+                              ctypes.POINTER(ctypes.c_int), dbl, cint, dp]
+    return L
+
+
+def cyl_golden(outdir):
+    h = np.array(CYL_H)
+    rec, meta = {}, {"h": CYL_H, "r_inner": CYL_RIN, "sweeps": [], "runs": [], "dt": 0.004}
+    for name, shape, method, c_iso in CYL_SWEEP_CASES:
+        q0 = problems.rotating_annulus(shape, r_inner=CYL_RIN, dr=CYL_H[0], seed=37)
+        rec["in_" + name] = q0
+        for d, form in CYL_SWEEPS:
+            for strict in (False, True):
+                q = q0.copy()
+                rc = cyl_lib(strict).ref_sweep_cyl(P(q), shape[0], shape[1], shape[2], q.shape[1], 1.4, 1e-5, c_iso,
+                                                   method, P(h), CYL_RIN, d, form, 0.004)
+                assert rc == 0, (name, d, form, rc)
+                rec["out_%s_d%d_f%d_%s" % (name, d, form, "strict" if strict else "fast")] = q
+        meta["sweeps"].append(dict(name=name, shape=list(shape), method=method, c_iso=c_iso))
+        print("wrote cyl sweeps", name, flush=True)
+    # CFL and the source term on one state; a cold copy makes the source's pressure reset act
+    q0 = problems.rotating_annulus((24, 20, 6), r_inner=CYL_RIN, dr=CYL_H[0], seed=41)
+    cold = q0.copy()
+    n = 24 * 20 * 6
+    cold[1, :n] = 0.5 * (cold[2, :n] ** 2 + cold[3, :n] ** 2 + cold[4, :n] ** 2) / cold[0, :n] + 1e-7
+    rec["src_in"], rec["src_cold_in"] = q0, cold
+    for strict in (False, True):
+        tag = "strict" if strict else "fast"
+        for key, src in (("src", q0), ("src_cold", cold)):
+            q = src.copy()
+            assert cyl_lib(strict).ref_cyl_source(P(q), 24, 20, 6, q.shape[1], P(h), CYL_RIN, 0.05) == 0
+            rec["%s_out_%s" % (key, tag)] = q
+        for shape in ((24, 20, 6), (24, 20, 1), (24, 1, 1)):
+            qs = problems.rotating_annulus(shape, r_inner=CYL_RIN, dr=CYL_H[0], seed=43)
+            rec["cfl_in_%dx%dx%d" % shape] = qs
+            for method in (1, 2, 3):
+                t = ctypes.c_double(0)
+                assert cyl_lib(strict).ref_cfl_cyl(P(qs), shape[0], shape[1], shape[2], qs.shape[1], 1.4, method,
+                                                   P(h), CYL_RIN, ctypes.byref(t)) == 0
+                rec["cfl_%dx%dx%d_m%d_%s" % (shape + (method, tag))] = np.array(t.value)
+    print("wrote cyl source and cfl", flush=True)
+    for name, shape, method, gamma, c_iso, bc, cfl, niter in CYL_RUN_CASES:
+        q0 = problems.rotating_annulus(shape, r_inner=CYL_RIN, dr=CYL_H[0], gamma=gamma, seed=47)
+        rec["run_in_" + name] = q0
+        bca = (ctypes.c_int * 6)(*[BC[b] for b in bc])
+        for strict in (False, True):
+            q = q0.copy()
+            dts = np.zeros(niter)
+            rc = cyl_lib(strict).ref_run_cyl(P(q), shape[0], shape[1], shape[2], q.shape[1], gamma, 1e-5, c_iso,
+                                             method, P(h), CYL_RIN, bca, cfl, niter, P(dts))
+            assert rc == 0, (name, rc)
+            tag = "strict" if strict else "fast"
+            rec["run_out_%s_%s" % (name, tag)] = q
+            rec["run_dts_%s_%s" % (name, tag)] = dts
+        meta["runs"].append(dict(name=name, shape=list(shape), method=method, gamma=gamma, c_iso=c_iso, bc=bc,
+                                 cfl=cfl, niter=niter))
+        print("wrote cyl run", name, flush=True)
+    np.savez_compressed(os.path.join(outdir, "cylindrical.npz"), meta=json.dumps(meta), **rec)
+
+
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     sel = [a.split("=", 1)[1].split(",") for a in sys.argv[1:] if a.startswith("--cases=")]
-    main(args[0] if args else os.path.dirname(os.path.abspath(__file__)),
-         only="etdrk2" if "--etdrk2-only" in sys.argv else None, cases=sel[0] if sel else None)
+    out = args[0] if args else os.path.dirname(os.path.abspath(__file__))
+    if "--cyl-only" in sys.argv:
+        os.makedirs(out, exist_ok=True)
+        cyl_golden(out)
+    else:
+        main(out, only="etdrk2" if "--etdrk2-only" in sys.argv else None, cases=sel[0] if sel else None)

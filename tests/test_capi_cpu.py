@@ -63,12 +63,20 @@ def test_invalid_calls_rejected_without_device():
     for bad in ((1e-3, 1, 1.4, 1e-5, 4, 1), (1e-3, 1, 1.4, 1e-5, 2, 4)):
         pb = (ctypes.c_double * 6)(*bad)
         assert L.ib_cudaFluidStep(ctypes.byref(f), ctypes.byref(geo), pb, 6, None, None) == -100
-    # MHD and cylindrical are not built
+    # MHD and shapes other than square and cylindrical are not built
     pm = (ctypes.c_double * 6)(1e-3, 0, 1.4, 1e-5, 2, 1)
     assert L.ib_cudaFluidStep(ctypes.byref(f), ctypes.byref(geo), pm, 6, None, None) == -105
     geo2 = imogen.IbGeometry()
-    geo2.shape = 1
+    geo2.shape = 2
     assert L.ib_cudaFluidStep(ctypes.byref(f), ctypes.byref(geo2), p, 6, None, None) == -105
+    # cylindrical: the theta layout parameter is 0 or 1; unknown numerics flags are rejected
+    geo3 = imogen.IbGeometry()
+    geo3.shape = 1
+    p8 = (ctypes.c_double * 8)(1e-3, 1, 1.4, 1e-5, 2, 2, -1, 2)
+    assert L.ib_cudaFluidStep(ctypes.byref(f), ctypes.byref(geo3), p8, 8, None, None) == -100
+    assert L.ib_cudaFluidStep(ctypes.byref(f), ctypes.byref(geo3), p, 9, None, None) == -100
+    nmf = imogen.IbNumerics(0, 0, 0, 4)
+    assert L.ib_cudaFluidStep(ctypes.byref(f), ctypes.byref(geo3), p, 6, ctypes.byref(nmf), None) == -100
     # null pointers
     assert L.ib_cudaFluidStep(None, ctypes.byref(geo), p, 6, None, None) == -102
     f0 = _fluid(imogen)

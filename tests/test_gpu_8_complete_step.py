@@ -4,9 +4,10 @@ Without a source the forward step's last sweep and the backward step's first are
 axis (the backward order is the forward one reversed) and run as one double-sweep launch where
 the boundary between them is periodic.  That must give the same bits as the reference's two
 fluidstep calls (ib_fluidstep +1 then -1), in both builds, for every kernel family the double
-sweep goes through: the row kernel (x), the TMA pencil pipeline (y, z), its wide-block variant (z
-of large x-y planes), the chunked pipeline and the tile kernel (which run the sweep twice), the
-1-D shortcut and the FP32-flux form.  Six iterations put the middle pair on x, y, x, y, z, z.
+sweep goes through: the row kernel (x), the pencil-pair kernel and the TMA pencil pipeline (y, z),
+the kernels of z sweeps of large x-y planes (4-pencil boxes in FP64, the wide-block pipeline in
+FP32 flux), the chunked pipeline and the tile kernel (which run the sweep twice), the 1-D shortcut
+and the FP32-flux form.  Six iterations put the middle pair on x, y, x, y, z, z.
 
 With the two-fluid drag as the source, the composition drag(dt/2), forward, drag(dt), backward,
 drag(dt/2) is checked against the same composition of the CPU oracle.
@@ -64,9 +65,9 @@ def test_complete_step_equals_two_fluidsteps(cuda, ib, shape, method, precision,
 
 
 def test_complete_step_wide_planes(cuda, ib):
-    """z sweeps of x-y planes above 1 MB go through the wide-block pipeline (FP32 flux: 8-column
-    boxes computed 4 at a time, results stored from the input tile); iterations 4 and 5 put the
-    middle pair on z."""
+    """z sweeps of x-y planes above 1 MB: FP64 through the pencil-pair kernel with 4-pencil boxes,
+    FP32 flux through the wide-block pipeline (8-column boxes computed 4 at a time, results stored
+    from the input tile); iterations 4 and 5 put the middle pair on z."""
     shape = (512, 512, 8)
     n = shape[0] * shape[1] * shape[2]
     for precision in ("fp32flux", "fp64"):

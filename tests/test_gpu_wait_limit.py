@@ -3,10 +3,11 @@
 Every wait of these kernels for a tile is bounded; one that runs out makes the kernel wait (with
 the full limit) for the copies it has issued, leave, and set the flag ib_device_wait_status reads.
 ib_setTileWaitLimit(0) makes every tile wait give up at once while the copies complete normally,
-so the drain path runs on valid loads.  For each TMA kernel family (pencil pipeline, its wide-block
-variant, the chunked pipeline) the test checks that the call returns, that the status reports the
-run-out, that the sweep left the state untouched (no tile was computed or stored), and that after
-the limit is restored and the flag cleared the same sweep is correct again.
+so the drain path runs on valid loads.  For each TMA kernel family (pencil-pair kernel with 2- and
+4-pencil boxes, wide-block pipeline, persistent pencil pipeline, chunked pipeline) the test checks
+that the call returns, that the status reports the run-out, that the sweep left the state
+untouched (no tile was computed or stored), and that after the limit is restored and the flag
+cleared the same sweep is correct again.
 """
 import numpy as np
 import pytest
@@ -17,8 +18,10 @@ from helpers import host, product_close, to_fluid
 pytestmark = pytest.mark.gpu
 
 CASES = [
-    ((64, 64, 64), 2, "fp64"),       # y: pencil pipeline (2-pencil blocks)
-    ((512, 512, 8), 3, "fp32flux"),  # z of 2 MB planes: wide-block pipeline
+    ((64, 64, 64), 2, "fp64"),       # y: pencil-pair kernel (2-pencil boxes)
+    ((512, 512, 8), 3, "fp64"),      # z of 2 MB planes: pencil-pair kernel with 4-pencil boxes
+    ((512, 512, 8), 3, "fp32flux"),  # the same in FP32 flux: wide-block pipeline (8-column boxes)
+    ((8, 300, 6), 2, "fp64"),        # y pencils of 257-511 cells: persistent pencil pipeline
     ((8, 600, 4), 2, "fp64"),        # y pencils above 512 cells: chunked pipeline
 ]
 
