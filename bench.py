@@ -5,7 +5,10 @@ Workload (one GPU): the 3-D Kelvin-Helmholtz problem, plain HLLC FP64 drop-in, M
 256^3 periodic unit cube, gamma = 5/3, P = 2.5, rho = 2 / v_x = +0.5 in the |y-1/2| < 1/4 band
 and rho = 1 / v_x = -0.5 elsewhere, seeded U(+-1e-2) velocity perturbations, CFL 0.4.
 One step = one main-loop iteration of the reference (imogen.m:115-139): CFL reduction, forward
-3-sweep fluid step, backward 3-sweep fluid step; the state advances by 2*dt.
+3-sweep fluid step, backward 3-sweep fluid step; the state advances by 2*dt.  The timed loop is
+the library's device-side main loop (GraphLoop: the time state in device memory, each iteration a
+replayed CUDA graph, with no host read between iterations); the end-to-end leg runs every step as
+a separate job through run_iteration with host buffers.
 Metric: Mcell-updates/s = cells x iterations / seconds / 1e6 (whole job over all ranks).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -41,9 +44,9 @@ E2E_BUFFERS = int(os.environ.get("IMOGEN_BENCH_E2E_BUFFERS", "3"))
 # DRAM bytes per cell of one sweep launch (dram__bytes_read.sum + dram__bytes_write.sum / cells),
 # from the ncu capture of this workload's three sweep kernels summarised in
 # profiles/sweep_kernels_kh256_fp64.md (KH 256^3, state larger than L2).
-TRAFFIC_B_PER_CELL = {"x_row": (671.12 + 612.90) * 1e6 / 256 ** 3,
-                      "y_pipe": (697.60 + 639.29) * 1e6 / 256 ** 3,
-                      "z_pipe": (699.63 + 644.84) * 1e6 / 256 ** 3}
+TRAFFIC_B_PER_CELL = {"x_row": (671.35 + 617.76) * 1e6 / 256 ** 3,
+                      "y_pair": (671.32 + 623.59) * 1e6 / 256 ** 3,
+                      "z_pair": (671.30 + 625.57) * 1e6 / 256 ** 3}
 
 
 def parse():
@@ -647,9 +650,12 @@ def main():
         if world > 1:
             dist.barrier()
 
-    tm = ib.TimeManager(cfl=CFL)
-    for _ in range(args.warmup):
-        ib.run_iteration([fl], geo, tm, METHOD, num)
+    # The main loop runs through GraphLoop (timestep.py): the time state stays on the device and
+    # every iteration -- CFL reduction, time update, forward and backward fluid steps, time advance
+    # -- is one replayed CUDA graph; its construction runs six eager iterations (setting up scratch
+    # memory and capturing), then W warm-up replays.
+    loop = ib.GraphLoop([fl], geo, METHOD, num, cfl=CFL)
+    loop.run(args.warmup, check_every=args.warmup + 1)
     torch.cuda.synchronize()
 
     # ---------------- device-resident timed region ----------------
@@ -658,18 +664,20 @@ def main():
     barrier()
     torch.cuda.synchronize()
     sampler.start()
-    l0 = ib.imogen.launch_count()
+    ph0 = loop.phase
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     t_begin = sampler.mark()
     e0.record(stream)
-    for _ in range(args.steps):
-        ib.run_iteration([fl], geo, tm, METHOD, num)
+    loop.run(args.steps, check_every=args.steps + 1)
     e1.record(stream)
     torch.cuda.synchronize()
     t_end = sampler.mark()
-    launches = ib.imogen.launch_count() - l0
+    # the library kernels the replayed graphs launched (each phase's count from its eager run)
+    launches = sum(loop.launches[(ph0 + k) % 6] for k in range(args.steps))
     clocks = sampler.stop(t_begin, t_end)
+    tm = ib.TimeManager(cfl=CFL)
+    tm.dTime = loop.state().dt
     ms = e0.elapsed_time(e1)
     barrier()
     ms_max = max_over_ranks(ms, world, dev)
@@ -679,7 +687,7 @@ def main():
     peak, peak_kind = measured_peaks()
     kern = {}
     reps = max(3, min(10, args.steps))
-    for d, name in ((1, "x_row"), (2, "y_pipe"), (3, "z_pipe")):
+    for d, name in ((1, "x_row"), (2, "y_pair"), (3, "z_pair")):
         dt = tm.dTime
         ib.cudaFluidStep(fl, geo, [dt, 1, GAMMA, 1e-5, METHOD, d], num)  # warm
         a = torch.cuda.Event(enable_timing=True)
@@ -702,7 +710,7 @@ def main():
     torch.cuda.synchronize()
     kern["cfl"] = a.elapsed_time(b) / reps
     # share per iteration: 2 x-row launches, 2 y, 2 z, 1 cfl
-    share = {"x_row": 2 * kern["x_row"], "y_pipe": 2 * kern["y_pipe"], "z_pipe": 2 * kern["z_pipe"],
+    share = {"x_row": 2 * kern["x_row"], "y_pair": 2 * kern["y_pair"], "z_pair": 2 * kern["z_pair"],
              "cfl": kern["cfl"]}
     dom = max(share, key=share.get)
     alg_bytes = (80 if dom != "cfl" else 40) * cells

@@ -71,8 +71,10 @@ __device__ __forceinline__ double cfl_cell_cyl(double rho, double px, double py,
     } else {
         double v;
         u = hx / (fabs(px) / rho + cs);
-        v = (rin + i * hx) * hy / (fabs(py) / rho + cs);
-        u = (u < v) ? u : v;
+        if constexpr (SIM > 1) {
+            v = (rin + i * hx) * hy / (fabs(py) / rho + cs);
+            u = (u < v) ? u : v;
+        }
         if constexpr (SIM > 2) {
             v = hz / (fabs(pz) / rho + cs);
             u = (u < v) ? u : v;

@@ -93,8 +93,10 @@ int launch_cfl(const double *q, const double *cs, int64_t slab, const int grid[3
     int sim = 1;
     if (geo->global_rez[1] > 1) sim = 2;
     if (geo->global_rez[2] > 1) sim = 3;
-    const bool xj = (method == IB_METHOD_XINJIN) && (sim > 1);  // 1-D XJ uses the HLL kernel
     const bool cyl = (geo->shape == IB_GEOMETRY_CYLINDRICAL);
+    // the reference's kernel table (cflTimestep.cu:175-193): square 1-D Xin-Jin takes the HLLC
+    // form (case 12), cylindrical 1-D Xin-Jin the Xin-Jin form (case 15)
+    const bool xj = (method == IB_METHOD_XINJIN) && (sim > 1 || cyl);
     double hmin = geo->h[0];
     if (cyl) {
         if (sim == 3) hmin = (hmin < geo->h[2]) ? hmin : geo->h[2];  // dr, dz (cflTimestep.cu:301-304)
@@ -117,12 +119,20 @@ int launch_cfl(const double *q, const double *cs, int64_t slab, const int grid[3
                                                partial, counter, tau_dev, grid[0], geo->r_inner)
 #define IB_CFL_LAUNCH(S, X, F) IB_CFL_LAUNCH_C(S, X, F, false)
     if (cyl && fused) {
-        if (xj) { if (sim == 2) IB_CFL_LAUNCH_C(2, true, true, true); else IB_CFL_LAUNCH_C(3, true, true, true); }
+        if (xj) {
+            if (sim == 1) IB_CFL_LAUNCH_C(1, true, true, true);
+            else if (sim == 2) IB_CFL_LAUNCH_C(2, true, true, true);
+            else IB_CFL_LAUNCH_C(3, true, true, true);
+        }
         else if (sim == 1) IB_CFL_LAUNCH_C(1, false, true, true);
         else if (sim == 2) IB_CFL_LAUNCH_C(2, false, true, true);
         else IB_CFL_LAUNCH_C(3, false, true, true);
     } else if (cyl) {
-        if (xj) { if (sim == 2) IB_CFL_LAUNCH_C(2, true, false, true); else IB_CFL_LAUNCH_C(3, true, false, true); }
+        if (xj) {
+            if (sim == 1) IB_CFL_LAUNCH_C(1, true, false, true);
+            else if (sim == 2) IB_CFL_LAUNCH_C(2, true, false, true);
+            else IB_CFL_LAUNCH_C(3, true, false, true);
+        }
         else if (sim == 1) IB_CFL_LAUNCH_C(1, false, false, true);
         else if (sim == 2) IB_CFL_LAUNCH_C(2, false, false, true);
         else IB_CFL_LAUNCH_C(3, false, false, true);

@@ -6,6 +6,8 @@
 // between (MGA_globalReduceDimension, cudaCommon.cu:919-1004).  Here one CTA owns one pencil (or
 // 2 to 4 adjacent y/z pencils): it keeps them in registers, reduces each freezing speed in-block,
 // and runs both stages, so a sweep is one launch with one read and one write of the state.
+#include <cstdlib>
+
 #include "ib_internal.cuh"
 
 namespace ib {
@@ -280,6 +282,216 @@ __global__ void __launch_bounds__(1024) xj_pencil_kernel(double *q, int64_t slab
     }
 }
 
+// y/z sweeps of pencils of up to 256 cells, or of 512: the pencil-pair kernel's structure.  One TMA
+// box of WC adjacent pencils (the box [slab][cell][column] with the column fastest, 16-byte rows for
+// WC = 2) per CTA of one thread per cell; the CTA sweeps the pencils one after the other through
+// xj_pencil_kernel's arithmetic (one column, one cell per thread: the freezing-speed reduction over
+// the block, the relaxation fluxes through shared memory), writes each result over its own column
+// of the box and leaves by one TMA store.  No strided loads from global memory (xj_pencil_kernel's
+// y/z loads are single doubles or 16-byte pieces a row apart) and four CTAs per SM at 256 cells.
+// Every tile wait is bounded (a.spin); one that runs out sets the error flag and leaves.
+struct XjPairArgs {
+    int n, npw;
+    DevScalar lambda;
+    double gamma, minmass, mintemp;
+    unsigned int *err;
+    uint32_t spin;
+};
+
+__host__ __device__ __forceinline__ size_t xj_box_bytes(int n, int wc) { return ((size_t)40 * n * wc + 127) / 128 * 128; }
+
+template <int FLIM, int DIR, int NFIX, int WC>
+__global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
+    xj_pair_kernel(const __grid_constant__ CUtensorMap tm, XjPairArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full;
+    __shared__ double red[32];
+    const int n = NFIX ? NFIX : a.n;
+    double *T = reinterpret_cast<double *>(smem_raw);                        // [5][n][WC]
+    double *Lb = reinterpret_cast<double *>(smem_raw + xj_box_bytes(n, WC));  // [5][n]
+    double *Rb = Lb + 5 * n;                                                  // [5][n]
+    const int i = threadIdx.x;
+    const bool act = i < n;
+    const int il = (i == 0) ? n - 1 : i - 1, ir = (i == n - 1) ? 0 : i + 1;
+    constexpr int nslot = 1 + DIR;
+    const double gm1 = a.gamma - 1.0;
+    const int64_t b = blockIdx.x;
+    if (a.lambda.off()) return;  // a device timestep of 0: after the end time
+    const double lambda = a.lambda.get();
+    const bool leader = threadIdx.x == 0;
+    if (leader) {
+        mbar_init(&full, 1);
+        fence_mbar_init();
+        mbar_arrive_expect_tx(&full, (uint32_t)(40 * WC * n));
+        tma_load_5d(T, &tm, (int)(b % a.npw) * WC, 0, 0, (int)(b / a.npw), 0, &full);
+    }
+    const bool ok = mbar_wait_cta(&full, 0, a.spin);  // uniform across the CTA
+    if (!ok) {
+        if (leader) {
+            atomicOr(a.err, 1u);
+            mbar_wait(&full, 0);  // one more bounded wait for the late box
+        }
+        return;
+    }
+#pragma unroll 1
+    for (int col = 0; col < WC; col++) {
+        auto TI = [&](int k) { return (k * n + i) * WC + col; };
+        double u0[5], u1[5];
+#ifndef IB_STRICT_ARITH
+        double rinv = 1.0;
+#endif
+#pragma unroll
+        for (int k = 0; k < 5; k++) u0[k] = act ? T[TI(k)] : 1.0;
+#pragma unroll
+        for (int stage = 0; stage < 2; stage++) {
+            const double lam = (stage == 0) ? 0.25 * lambda : 0.5 * lambda;
+            const double(&X)[5] = (stage == 0) ? u0 : u1;
+            // a NaN freezing speed (negative pressure) never wins, as in the reference's max
+            double cm = 0.0;
+            if (act) {
+#ifdef IB_STRICT_ARITH
+                const double v = freeze_cell(X, 1.0 / X[0], a.gamma, gm1);
+#else
+                if (stage == 0) rinv = 1.0 / X[0];
+                const double v = freeze_cell(X, rinv, a.gamma, gm1);
+#endif
+                cm = (v > cm) ? v : cm;
+            }
+            const double Cf = block_max_keep<1>(cm, red, 0);
+            if (act) {
+                const double q1 = X[1], q2 = X[2], q3 = X[3], q4 = X[4];
+#ifdef IB_STRICT_ARITH
+                const double Pv = gm1 * (q1 - .5 * (q4 * q4 + q3 * q3 + q2 * q2) / X[0]);
+                const double Vx = X[nslot] / X[0];
+#else
+                const double Pv = gm1 * (q1 - .5 * (q4 * q4 + q3 * q3 + q2 * q2) * rinv);
+                const double Vx = X[nslot] * rinv;
+#endif
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    const double qk = X[k];
+                    double w;
+                    if (k == 0) w = X[nslot];
+                    else if (k == 1) w = Vx * (qk + Pv);
+                    else if (k == nslot) w = Vx * qk + Pv;
+                    else w = Vx * qk;
+                    Lb[k * n + i] = (Cf * qk - w);
+                    Rb[k * n + i] = (Cf * qk + w);
+                }
+            }
+            __syncthreads();
+            if (stage == 1) {
+                double nl[5], nr[5];
+                if (act) {
+#pragma unroll
+                    for (int k = 0; k < 5; k++) {
+                        const double Lm = Lb[k * n + il], L0 = Lb[k * n + i], Lp = Lb[k * n + ir];
+                        const double Rm = Rb[k * n + il], R0 = Rb[k * n + i], Rp = Rb[k * n + ir];
+                        const double dL0 = 0.5 * (L0 - Lm), dLp = 0.5 * (Lp - L0);
+                        const double dR0 = 0.5 * (R0 - Rm), dRp = 0.5 * (Rp - R0);
+                        double limL, limR;
+                        flux_limit_pair<FLIM>(dL0, dLp, dR0, dRp, limL, limR);
+                        nl[k] = L0 - limL;
+                        nr[k] = R0 + limR;
+                    }
+                }
+                __syncthreads();
+                if (act) {
+#pragma unroll
+                    for (int k = 0; k < 5; k++) { Lb[k * n + i] = nl[k]; Rb[k * n + i] = nr[k]; }
+                }
+                __syncthreads();
+            }
+            if (act) {
+                double pr[5];
+#pragma unroll
+                for (int k = 0; k < 5; k++)
+                    pr[k] = u0[k] - lam * (Rb[k * n + i] - Rb[k * n + il] - Lb[k * n + ir] + Lb[k * n + i]);
+                double p0 = pr[0], p1 = pr[1];
+                const double p2 = pr[2], p3 = pr[3], p4 = pr[4];
+                p0 = (p0 < a.minmass) ? a.minmass : p0;
+#ifdef IB_STRICT_ARITH
+                double w = .5 * (p2 * p2 + p3 * p3 + p4 * p4) / p0;
+#else
+                rinv = 1.0 / p0;
+                double w = .5 * (p2 * p2 + p3 * p3 + p4 * p4) * rinv;
+#endif
+                if ((p1 - w) < p0 * a.mintemp) p1 = w + p0 * a.mintemp;
+                u1[0] = p0; u1[1] = p1; u1[2] = p2; u1[3] = p3; u1[4] = p4;
+            }
+        }
+        // this pencil's result over its own column of the box (its inputs were read above)
+        if (act) {
+#pragma unroll
+            for (int k = 0; k < 5; k++) T[TI(k)] = u1[k];
+        }
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (leader) {
+        tma_store_5d(&tm, T, (int)(b % a.npw) * WC, 0, 0, (int)(b / a.npw), 0);
+        bulk_commit();
+        bulk_wait_all();
+    }
+}
+
+// Returns IB_ERROR_NOIMPLEMENT (the caller falls back to xj_pencil_kernel) where TMA's rules or
+// the kernel's sizes do not hold: nx a multiple of WC, 16-byte aligned base and slab pitch, pencils
+// of up to 256 cells or of 512.
+template <int FLIM, int DIR, int NFIX, int WC>
+static int launch_xj_pair(double *q, int64_t slab, const int grid[3], DevScalar lambda, double gamma, double rho_min,
+                          double mintemp, cudaStream_t st)
+{
+    const int nx = grid[0], ny = grid[1], nz = grid[2];
+    const int n = grid[DIR - 1];
+    if ((NFIX && n != NFIX) || (!NFIX && n > 256) || n < 3 || (nx % WC)) return IB_ERROR_NOIMPLEMENT;
+    if (((uintptr_t)q & 15) || (slab * 8) % 16) return IB_ERROR_NOIMPLEMENT;
+    const uint64_t other = (DIR == 2) ? nz : ny;
+    const uint64_t rs = (DIR == 2) ? (uint64_t)nx * 8 : (uint64_t)nx * ny * 8;  // along the pencil
+    const uint64_t os = (DIR == 2) ? (uint64_t)nx * ny * 8 : (uint64_t)nx * 8;  // across pencils
+    // TMA boxes are at most 256 rows: a 512-cell pencil comes as two rows of 256
+    const int bh = (n > 256) ? n / 2 : n, nh = (n > 256) ? 2 : 1;
+    uint64_t dims[5] = {(uint64_t)nx, (uint64_t)bh, (uint64_t)nh, other, 5};
+    uint64_t strides[4] = {rs, rs * bh, os, (uint64_t)slab * 8};
+    uint32_t box[5] = {WC, (uint32_t)bh, (uint32_t)nh, 1, 5};
+    const int npw = nx / WC;
+    const int64_t nblocks = (int64_t)npw * other;
+    if (nblocks >= (int64_t)1 << 31) return IB_ERROR_NOIMPLEMENT;
+    CUtensorMap tm;
+    int rc = encode_tmap_f64(&tm, q, 5, dims, strides, box);
+    if (rc) return rc;
+    unsigned int *err = scratch().wait_flag();
+    if (!err) return IB_ERROR_NOMEM;
+    const int nt = (n + 31) / 32 * 32;
+    const size_t shm = xj_box_bytes(n, WC) + (size_t)80 * n;
+    static int attr_bytes = 0;
+    if ((int)shm > attr_bytes) {
+        rc = check_cuda(cudaFuncSetAttribute(xj_pair_kernel<FLIM, DIR, NFIX, WC>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        if (rc) return rc;
+        attr_bytes = (int)shm;
+    }
+    XjPairArgs a{n, npw, lambda, gamma, rho_min, mintemp, err, tile_wait_limit()};
+    xj_pair_kernel<FLIM, DIR, NFIX, WC><<<(unsigned)nblocks, nt, shm, st>>>(tm, a);
+    return check_launch();
+}
+
+template <int FLIM>
+static int launch_xj_pair_dir(int dir, double *q, int64_t slab, const int grid[3], DevScalar lambda, double gamma,
+                              double rho_min, double mintemp, cudaStream_t st)
+{
+    const int n = grid[dir - 1];
+    if (dir == 2) {
+        if (n == 512) return launch_xj_pair<FLIM, 2, 512, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
+        if (n == 256) return launch_xj_pair<FLIM, 2, 256, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
+        return launch_xj_pair<FLIM, 2, 0, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
+    }
+    if (n == 512) return launch_xj_pair<FLIM, 3, 512, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
+    if (n == 256) return launch_xj_pair<FLIM, 3, 256, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
+    return launch_xj_pair<FLIM, 3, 0, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
+}
+
 int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3], DevScalar lambda, double gamma,
                     double rho_min, cudaStream_t st, const CylSweep *cyl)
 {
@@ -287,6 +499,23 @@ int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3
     const CylPencil cp = cyl ? cyl->pencil : CylPencil{0.0, 0.0, 0, 0};
     if ((geo == CYL_RADIAL && dir != 1) || ((geo == CYL_THETA_DIV || geo == CYL_THETA_LAM) && dir != 2))
         return IB_ERROR_INVALID_ARGS;
+    // y/z pencils of square grids: TMA pencil boxes (IMOGEN_B200_XJPAIR=0: the pencil kernel)
+    static const bool xj_pair = [] {
+        const char *e = getenv("IMOGEN_B200_XJPAIR");
+        return !(e && e[0] == '0');
+    }();
+    if (xj_pair && dir > 1 && geo == CYL_NONE) {
+        const double mt = 1e-5 / (gamma - 1);
+        int rc;
+        switch (flim) {
+        case IB_FLUX_OSPRE: rc = launch_xj_pair_dir<IB_FLUX_OSPRE>(dir, q, slab, grid, lambda, gamma, rho_min, mt, st); break;
+        case IB_FLUX_VANLEER: rc = launch_xj_pair_dir<IB_FLUX_VANLEER>(dir, q, slab, grid, lambda, gamma, rho_min, mt, st); break;
+        case IB_FLUX_MINMOD: rc = launch_xj_pair_dir<IB_FLUX_MINMOD>(dir, q, slab, grid, lambda, gamma, rho_min, mt, st); break;
+        case IB_FLUX_SUPERBEE: rc = launch_xj_pair_dir<IB_FLUX_SUPERBEE>(dir, q, slab, grid, lambda, gamma, rho_min, mt, st); break;
+        default: rc = launch_xj_pair_dir<IB_FLUX_ZERO>(dir, q, slab, grid, lambda, gamma, rho_min, mt, st); break;
+        }
+        if (rc != IB_ERROR_NOIMPLEMENT) return rc;
+    }
     const int n = grid[dir - 1];
     const int64_t N = (int64_t)grid[0] * grid[1] * grid[2];
     if (n > 2048) return IB_ERROR_NOIMPLEMENT;  // 1024 threads x 2 cells per pencil block

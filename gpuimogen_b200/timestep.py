@@ -99,8 +99,12 @@ class GraphLoop:
         self._dt_ptr = self.ts_ptr + ib.IbTimeState.dt.offset
         self._graphs = []
         self.phase = 0
+        # the library's kernel launches of each phase's iteration (what a replay of its graph runs)
+        self.launches = []
         for _ in range(6):
+            l0 = ib.launch_count()
             self._iteration(self.phase)
+            self.launches.append(ib.launch_count() - l0)
             self.phase += 1
         torch.cuda.synchronize()
         for p in range(6):

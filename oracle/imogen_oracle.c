@@ -1019,8 +1019,9 @@ double or_cfl_timestep_geo(const double *q, const double *cs, const or_grid *g, 
     if (global_rez[1] > 1) spacedim = 1;
     if (global_rez[2] > 1) spacedim = 2;
     sim = spacedim + 1;
-    /* ctype table (cflTimestep.cu:175-193): 1-D Xin-Jin uses the HLL/HLLC kernel */
-    algo_xj = (method == 3) && (sim > 1);
+    /* ctype table (cflTimestep.cu:175-193): square 1-D Xin-Jin uses the HLLC kernel (case 12), the
+     * cylindrical one the Xin-Jin kernel (case 15) */
+    algo_xj = (method == 3) && (sim > 1 || geometry == OR_GEO_CYLINDRICAL);
     hmin = h[0];
     if (geometry == OR_GEO_CYLINDRICAL) {
         /* dr, and dz in 3-D; the theta extent is taken per cell (cflTimestep.cu:301-304) */
@@ -1059,11 +1060,13 @@ double or_cfl_timestep_geo(const double *q, const double *cs, const or_grid *g, 
         } else {
             double r = rho[x];
             u = h[0] / (fabs(px[x]) / r + cs[x]);
-            if (geometry == OR_GEO_CYLINDRICAL)
-                v = (r_inner + (x % g->nx) * h[0]) * h[1] / (fabs(py[x]) / r + cs[x]);
-            else
-                v = h[1] / (fabs(py[x]) / r + cs[x]);
-            u = (u < v) ? u : v;
+            if (sim > 1) {
+                if (geometry == OR_GEO_CYLINDRICAL)
+                    v = (r_inner + (x % g->nx) * h[0]) * h[1] / (fabs(py[x]) / r + cs[x]);
+                else
+                    v = h[1] / (fabs(py[x]) / r + cs[x]);
+                u = (u < v) ? u : v;
+            }
             if (sim > 2) {
                 v = h[2] / (fabs(pz[x]) / r + cs[x]);
                 u = (u < v) ? u : v;

@@ -156,3 +156,23 @@ def test_xinjin_tiny_momenta_stay_finite(cuda, ib, po, direction):
         out = host(fl)
         assert np.all(np.isfinite(out[:, :N])), variant
         assert np.allclose(out[:, :N], ref[:, :N], rtol=1e-12, atol=1e-300), variant
+
+
+@pytest.mark.parametrize("shape,direction", [((4, 256, 5), 2), ((2, 5, 512), 3), ((6, 512, 2), 2), ((10, 4, 256), 3)])
+def test_xinjin_pencil_boxes_fixed_lengths(cuda, ib, po, shape, direction):
+    """Xin-Jin y/z sweeps of 256- and 512-cell pencils go through the TMA pencil-box kernel's
+    fixed-length forms (a 512-cell pencil as two box rows of 256): bit for bit the oracle's."""
+    n = shape[0] * shape[1] * shape[2]
+    q = problems.random_jumpy(shape, gamma=1.4, seed=17)
+    h = (0.05, 0.04, 0.03)
+    ref = q.copy()
+    po.fluid_sweep(ref, shape, po.step_params(2e-3, h, 1.4, method=3), direction)
+    ib.use_variant("strict")
+    try:
+        fl = to_fluid(q, shape)
+        ib.cudaFluidStep(fl, ib.Geometry(shape, h), [2e-3, 1, 1.4, 1e-5, 3, direction])
+        out = host(fl)
+    finally:
+        ib.use_variant("product")
+    assert bits_equal(out, ref, n), first_diff(out, ref, n)
+    assert ib.device_wait_status() == 0

@@ -59,3 +59,29 @@ def test_tile_wait_runs_out_and_recovers(cuda, ib, po, shape, direction, precisi
     else:   # FP32 flux arithmetic: within the form's stated 1e-5 relative L1
         ok, info = product_close(out, ref, n, l1=1e-5, scale=1e-4)
     assert ok, info
+
+
+def test_xinjin_tile_wait_runs_out_and_recovers(cuda, ib, po):
+    """The same for the Xin-Jin pencil-box kernel (y sweep of 64-cell pencils)."""
+    L = ib.load("product")
+    shape = (64, 64, 16)
+    n = shape[0] * shape[1] * shape[2]
+    q0 = problems.random_smooth(shape, gamma=1.4, seed=6, amp=0.3)
+    geo = ib.Geometry(shape)
+    params = [2e-4, 1, 1.4, 1e-5, 3, 2]
+    ib.device_wait_status(clear=True)
+    fl = to_fluid(q0.copy(), shape, gamma=1.4)
+    try:
+        assert L.ib_setTileWaitLimit(0) == 0
+        ib.cudaFluidStep(fl, geo, params)
+        assert ib.device_wait_status() == 1
+        assert np.array_equal(host(fl)[:, :n], q0[:, :n])
+    finally:
+        L.ib_setTileWaitLimit(-1)
+    assert ib.device_wait_status(clear=True) == 1
+    ib.cudaFluidStep(fl, geo, params)
+    assert ib.device_wait_status() == 0
+    ref = q0.copy()
+    po.fluid_sweep(ref, shape, po.step_params(2e-4, geo.h, 1.4, method=3), 2)
+    ok, info = product_close(host(fl), ref, n)
+    assert ok, info
