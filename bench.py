@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--fluxlim", default="vanleer")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32flux"])
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--cyl", action="store_true", help="case time-sweeps: cylindrical geometry")
+    ap.add_argument("--t-end", type=float, default=0.01, help="case ensemble: end time")
     return ap.parse_args()
 
 
@@ -102,14 +104,21 @@ def case_sweeps(args):
 
 def case_time_sweeps(args):
     """Per-direction sweep time (CUDA events, mean of --reps launches after one untimed launch)
-    of cudaFluidStep on the Kelvin-Helmholtz state: n^3 (default 256) or --shape."""
+    of cudaFluidStep on the Kelvin-Helmholtz state: n^3 (default 256) or --shape.  --cyl: the
+    rotating annulus in cylindrical geometry instead (x = r, y = theta)."""
     import torch
     import gpuimogen_b200 as ib
     from gpuimogen_b200 import problems
     shape = _case_shape(args, 256)
     num = ib.numerics(slope=args.slope, fluxlim=args.fluxlim, precision=args.precision)
-    fl = ib.Fluid(shape, q=torch.from_numpy(problems.kelvin_helmholtz(shape, seed=1)).cuda(), gamma=GAMMA)
-    geo = ib.Geometry(shape)
+    if args.cyl:
+        h = [1.0 / shape[0], 2 * math.pi / shape[1], 1.0 / shape[2]]
+        q = problems.rotating_annulus(shape, r_inner=1.0, dr=h[0], gamma=GAMMA, seed=1)
+        geo = ib.Geometry(shape, h=h, cylindrical=True, r_inner=1.0)
+    else:
+        q = problems.kelvin_helmholtz(shape, seed=1)
+        geo = ib.Geometry(shape)
+    fl = ib.Fluid(shape, q=torch.from_numpy(q).cuda(), gamma=GAMMA)
     out = []
     for d in (1, 2, 3):
         if shape[d - 1] < 3:
@@ -126,7 +135,25 @@ def case_time_sweeps(args):
         torch.cuda.synchronize()
         out.append(round(a.elapsed_time(b) / args.reps, 4))
     print(json.dumps({"case": "time-sweeps", "shape": list(shape), "method": args.method, "slope": args.slope,
-                      "fluxlim": args.fluxlim, "precision": args.precision, "ms_x_y_z": out}))
+                      "fluxlim": args.fluxlim, "precision": args.precision, "cylindrical": bool(args.cyl),
+                      "ms_x_y_z": out}))
+
+
+def case_ensemble(args):
+    """One launch of the 4096-problem Riemann ensemble (the batching form's problems, HLLC MC,
+    FP64 or --precision) to --t-end (default 0.01, a tenth of the form's end time: a short launch
+    for an ncu capture), after one untimed launch; prints its CUDA-event time and throughput."""
+    import torch
+    from gpuimogen_b200 import ensemble
+    ens = ensemble.RiemannEnsemble.random(4096, seed=1)
+    kw = dict(t_end=args.t_end, cfl=CFL, slope="mc", precision=args.precision,
+              tuning={"threads": 512, "chunk": 504, "ctas_per_sm": 0})
+    ens.run(**kw)
+    ens.reset()
+    torch.cuda.synchronize()
+    ms = _events_ms(lambda: ens.run(**kw))
+    print(json.dumps({"case": "ensemble", "problems": 4096, "t_end": args.t_end, "precision": args.precision,
+                      "ms": ms, "mcell_updates_per_s": ens.cell_updates() / (ms / 1e3) / 1e6}))
 
 
 def case_cfl(args):
@@ -283,7 +310,7 @@ def case_graph(args):
     print(json.dumps({"case": "graph", **graph_loop_timing()}))
 
 
-CASES = {"graph": case_graph, "sweeps": case_sweeps, "time-sweeps": case_time_sweeps, "cfl": case_cfl, "drag": case_drag,
+CASES = {"ensemble": case_ensemble, "graph": case_graph, "sweeps": case_sweeps, "time-sweeps": case_time_sweeps, "cfl": case_cfl, "drag": case_drag,
          "all": case_all}
 
 
