@@ -147,7 +147,7 @@ def case_ensemble(args):
     from gpuimogen_b200 import ensemble
     ens = ensemble.RiemannEnsemble.random(4096, seed=1)
     kw = dict(t_end=args.t_end, cfl=CFL, slope="mc", precision=args.precision,
-              tuning={"threads": 512, "chunk": 504, "ctas_per_sm": 0})
+              tuning={"threads": 256, "chunk": 248, "ctas_per_sm": 0})
     ens.run(**kw)
     ens.reset()
     torch.cuda.synchronize()

@@ -8,8 +8,9 @@
 // (TimeManager.m:270-277).  Here a CTA takes a problem from a device work counter and runs it to
 // its end without leaving the kernel; the problem's cells stay in L2 between sweeps (one
 // problem is at most a few hundred KB), so the launch reads and writes HBM about once per cell.
-// The per-cell arithmetic is the library's sweep (tile_sweep), CFL and boundary code, so every
-// problem's result equals running it alone through the library's 1-D entry points.
+// The per-cell arithmetic is the library's sweep arithmetic (stage_prims / stage_faces /
+// stage_flux in ens_sweep), CFL and boundary code, so every problem's result equals running it
+// alone through the library's 1-D entry points.
 #include "ib_bc.cuh"
 #include "ib_cfl.cuh"
 #include "ib_internal.cuh"
@@ -30,7 +31,7 @@ struct EnsArgs {
     int32_t bc0, bc1;
     int32_t itermax;
     int32_t target;    // chunk length to aim for
-    int32_t lcap;      // largest chunk the shared memory holds
+    int32_t lcap;      // tile rows (chunk + 8 halo cells) the shared memory planes hold, <= threads
     double gg1;        // gamma (gamma - 1), soundspeed
     double cfl, t_end;
     int32_t halve;
@@ -49,32 +50,158 @@ __device__ __forceinline__ void ens_boundary(double *qb, int64_t S, int n, int b
     }
 }
 
-// Chunk length for a pencil of n cells: as in the tile launcher, every chunk >= 8 cells.
-__device__ __forceinline__ int ens_chunk(int n, int target)
+// Number of chunks for a problem of n cells: chunk ch covers cells [ch n / nc, (ch + 1) n / nc), so
+// no chunk is longer than the target and, as the in-place rules need, none is shorter than 8 cells.
+// Every output cell is the same function of the 9 original cells around it whatever the chunks.
+__device__ __forceinline__ int ens_nchunks(int n, int target)
 {
     int nc = max(1, (n + target - 1) / target);
-    int Lc = (n + nc - 1) / nc;
-    while (nc > 1 && (Lc < 8 || n - (nc - 1) * Lc < 8)) {
-        nc--;
-        Lc = (n + nc - 1) / nc;
-    }
-    return Lc;
+    while (nc > 1 && n / nc < 8) nc--;
+    return nc;
 }
 
+// One x sweep of a problem of n cells in nc chunks (ens_nchunks; the longest chunk + 8 <= lcap <= NT):
+// the tile sweep's in-place rules (each chunk loads its cells and 4 halo cells a side of the original
+// state; the last four outputs of a chunk wait in `pend` until the next chunk has loaded them, the
+// first chunk's first four in `first` until the last chunk has read them through the periodic
+// wrap) with the row kernel's phases: tile row i of a chunk is thread i, which keeps that cell's
+// state in registers through both stages; two shared-memory planes of FT swap roles between the
+// stages, so a chunk takes seven barriers.  The arithmetic is the library's sweep arithmetic
+// (stage_prims / stage_faces / stage_flux), so the results are those of the tile sweep.
 template <int METHOD, int SLOPE, typename FT, int NT>
-__global__ void __launch_bounds__(NT, 1024 / NT) ensemble_kernel(EnsArgs a, FluidConsts<FT> c)
+__device__ __forceinline__ void ens_sweep(double *qb, int64_t S, int n, int nchunks, double lambda,
+                                          const FluidConsts<FT> &c, FT *SA, FT *SB, int TR, double *pend,
+                                          double *first)
+{
+    const int i = threadIdx.x;
+    const bool single = (nchunks == 1);
+    for (int ch = 0; ch < nchunks; ch++) {
+        const int cb = (int)((int64_t)ch * n / nchunks);
+        const int len = (int)((int64_t)(ch + 1) * n / nchunks) - cb;
+        const int tr = len + 8;
+        double u0[5], u1[5];
+        V5<FT> keep;
+        if (i < tr) {
+            const int cell = mod_n(cb - 4 + i, n);
+#pragma unroll
+            for (int k = 0; k < 5; k++) u0[k] = qb[(int64_t)k * S + cell];
+        }
+        __syncthreads();  // this chunk has loaded the original state of its halo
+        if (ch > 0 && i < 4) {
+#pragma unroll
+            for (int k = 0; k < 5; k++) qb[(int64_t)k * S + cb - 4 + i] = pend[k * 4 + i];
+        }
+        // ---- stage A: prims and fluxes in SA, left faces in SB ----
+        if (i < tr) {
+            V5<FT> w = stage_prims<METHOD, 1, FT>(u0, c);  // HLL floors u0
+#pragma unroll
+            for (int k = 0; k < 5; k++) SA[k * TR + i] = w.a[k];
+        }
+        __syncthreads();
+        if (i >= 1 && i <= tr - 2) {
+            V5<FT> w, dl, dr, L;
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                w.a[k] = SA[k * TR + i];
+                dl.a[k] = w.a[k] - SA[k * TR + i - 1];
+                dr.a[k] = SA[k * TR + i + 1] - w.a[k];
+            }
+            stage_faces<METHOD, SLOPE, FT>(c, w, dl, dr, L, keep);
+#pragma unroll
+            for (int k = 0; k < 5; k++) SB[k * TR + i] = L.a[k];
+        }
+        __syncthreads();
+        if (i >= 1 && i <= tr - 3) {
+            V5<FT> Lr;
+#pragma unroll
+            for (int k = 0; k < 5; k++) Lr.a[k] = SB[k * TR + i + 1];
+            keep = stage_flux<METHOD, FT>(c, keep, Lr);
+#pragma unroll
+            for (int k = 0; k < 5; k++) SA[k * TR + i] = keep.a[k];
+        }
+        __syncthreads();
+        if (i >= 2 && i <= tr - 3) {
+#pragma unroll
+            for (int k = 0; k < 5; k++) u1[k] = u0[k] - lambda * ((double)keep.a[k] - (double)SA[k * TR + i - 1]);
+        }
+        // ---- stage B: prims and fluxes in SB, left faces in SA (no barrier: stage A's last
+        // phase read SA only) ----
+        if (i >= 2 && i <= tr - 3) {
+            V5<FT> w = stage_prims<METHOD, 1, FT>(u1, c);  // HLL floors u1
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                SB[k * TR + i] = w.a[k];
+                u0[k] = u1[k] + u0[k];  // the output's (u1 + u0), rounded as it is there first
+            }
+        }
+        __syncthreads();
+        if (i >= 3 && i <= tr - 4) {
+            V5<FT> w, dl, dr, L;
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                w.a[k] = SB[k * TR + i];
+                dl.a[k] = w.a[k] - SB[k * TR + i - 1];
+                dr.a[k] = SB[k * TR + i + 1] - w.a[k];
+            }
+            stage_faces<METHOD, SLOPE, FT>(c, w, dl, dr, L, keep);
+#pragma unroll
+            for (int k = 0; k < 5; k++) SA[k * TR + i] = L.a[k];
+        }
+        __syncthreads();
+        if (i >= 3 && i <= tr - 5) {
+            V5<FT> Lr;
+#pragma unroll
+            for (int k = 0; k < 5; k++) Lr.a[k] = SA[k * TR + i + 1];
+            keep = stage_flux<METHOD, FT>(c, keep, Lr);
+#pragma unroll
+            for (int k = 0; k < 5; k++) SB[k * TR + i] = keep.a[k];
+        }
+        __syncthreads();
+        if (i >= 4 && i <= tr - 5) {
+            const int m = i - 4;  // output cell cb + m
+            double out[5];
+#pragma unroll
+            for (int k = 0; k < 5; k++)
+                out[k] = .5 * (u0[k] - lambda * ((double)keep.a[k] - (double)SB[k * TR + i - 1]));
+            if (!single && ch == 0 && m < 4) {
+#pragma unroll
+                for (int k = 0; k < 5; k++) first[k * 4 + m] = out[k];
+            } else if (!single && m >= len - 4) {
+#pragma unroll
+                for (int k = 0; k < 5; k++) pend[k * 4 + m - (len - 4)] = out[k];
+            } else {
+#pragma unroll
+                for (int k = 0; k < 5; k++) qb[(int64_t)k * S + cb + m] = out[k];
+            }
+        }
+        // the next chunk's first barrier separates these reads of SB and writes of pend from its
+        // stage A
+    }
+    __syncthreads();
+    if (!single && i < 4) {
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            qb[(int64_t)k * S + n - 4 + i] = pend[k * 4 + i];
+            qb[(int64_t)k * S + i] = first[k * 4 + i];
+        }
+    }
+    __syncthreads();
+}
+
+// Three CTAs of 256 threads per SM (80 registers) rather than four: at 64 registers a thread's
+// state of two stages spills; 512-thread CTAs keep two per SM, one would idle half the SM.
+template <int METHOD, int SLOPE, typename FT, int NT>
+__global__ void __launch_bounds__(NT, NT == 512 ? 2 : 768 / NT) ensemble_kernel(EnsArgs a, FluidConsts<FT> c)
 {
     extern __shared__ __align__(16) double tsm[];
-    __shared__ int64_t colbase[1];
-    __shared__ bool colok[1];
     __shared__ int s_prob;
     __shared__ double s_red[NT / 32];
     __shared__ double s_dt;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    if (tid == 0) {
-        colbase[0] = 0;
-        colok[0] = true;
-    }
+    double *pend = tsm;        // [5][4]
+    double *first = tsm + 20;  // [5][4]
+    FT *SA = reinterpret_cast<FT *>(tsm + 40);  // [5][lcap]
+    FT *SB = SA + 5 * a.lcap;
     for (;;) {
         if (tid == 0) {
             const unsigned k = atomicAdd(a.counter, 1u);
@@ -87,8 +214,8 @@ __global__ void __launch_bounds__(NT, 1024 / NT) ensemble_kernel(EnsArgs a, Flui
         const int64_t nn = a.off[p + 1] - off;
         const double h = a.h[p];
         const int n = (int)nn;
-        const int Lc = (nn >= 9 && nn < (1 << 30)) ? ens_chunk(n, a.target) : 0;
-        if (Lc == 0 || Lc > a.lcap || p >= a.np) {
+        const int nc = (nn >= 9 && nn < (1 << 30)) ? ens_nchunks(n, a.target) : 0;
+        if (nc == 0 || (n + nc - 1) / nc + 8 > a.lcap || p >= a.np) {
             if (tid == 0 && p < a.np) {
                 a.t_out[p] = 0.0;
                 a.it_out[p] = -1;  // not run: fewer than 9 cells or a chunk beyond the tile
@@ -123,7 +250,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) ensemble_kernel(EnsArgs a, Flui
             const double dt = s_dt;
             const double lambda = dt / h;
             for (int half = 0; half < 2; half++) {
-                tile_sweep<METHOD, SLOPE, FT, 1, 1>(qb, a.S, colbase, colok, 1, n, Lc, lambda, c, tsm);
+                ens_sweep<METHOD, SLOPE, FT, NT>(qb, a.S, n, nc, lambda, c, SA, SB, a.lcap, pend, first);
                 if (tid == 0) ens_boundary(qb, a.S, n, a.bc0, a.bc1);
                 __syncthreads();
             }
@@ -141,11 +268,12 @@ __global__ void __launch_bounds__(NT, 1024 / NT) ensemble_kernel(EnsArgs a, Flui
     }
 }
 
-// Shared memory of one CTA: the tile of a chunk of up to lcap cells.
+// Shared memory of one CTA: the pending and first outputs, two planes of a chunk of up to lcap
+// tile rows.
 template <typename FT>
 static size_t ens_smem(int lcap)
 {
-    return tile_smem_bytes<1>(lcap, sizeof(FT));
+    return sizeof(double) * 40 + sizeof(FT) * 10 * (size_t)lcap;
 }
 
 template <int METHOD, int SLOPE, typename FT, int NT>
@@ -163,7 +291,7 @@ static int launch_ens_nt(const EnsArgs &a0, const FluidConsts<FT> &c, int ctas_p
     }
     int per_sm = 0;
     if ((rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, shm)))) return rc;
-    if (per_sm < 1) return IB_ERROR_INVALID_ARGS;
+    if (per_sm < 1 || a.lcap > NT) return IB_ERROR_INVALID_ARGS;
     if (ctas_per_sm > 0 && ctas_per_sm < per_sm) per_sm = ctas_per_sm;
     const int64_t grid = std::min<int64_t>((int64_t)per_sm * num_sms(), a.np);
     if ((rc = check_cuda(cudaMemsetAsync(a.counter, 0, sizeof(unsigned int), st)))) return rc;
