@@ -212,11 +212,51 @@ __device__ __forceinline__ V5<FT> stage_flux(const FluidConsts<FT> &c, const V5<
     else return hll_flux<FT>(c, l, r);
 }
 
+// lambda times the flux difference of one cell in cylindrical geometry, component by component
+// (local order rho, E, p_n, p_t1, p_t2; p_n = p_r in a radial sweep).  fR / fL: fluxes through the
+// cell's outer / inner face.  Radial: rc = the cell centre radius; HLLC weights the faces by
+// (rc +- dr/2) / rc and subtracts dr / (2 rc) times the cell's two face pressures from p_r's
+// difference (cudaFluidStep.cu:1164-1171, 1488-1495); HLL folds lambda into those factors and
+// subtracts the stage input's pressure (adiabatic) or rho c_iso^2 with rho the predicted density
+// (isothermal) times lambda dr / rc (1837-1842, 2270-2290, 2371-2391).  CYL_THETA_DIV divides by
+// the pencil radius; CYL_THETA_LAM gets lambda already divided by it.
+template <int METHOD, int GEO>
+__device__ __forceinline__ double cyl_dflux(int k, double fR, double fL, double lam, double rc, double dr,
+                                            double rpen, double psum, double p_hll, double rho1,
+                                            const FluidConsts<double> &c)
+{
+    if constexpr (GEO == CYL_RADIAL) {
+        if constexpr (METHOD == IB_METHOD_HLLC) {
+            const double cA = (rc - .5 * dr) / (rc);
+            const double cB = (rc + .5 * dr) / (rc);
+            const double cC = 0.5 * dr / rc;
+            double d = cB * fR - cA * fL;
+            if (k == 2) d = d - cC * psum;
+            return lam * d;
+        } else {
+            const double cA = lam * (rc - .5 * dr) / (rc);
+            const double cB = lam * (rc + .5 * dr) / (rc);
+            const double cC = lam * dr / rc;
+            double d = cB * fR - cA * fL;
+            if (k == 2) {
+                if (c.isotemp == -1) d = d - p_hll * cC;
+                else d = d - rho1 * c.isotempsq * cC;
+            }
+            return d;
+        }
+    } else if constexpr (GEO == CYL_THETA_DIV) {
+        return lam * (fR - fL) / rpen;
+    } else {
+        return lam * (fR - fL);
+    }
+}
+
 struct SweepArgs {
     double *q;
     int64_t slab;
     int nx, ny, nz;
     DevScalar lambda;
+    double crin, cdr;  // radial sweeps (GEO == CYL_RADIAL): radius of cell 0's centre, radial cell size
 };
 
 // ------------------------------------------------------------------------------------------
@@ -232,15 +272,23 @@ struct SweepArgs {
 template <int CPT, int NFIX>
 __host__ __device__ constexpr bool row_ssum() { return CPT == 1 && NFIX != 512; }
 
-// NS: sweeps applied in a row (1, or 2 for the two same-axis sweeps in the middle of an iteration)
-template <int METHOD, int SLOPE, typename FT, int CPT, int NFIX = 0, int NS = 1>
+// NS: sweeps applied in a row (1, or 2 for the two same-axis sweeps in the middle of an iteration).
+// GEO == CYL_RADIAL: the radial sweep of cylindrical geometry (x = r), whose update weights the
+// faces by their radii and adds the geometric pressure term to p_r (cyl_dflux); one cell per
+// thread, FP64, one sweep.
+template <int METHOD, int SLOPE, typename FT, int CPT, int NFIX = 0, int NS = 1, int GEO = CYL_NONE>
 __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_kernel(SweepArgs a, FluidConsts<FT> c)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    static_assert(GEO == CYL_NONE || (GEO == CYL_RADIAL && row_ssum<CPT, NFIX>() && NS == 1 &&
+                                      std::is_same<FT, double>::value),
+                  "radial rows: one cell per thread with the SSPRK sum in shared memory, one FP64 sweep");
+    // its own name: every declaration of one extern shared array must agree on the alignment, and
+    // the TMA kernels' smem_raw is 1024-byte aligned
+    extern __shared__ __align__(16) unsigned char row_smem_raw[];
     const int n = NFIX ? NFIX : a.nx;  // NFIX: the row length fixed at compile time
-    FT *SA = reinterpret_cast<FT *>(smem_raw);
+    FT *SA = reinterpret_cast<FT *>(row_smem_raw);
     FT *SB = SA + 5 * n;
-    double *SS = reinterpret_cast<double *>(smem_raw + (size_t)10 * n * sizeof(FT));
+    double *SS = reinterpret_cast<double *>(row_smem_raw + (size_t)10 * n * sizeof(FT));
     const int64_t row = blockIdx.x;
     double *q = a.q + row * n;
     const int64_t S = a.slab;
@@ -250,6 +298,8 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
     double u0[CPT][5], u1[CPT][5];
     V5<FT> keep[CPT];  // right faces, later fluxes
     bool act[CPT];
+    // radial rows: the stage's face pressure sum (HLLC) or its input's pressure (HLL)
+    double psum = 0.0, php = 0.0;
 #pragma unroll
     for (int m = 0; m < CPT; m++) {
         int i = threadIdx.x + m * blockDim.x;
@@ -282,6 +332,7 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
                 V5<FT> w = stage_prims<METHOD, 1, FT>(u[m], c);
 #pragma unroll
                 for (int k = 0; k < 5; k++) PX[k * n + i] = w.a[k];
+                if (GEO == CYL_RADIAL && METHOD == IB_METHOD_HLL) php = (double)w.a[2];
                 if (row_ssum<CPT, NFIX>() && stage == 1) {  // after the prims: HLL floors u1 in place
 #pragma unroll
                     for (int k = 0; k < 5; k++) SS[k * n + i] = u1[m][k] + u0[m][k];
@@ -305,6 +356,7 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
                 stage_faces<METHOD, SLOPE, FT>(c, w, dl, dr, L, keep[m]);
 #pragma unroll
                 for (int k = 0; k < 5; k++) PY[k * n + i] = L.a[k];
+                if (GEO == CYL_RADIAL && METHOD == IB_METHOD_HLLC) psum = (double)L.a[1] + (double)keep[m].a[1];
             }
         }
         __syncthreads();
@@ -329,12 +381,27 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
             int i = threadIdx.x + m * blockDim.x;
             if (act[m]) {
                 int il = (i == 0) ? n - 1 : i - 1;
+                if constexpr (GEO == CYL_RADIAL) {
+                    const double rc = a.crin + i * a.cdr;
+                    // the isothermal HLL term's density: the new prediction (stage 0), the stage's
+                    // own floored input (stage 1)
+                    const double rho_in = u1[m][0];
 #pragma unroll
-                for (int k = 0; k < 5; k++) {
-                    double df = (double)keep[m].a[k] - (double)PX[k * n + il];
-                    if (stage == 0) u1[m][k] = u0[m][k] - lambda * df;
-                    else if (row_ssum<CPT, NFIX>()) u1[m][k] = .5 * (SS[k * n + i] - lambda * df);
-                    else u1[m][k] = .5 * (u1[m][k] + u0[m][k] - lambda * df);
+                    for (int k = 0; k < 5; k++) {
+                        const double rho1 = (stage == 0) ? (k == 0 ? 0.0 : u1[m][0]) : rho_in;
+                        const double d = cyl_dflux<METHOD, GEO>(k, (double)keep[m].a[k], (double)PX[k * n + il], lambda,
+                                                                rc, a.cdr, 0.0, psum, php, rho1, c);
+                        if (stage == 0) u1[m][k] = u0[m][k] - d;
+                        else u1[m][k] = .5 * (SS[k * n + i] - d);
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 5; k++) {
+                        double df = (double)keep[m].a[k] - (double)PX[k * n + il];
+                        if (stage == 0) u1[m][k] = u0[m][k] - lambda * df;
+                        else if (row_ssum<CPT, NFIX>()) u1[m][k] = .5 * (SS[k * n + i] - lambda * df);
+                        else u1[m][k] = .5 * (u1[m][k] + u0[m][k] - lambda * df);
+                    }
                 }
             }
         }
@@ -602,10 +669,16 @@ __host__ __device__ __forceinline__ size_t pair_smem_bytes(int n, int ftsize, in
 
 // WC: pencils per box (2; 4 for z sweeps of x-y planes above 1 MB, whose 16-byte rows a plane
 // apart the memory system serves poorly: 32-byte rows, three CTAs per SM)
-template <int METHOD, int SLOPE, typename FT, int DIR, int NFIX = 0, int NS = 1, int WC = 2>
+// GEO == CYL_THETA_DIV / CYL_THETA_LAM: the theta sweep of cylindrical geometry (y = theta), the
+// flux difference divided by the pencil's radius or lambda divided by it first (cyl_dflux); the
+// radius of the pencil at radial index x and z index z is theta_radius(cyl, x, z).  FP64, one sweep.
+template <int METHOD, int SLOPE, typename FT, int DIR, int NFIX = 0, int NS = 1, int WC = 2, int GEO = CYL_NONE>
 __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : (WC == 4 ? 3 : 4))
-    sweep_pair_kernel(const __grid_constant__ CUtensorMap tm, PipeArgs a, FluidConsts<FT> c)
+    sweep_pair_kernel(const __grid_constant__ CUtensorMap tm, PipeArgs a, FluidConsts<FT> c, CylPencil cyl)
 {
+    static_assert(GEO == CYL_NONE || ((GEO == CYL_THETA_DIV || GEO == CYL_THETA_LAM) && DIR == 2 && NS == 1 &&
+                                      std::is_same<FT, double>::value),
+                  "theta pencils: y sweeps, one FP64 sweep");
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full;
     const int n = NFIX ? NFIX : a.n;
@@ -623,6 +696,12 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : (WC
     if (a.lambda.off()) return;  // a device timestep of 0: after the end time
     const double lambda = a.lambda.get();
     const bool leader = threadIdx.x == 0;
+    // the box's TMA copy needs a 128-byte aligned destination: a CTA whose tile is not aligned
+    // leaves its block undone and sets bit 2 of the wait flag instead of issuing the copy
+    if (smem_u32(T) & 127u) {
+        if (leader) atomicOr(a.err, 2u);
+        return;
+    }
     if (leader) {
         mbar_init(&full, 1);
         fence_mbar_init();
@@ -642,6 +721,11 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : (WC
         auto TI = [&](int k) { return (k * n + i) * WC + col; };
         double u0[5], u1[5];
         V5<FT> keep;
+        double rp = 0.0, lam = lambda;  // theta pencils: the pencil's radius and the lambda it takes
+        if constexpr (GEO != CYL_NONE) {
+            rp = theta_radius(cyl, (int)(b % a.npw) * WC + col, (int)(b / a.npw));
+            if (GEO == CYL_THETA_LAM) lam = lambda / rp;
+        }
 #pragma unroll
         for (int k = 0; k < 5; k++) u0[k] = act ? T[TI(slots[k])] : 1.0;
 #pragma unroll
@@ -690,9 +774,16 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : (WC
                 if (act) {
 #pragma unroll
                     for (int k = 0; k < 5; k++) {
-                        double df = (double)keep.a[k] - (double)PX[k * n + il];
-                        if (stage == 0) u1[k] = u0[k] - lambda * df;
-                        else u1[k] = .5 * (SS[k * n + i] - lambda * df);
+                        if constexpr (GEO == CYL_NONE) {
+                            double df = (double)keep.a[k] - (double)PX[k * n + il];
+                            if (stage == 0) u1[k] = u0[k] - lambda * df;
+                            else u1[k] = .5 * (SS[k * n + i] - lambda * df);
+                        } else {
+                            const double d = cyl_dflux<METHOD, GEO>(k, (double)keep.a[k], (double)PX[k * n + il], lam,
+                                                                    0.0, 0.0, rp, 0.0, 0.0, 0.0, c);
+                            if (stage == 0) u1[k] = u0[k] - d;
+                            else u1[k] = .5 * (SS[k * n + i] - d);
+                        }
                     }
                 }
             }
@@ -1145,45 +1236,6 @@ __host__ __device__ __forceinline__ size_t tile_smem_bytes(int Lc, size_t ft)
     const size_t TR = Lc + 8, TR1 = Lc + 4;
     return sizeof(double) * (5 * TR * W + 5 * TR1 * W + 2 * 5 * 4 * W) + ft * 3 * 5 * TR * W +
            (GEO == CYL_RADIAL ? sizeof(double) * TR * W : 0);
-}
-
-// lambda times the flux difference of one cell in cylindrical geometry, component by component
-// (local order rho, E, p_n, p_t1, p_t2; p_n = p_r in a radial sweep).  fR / fL: fluxes through the
-// cell's outer / inner face.  Radial: rc = the cell centre radius; HLLC weights the faces by
-// (rc +- dr/2) / rc and subtracts dr / (2 rc) times the cell's two face pressures from p_r's
-// difference (cudaFluidStep.cu:1164-1171, 1488-1495); HLL folds lambda into those factors and
-// subtracts the stage input's pressure (adiabatic) or rho c_iso^2 with rho the predicted density
-// (isothermal) times lambda dr / rc (1837-1842, 2270-2290, 2371-2391).  CYL_THETA_DIV divides by
-// the pencil radius; CYL_THETA_LAM gets lambda already divided by it.
-template <int METHOD, int GEO>
-__device__ __forceinline__ double cyl_dflux(int k, double fR, double fL, double lam, double rc, double dr,
-                                            double rpen, double psum, double p_hll, double rho1,
-                                            const FluidConsts<double> &c)
-{
-    if constexpr (GEO == CYL_RADIAL) {
-        if constexpr (METHOD == IB_METHOD_HLLC) {
-            const double cA = (rc - .5 * dr) / (rc);
-            const double cB = (rc + .5 * dr) / (rc);
-            const double cC = 0.5 * dr / rc;
-            double d = cB * fR - cA * fL;
-            if (k == 2) d = d - cC * psum;
-            return lam * d;
-        } else {
-            const double cA = lam * (rc - .5 * dr) / (rc);
-            const double cB = lam * (rc + .5 * dr) / (rc);
-            const double cC = lam * dr / rc;
-            double d = cB * fR - cA * fL;
-            if (k == 2) {
-                if (c.isotemp == -1) d = d - p_hll * cC;
-                else d = d - rho1 * c.isotempsq * cC;
-            }
-            return d;
-        }
-    } else if constexpr (GEO == CYL_THETA_DIV) {
-        return lam * (fR - fL) / rpen;
-    } else {
-        return lam * (fR - fL);
-    }
 }
 
 // One sweep of W pencils by one CTA.  colbase[c] = offset of pencil c's first cell, colok[c] =

@@ -1,5 +1,7 @@
-// ib_sweep_cyl.cu -- instantiates the cylindrical-geometry sweeps (HLL and HLLC, FP64): radial x
-// sweeps and theta y sweeps in the tile kernel with the geometry's update (ib_cyl.cuh).
+// ib_sweep_cyl.cu -- instantiates the cylindrical-geometry sweeps (HLL and HLLC, FP64) with the
+// geometry's update (ib_cyl.cuh): radial x sweeps in the row kernel (rows up to 512 cells) and
+// theta y sweeps in the pencil-pair kernel (pencils up to 256 cells, x even), the tile kernel
+// for other shapes.
 #include "ib_sweep_launch.cuh"
 
 namespace ib {

@@ -122,11 +122,14 @@ int launch_pipe(double *q, int64_t slab, const int grid[3], DevScalar lambda, co
 
 // Pencil-pair kernel (sweep_pair_kernel): y/z pencils of at most 256 cells or of 512 (the box
 // arrives as two rows of 256), x even; one CTA per block of two adjacent pencils.  Returns
-// IB_ERROR_NOIMPLEMENT (caller falls back) otherwise.
-template <int METHOD, int SLOPE, typename FT, int DIR, int NFIX = 0, int WC = 2>
+// IB_ERROR_NOIMPLEMENT (caller falls back) otherwise.  GEO: cylindrical theta pencils (y, one
+// sweep), with their radius rule in cyl.
+template <int METHOD, int SLOPE, typename FT, int DIR, int NFIX = 0, int WC = 2, int GEO = CYL_NONE>
 int launch_pair(double *q, int64_t slab, const int grid[3], DevScalar lambda, const FluidConsts<FT> &c, cudaStream_t st,
-                int nsweep)
+                int nsweep, CylPencil cyl = CylPencil{0.0, 0.0, 0, 0})
 {
+    static_assert(GEO == CYL_NONE || DIR == 2, "theta pencils run along y");
+    if (GEO != CYL_NONE && nsweep != 1) return IB_ERROR_NOIMPLEMENT;
     static_assert(DIR != 1, "x rows take the row kernel");
     static_assert(WC == 2 || (WC == 4 && NFIX != 512), "boxes of 2 pencils, or 4 of at most 256 cells");
     const int nx = grid[0], ny = grid[1], nz = grid[2];
@@ -153,8 +156,10 @@ int launch_pair(double *q, int64_t slab, const int grid[3], DevScalar lambda, co
     const int nt = (n + 31) / 32 * 32;
     const size_t shm = pair_smem_bytes(n, (int)sizeof(FT), WC);
     const int ns = (nsweep == 2) ? 2 : 1;
-    auto kern = ns == 2 ? &sweep_pair_kernel<METHOD, SLOPE, FT, DIR, NFIX, 2, WC>
-                        : &sweep_pair_kernel<METHOD, SLOPE, FT, DIR, NFIX, 1, WC>;
+    auto kern = &sweep_pair_kernel<METHOD, SLOPE, FT, DIR, NFIX, 1, WC, GEO>;
+    if constexpr (GEO == CYL_NONE) {
+        if (ns == 2) kern = &sweep_pair_kernel<METHOD, SLOPE, FT, DIR, NFIX, 2, WC>;
+    }
     static int attr_bytes[2] = {0, 0};
     if ((int)shm > attr_bytes[ns - 1]) {
         rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
@@ -162,7 +167,30 @@ int launch_pair(double *q, int64_t slab, const int grid[3], DevScalar lambda, co
         attr_bytes[ns - 1] = (int)shm;
     }
     PipeArgs a{n, npw, bh, nh, nblocks, lambda, err, tile_wait_limit()};
-    kern<<<(unsigned)nblocks, nt, shm, st>>>(tm, a, c);
+    kern<<<(unsigned)nblocks, nt, shm, st>>>(tm, a, c, cyl);
+    return check_launch();
+}
+
+// Radial rows (cylindrical x sweeps) of at most 512 cells: the row kernel with the radial update,
+// one CTA per row.  Returns IB_ERROR_NOIMPLEMENT (caller falls back) for longer rows.
+template <int METHOD, int SLOPE>
+int launch_row_radial(double *q, int64_t slab, const int grid[3], DevScalar lambda, const FluidConsts<double> &c,
+                      cudaStream_t st, const CylPencil &cyl)
+{
+    const int nx = grid[0];
+    if (nx > 512) return IB_ERROR_NOIMPLEMENT;
+    SweepArgs a{q, slab, grid[0], grid[1], grid[2], lambda, cyl.rin, cyl.dr};
+    const int64_t rows = (int64_t)grid[1] * grid[2];
+    const int nt = ((nx + 31) / 32) * 32;
+    const size_t shm = (size_t)10 * nx * sizeof(double) + (size_t)40 * nx;  // two planes, the SSPRK sum
+    auto kern = sweep_row_kernel<METHOD, SLOPE, double, 1, 0, 1, CYL_RADIAL>;
+    static int attr_bytes = 0;
+    if ((int)shm > attr_bytes) {
+        int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        if (rc) return rc;
+        attr_bytes = (int)shm;
+    }
+    kern<<<(unsigned)rows, nt, shm, st>>>(a, c);
     return check_launch();
 }
 
@@ -441,17 +469,30 @@ int launch_sweep_slope(int slope, int dir, double *q, int64_t slab, const int gr
     }
 }
 
-// Cylindrical sweeps (radial x, theta y) run in the tile kernel with the geometry's update, FP64
+// Cylindrical sweeps, FP64: radial x rows of up to 512 cells in the row kernel and theta y pencils
+// of up to 256 cells (x even) in the pencil-pair kernel, each with the geometry's update; other
+// shapes in the tile kernel with the same update
 template <int METHOD, int SLOPE>
 int launch_sweep_cyl_t(double *q, int64_t slab, const int grid[3], DevScalar lambda, const FluidConsts<double> &c,
                        cudaStream_t st, const CylSweep &cs)
 {
+    static const bool fast = [] {
+        const char *e = getenv("IMOGEN_B200_CYLFAST");  // 0 = the tile kernel for every cylindrical sweep
+        return !(e && e[0] == '0');
+    }();
+    int rc = IB_ERROR_NOIMPLEMENT;
     switch (cs.kind) {
     case CYL_RADIAL:
+        if (fast) rc = launch_row_radial<METHOD, SLOPE>(q, slab, grid, lambda, c, st, cs.pencil);
+        if (rc != IB_ERROR_NOIMPLEMENT) return rc;
         return launch_tile_dw<METHOD, SLOPE, double, 1, 1, CYL_RADIAL>(q, slab, grid, lambda, c, st, 248, cs.pencil);
     case CYL_THETA_DIV:
+        if (fast) rc = launch_pair<METHOD, SLOPE, double, 2, 0, 2, CYL_THETA_DIV>(q, slab, grid, lambda, c, st, 1, cs.pencil);
+        if (rc != IB_ERROR_NOIMPLEMENT) return rc;
         return launch_tile_dw<METHOD, SLOPE, double, 2, 4, CYL_THETA_DIV>(q, slab, grid, lambda, c, st, 56, cs.pencil);
     case CYL_THETA_LAM:
+        if (fast) rc = launch_pair<METHOD, SLOPE, double, 2, 0, 2, CYL_THETA_LAM>(q, slab, grid, lambda, c, st, 1, cs.pencil);
+        if (rc != IB_ERROR_NOIMPLEMENT) return rc;
         return launch_tile_dw<METHOD, SLOPE, double, 2, 4, CYL_THETA_LAM>(q, slab, grid, lambda, c, st, 56, cs.pencil);
     default: return IB_ERROR_INVALID_ARGS;
     }

@@ -216,8 +216,9 @@ IB_API long long ib_launch_count(void);
 /* Health of the TMA-fed sweep kernels on the current device (no reference counterpart: the
  * reference has no asynchronous copies).  Their waits for a tile are bounded; a wait that runs
  * out makes the kernel leave early and sets a flag, which this call reads (synchronising with
- * the device): 0 = no wait ran out, 1 = one did and the state of that sweep is invalid, < 0 =
- * status code.  clear != 0 resets the flag. */
+ * the device): 0 = no wait ran out, bit 1 = one did and the state of that sweep is invalid,
+ * bit 2 = a pencil-pair kernel found its shared-memory tile unaligned for the TMA copy and left
+ * its block undone, < 0 = status code.  clear != 0 resets the flag. */
 IB_API int ib_device_wait_status(int clear);
 
 /* For failure-detection tests (no reference counterpart): how many times the TMA-fed sweep

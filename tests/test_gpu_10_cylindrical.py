@@ -28,7 +28,9 @@ def _n(shape):
 
 @pytest.mark.parametrize("variant", ["strict", "product"])
 @pytest.mark.parametrize("geometric", [False, True])
-@pytest.mark.parametrize("shape", [(32, 24, 6), (32, 24, 1), (20, 9, 5)])
+# radial rows up to 512 cells take the row kernel, theta pencils with x even the pencil-pair
+# kernel; (21, 9, 5) sends theta to the tile kernel (x odd), (520, 6, 1) the radial rows
+@pytest.mark.parametrize("shape", [(32, 24, 6), (32, 24, 1), (20, 9, 5), (21, 9, 5), (520, 6, 1)])
 @pytest.mark.parametrize("method,c_iso", [(2, -1.0), (1, -1.0), (1, 0.8), (3, -1.0)])
 def test_cyl_sweeps_vs_oracle(cuda, ib, po, variant, geometric, shape, method, c_iso):
     n = _n(shape)
