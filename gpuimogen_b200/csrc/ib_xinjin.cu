@@ -296,14 +296,20 @@ struct XjPairArgs {
     double gamma, minmass, mintemp;
     unsigned int *err;
     uint32_t spin;
+    CylPencil cyl;  // cylindrical theta pencils (GEO): the radius rule
 };
 
 __host__ __device__ __forceinline__ size_t xj_box_bytes(int n, int wc) { return ((size_t)40 * n * wc + 127) / 128 * 128; }
 
-template <int FLIM, int DIR, int NFIX, int WC>
+// GEO == CYL_THETA_DIV / CYL_THETA_LAM: cylindrical theta pencils (y), the update's flux
+// difference divided by the pencil's radius or the stage's lambda divided by it, as in
+// xj_pencil_kernel.
+template <int FLIM, int DIR, int NFIX, int WC, int GEO = CYL_NONE>
 __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
     xj_pair_kernel(const __grid_constant__ CUtensorMap tm, XjPairArgs a)
 {
+    static_assert(GEO == CYL_NONE || ((GEO == CYL_THETA_DIV || GEO == CYL_THETA_LAM) && DIR == 2),
+                  "theta pencils run along y");
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full;
     __shared__ double red[32];
@@ -320,6 +326,12 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
     if (a.lambda.off()) return;  // a device timestep of 0: after the end time
     const double lambda = a.lambda.get();
     const bool leader = threadIdx.x == 0;
+    // the box's TMA copy needs a 128-byte aligned destination: a CTA whose tile is not aligned
+    // leaves its block undone and sets bit 2 of the wait flag instead of issuing the copy
+    if (smem_u32(T) & 127u) {
+        if (leader) atomicOr(a.err, 2u);
+        return;
+    }
     if (leader) {
         mbar_init(&full, 1);
         fence_mbar_init();
@@ -341,6 +353,7 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
 #ifndef IB_STRICT_ARITH
         double rinv = 1.0;
 #endif
+        const double rpen = (GEO != CYL_NONE) ? theta_radius(a.cyl, (int)(b % a.npw) * WC + col, (int)(b / a.npw)) : 1.0;
 #pragma unroll
         for (int k = 0; k < 5; k++) u0[k] = act ? T[TI(k)] : 1.0;
 #pragma unroll
@@ -406,8 +419,16 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
             if (act) {
                 double pr[5];
 #pragma unroll
-                for (int k = 0; k < 5; k++)
-                    pr[k] = u0[k] - lam * (Rb[k * n + i] - Rb[k * n + il] - Lb[k * n + ir] + Lb[k * n + i]);
+                for (int k = 0; k < 5; k++) {
+                    if constexpr (GEO == CYL_NONE) {
+                        pr[k] = u0[k] - lam * (Rb[k * n + i] - Rb[k * n + il] - Lb[k * n + ir] + Lb[k * n + i]);
+                    } else if constexpr (GEO == CYL_THETA_DIV) {
+                        pr[k] = u0[k] - lam * (Rb[k * n + i] - Rb[k * n + il] - Lb[k * n + ir] + Lb[k * n + i]) / rpen;
+                    } else {
+                        const double lr = lam / rpen;
+                        pr[k] = u0[k] - lr * (Rb[k * n + i] - Rb[k * n + il] - Lb[k * n + ir] + Lb[k * n + i]);
+                    }
+                }
                 double p0 = pr[0], p1 = pr[1];
                 const double p2 = pr[2], p3 = pr[3], p4 = pr[4];
                 p0 = (p0 < a.minmass) ? a.minmass : p0;
@@ -439,9 +460,9 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
 // Returns IB_ERROR_NOIMPLEMENT (the caller falls back to xj_pencil_kernel) where TMA's rules or
 // the kernel's sizes do not hold: nx a multiple of WC, 16-byte aligned base and slab pitch, pencils
 // of up to 256 cells or of 512.
-template <int FLIM, int DIR, int NFIX, int WC>
+template <int FLIM, int DIR, int NFIX, int WC, int GEO = CYL_NONE>
 static int launch_xj_pair(double *q, int64_t slab, const int grid[3], DevScalar lambda, double gamma, double rho_min,
-                          double mintemp, cudaStream_t st)
+                          double mintemp, cudaStream_t st, CylPencil cyl = CylPencil{0.0, 0.0, 0, 0})
 {
     const int nx = grid[0], ny = grid[1], nz = grid[2];
     const int n = grid[DIR - 1];
@@ -467,14 +488,30 @@ static int launch_xj_pair(double *q, int64_t slab, const int grid[3], DevScalar 
     const size_t shm = xj_box_bytes(n, WC) + (size_t)80 * n;
     static int attr_bytes = 0;
     if ((int)shm > attr_bytes) {
-        rc = check_cuda(cudaFuncSetAttribute(xj_pair_kernel<FLIM, DIR, NFIX, WC>,
+        rc = check_cuda(cudaFuncSetAttribute(xj_pair_kernel<FLIM, DIR, NFIX, WC, GEO>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
         if (rc) return rc;
         attr_bytes = (int)shm;
     }
-    XjPairArgs a{n, npw, lambda, gamma, rho_min, mintemp, err, tile_wait_limit()};
-    xj_pair_kernel<FLIM, DIR, NFIX, WC><<<(unsigned)nblocks, nt, shm, st>>>(tm, a);
+    XjPairArgs a{n, npw, lambda, gamma, rho_min, mintemp, err, tile_wait_limit(), cyl};
+    xj_pair_kernel<FLIM, DIR, NFIX, WC, GEO><<<(unsigned)nblocks, nt, shm, st>>>(tm, a);
     return check_launch();
+}
+
+// Cylindrical theta pencils (y) of up to 256 cells in the pencil-box kernel
+template <int FLIM>
+static int launch_xj_pair_theta(int geo, double *q, int64_t slab, const int grid[3], DevScalar lambda, double gamma,
+                                double rho_min, double mintemp, cudaStream_t st, const CylPencil &cyl)
+{
+    const int n = grid[1];
+    if (geo == CYL_THETA_DIV) {
+        if (n == 256)
+            return launch_xj_pair<FLIM, 2, 256, 2, CYL_THETA_DIV>(q, slab, grid, lambda, gamma, rho_min, mintemp, st, cyl);
+        return launch_xj_pair<FLIM, 2, 0, 2, CYL_THETA_DIV>(q, slab, grid, lambda, gamma, rho_min, mintemp, st, cyl);
+    }
+    if (n == 256)
+        return launch_xj_pair<FLIM, 2, 256, 2, CYL_THETA_LAM>(q, slab, grid, lambda, gamma, rho_min, mintemp, st, cyl);
+    return launch_xj_pair<FLIM, 2, 0, 2, CYL_THETA_LAM>(q, slab, grid, lambda, gamma, rho_min, mintemp, st, cyl);
 }
 
 template <int FLIM>
@@ -513,6 +550,18 @@ int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3
         case IB_FLUX_MINMOD: rc = launch_xj_pair_dir<IB_FLUX_MINMOD>(dir, q, slab, grid, lambda, gamma, rho_min, mt, st); break;
         case IB_FLUX_SUPERBEE: rc = launch_xj_pair_dir<IB_FLUX_SUPERBEE>(dir, q, slab, grid, lambda, gamma, rho_min, mt, st); break;
         default: rc = launch_xj_pair_dir<IB_FLUX_ZERO>(dir, q, slab, grid, lambda, gamma, rho_min, mt, st); break;
+        }
+        if (rc != IB_ERROR_NOIMPLEMENT) return rc;
+    }
+    if (xj_pair && dir == 2 && (geo == CYL_THETA_DIV || geo == CYL_THETA_LAM)) {
+        const double mt = 1e-5 / (gamma - 1);
+        int rc;
+        switch (flim) {
+        case IB_FLUX_OSPRE: rc = launch_xj_pair_theta<IB_FLUX_OSPRE>(geo, q, slab, grid, lambda, gamma, rho_min, mt, st, cp); break;
+        case IB_FLUX_VANLEER: rc = launch_xj_pair_theta<IB_FLUX_VANLEER>(geo, q, slab, grid, lambda, gamma, rho_min, mt, st, cp); break;
+        case IB_FLUX_MINMOD: rc = launch_xj_pair_theta<IB_FLUX_MINMOD>(geo, q, slab, grid, lambda, gamma, rho_min, mt, st, cp); break;
+        case IB_FLUX_SUPERBEE: rc = launch_xj_pair_theta<IB_FLUX_SUPERBEE>(geo, q, slab, grid, lambda, gamma, rho_min, mt, st, cp); break;
+        default: rc = launch_xj_pair_theta<IB_FLUX_ZERO>(geo, q, slab, grid, lambda, gamma, rho_min, mt, st, cp); break;
         }
         if (rc != IB_ERROR_NOIMPLEMENT) return rc;
     }
