@@ -77,8 +77,11 @@ double *Scratch::cfl_partial(int nblocks)
         if (partial_) cudaFree(partial_);
         partial_ = nullptr;
         partial_n_ = 0;
-        if (cudaMalloc(&partial_, sizeof(double) * nblocks) != cudaSuccess) return nullptr;
-        partial_n_ = nblocks;
+        // room for every grid the CFL launch sizes (at most 8 resident 256-thread blocks per SM),
+        // so the array is never replaced under a CUDA graph that captured its address
+        const int cap = std::max(nblocks, 8 * num_sms());
+        if (cudaMalloc(&partial_, sizeof(double) * cap) != cudaSuccess) return nullptr;
+        partial_n_ = cap;
     }
     return partial_;
 }

@@ -24,6 +24,11 @@ __global__ void soundspeed_kernel(const double *__restrict__ q, int64_t slab, in
     }
 }
 
+// The cells one pass of the CFL loop reads: U cells a grid stride apart, every load issued before
+// the arithmetic, so that a thread keeps U cells' loads in flight (the minimum does not depend on
+// the order in which the cells are visited).
+constexpr int kCflUnroll = 2;
+
 template <int SIM, bool XJ, bool FUSED, bool CYL = false>
 __global__ void __launch_bounds__(256) cfl_kernel(const double *__restrict__ q, const double *__restrict__ cs_in,
                                                   int64_t slab, int64_t n, double gg1, double hmin, double hx,
@@ -32,20 +37,35 @@ __global__ void __launch_bounds__(256) cfl_kernel(const double *__restrict__ q, 
                                                   int nx = 1, double rin = 0.0)
 {
     double tmin = 1e37;
-    for (int64_t x = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; x < n; x += (int64_t)blockDim.x * gridDim.x) {
-        double rho = q[x], px = q[x + 2 * slab], py = 0, pz = 0;
-        if (SIM > 1 || XJ) py = q[x + 3 * slab];
-        if (SIM > 2 || XJ) pz = q[x + 4 * slab];
-        double cs;
-        if constexpr (FUSED) {
-            cs = soundspeed_cell(rho, q[x + slab], px, q[x + 3 * slab], q[x + 4 * slab], gg1);
-        } else {
-            cs = cs_in[x];
+    const int64_t stride = (int64_t)blockDim.x * gridDim.x;
+    constexpr bool NEED_E = FUSED, NEED_PY = FUSED || SIM > 1 || XJ, NEED_PZ = FUSED || SIM > 2 || XJ;
+    int64_t x0 = threadIdx.x + (int64_t)blockIdx.x * blockDim.x;
+    for (; x0 < n; x0 += kCflUnroll * stride) {
+        double rho[kCflUnroll], E[kCflUnroll], px[kCflUnroll], py[kCflUnroll], pz[kCflUnroll], cs[kCflUnroll];
+#pragma unroll
+        for (int u = 0; u < kCflUnroll; u++) {
+            const int64_t x = x0 + u * stride;
+            const bool in = (u == 0) || x < n;
+            rho[u] = in ? q[x] : 1.0;
+            px[u] = in ? q[x + 2 * slab] : 0.0;
+            E[u] = (NEED_E && in) ? q[x + slab] : 0.0;
+            py[u] = (NEED_PY && in) ? q[x + 3 * slab] : 0.0;
+            pz[u] = (NEED_PZ && in) ? q[x + 4 * slab] : 0.0;
+            if constexpr (!FUSED) cs[u] = in ? cs_in[x] : 0.0;
         }
-        if constexpr (CYL)
-            tmin = min_keep(tmin, cfl_cell_cyl<SIM, XJ>(rho, px, py, pz, cs, hmin, hx, hy, hz, rin, (int)(x % nx)));
-        else
-            tmin = min_keep(tmin, cfl_cell<SIM, XJ>(rho, px, py, pz, cs, hmin, hx, hy, hz));
+#pragma unroll
+        for (int u = 0; u < kCflUnroll; u++) {
+            const int64_t x = x0 + u * stride;
+            if (u > 0 && x >= n) break;
+            if constexpr (FUSED) cs[u] = soundspeed_cell(rho[u], E[u], px[u], py[u], pz[u], gg1);
+            // the cell's own velocity terms: a sweep dimension the grid lacks contributes nothing
+            const double vy = (SIM > 1 || XJ) ? py[u] : 0.0, vz = (SIM > 2 || XJ) ? pz[u] : 0.0;
+            if constexpr (CYL)
+                tmin = min_keep(tmin, cfl_cell_cyl<SIM, XJ>(rho[u], px[u], vy, vz, cs[u], hmin, hx, hy, hz, rin,
+                                                            (int)(x % nx)));
+            else
+                tmin = min_keep(tmin, cfl_cell<SIM, XJ>(rho[u], px[u], vy, vz, cs[u], hmin, hx, hy, hz));
+        }
     }
     // warp then block reduction
 #pragma unroll
@@ -87,6 +107,20 @@ __global__ void __launch_bounds__(256) cfl_kernel(const double *__restrict__ q, 
     }
 }
 
+// Blocks of the allocating CFL launch: as many as are resident at once (the loop strides over the
+// cells, so a second wave would only add a tail), at most one per 256 cells.
+template <int S, bool X, bool F, bool C>
+static int cfl_grid(int64_t n)
+{
+    static const int per_sm = [] {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, cfl_kernel<S, X, F, C>, 256, 0) != cudaSuccess || b < 1)
+            b = 4;
+        return b;
+    }();
+    return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)per_sm * num_sms()));
+}
+
 int launch_cfl(const double *q, const double *cs, int64_t slab, const int grid[3], const ib_geometry *geo,
                int method, double gamma, double *tau_dev, cudaStream_t st)
 {
@@ -105,18 +139,20 @@ int launch_cfl(const double *q, const double *cs, int64_t slab, const int grid[3
         if (sim > 2 && geo->h[2] < hmin) hmin = geo->h[2];
     }
     int64_t n = (int64_t)grid[0] * grid[1] * grid[2];
-    int nb = (int)std::min<int64_t>((n + 255) / 256, (int64_t)4 * num_sms());
-    if (nb < 1) nb = 1;
     Scratch &sc = scratch();
-    double *partial = sc.cfl_partial(nb);
     unsigned int *counter = sc.cfl_counter();
-    if (!partial || !counter) return IB_ERROR_NOMEM;
+    if (!counter) return IB_ERROR_NOMEM;
     int halve = (method == IB_METHOD_HLL || method == IB_METHOD_HLLC) ? 1 : 0;
     double gg1 = gamma * (gamma - 1);
     bool fused = (cs == nullptr);
 #define IB_CFL_LAUNCH_C(S, X, F, C)                                                                          \
-    cfl_kernel<S, X, F, C><<<nb, 256, 0, st>>>(q, cs, slab, n, gg1, hmin, geo->h[0], geo->h[1], geo->h[2], halve, \
-                                               partial, counter, tau_dev, grid[0], geo->r_inner)
+    do {                                                                                                     \
+        const int nb = cfl_grid<S, X, F, C>(n);                                                              \
+        double *partial = sc.cfl_partial(nb);                                                                \
+        if (!partial) return IB_ERROR_NOMEM;                                                                 \
+        cfl_kernel<S, X, F, C><<<nb, 256, 0, st>>>(q, cs, slab, n, gg1, hmin, geo->h[0], geo->h[1], geo->h[2],  \
+                                                   halve, partial, counter, tau_dev, grid[0], geo->r_inner);    \
+    } while (0)
 #define IB_CFL_LAUNCH(S, X, F) IB_CFL_LAUNCH_C(S, X, F, false)
     if (cyl && fused) {
         if (xj) {
