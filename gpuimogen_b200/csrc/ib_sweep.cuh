@@ -225,18 +225,35 @@ __device__ __forceinline__ double cyl_dflux(int k, double fR, double fL, double 
                                             double rpen, double psum, double p_hll, double rho1,
                                             const FluidConsts<double> &c)
 {
+    // The product build multiplies by one reciprocal of the radius where the reference divides
+    // (one division per cell or pencil instead of three or five); the strict build divides.
     if constexpr (GEO == CYL_RADIAL) {
+#ifndef IB_STRICT_ARITH
+        const double ri = 1.0 / rc;
+#endif
         if constexpr (METHOD == IB_METHOD_HLLC) {
+#ifdef IB_STRICT_ARITH
             const double cA = (rc - .5 * dr) / (rc);
             const double cB = (rc + .5 * dr) / (rc);
             const double cC = 0.5 * dr / rc;
+#else
+            const double cA = (rc - .5 * dr) * ri;
+            const double cB = (rc + .5 * dr) * ri;
+            const double cC = 0.5 * dr * ri;
+#endif
             double d = cB * fR - cA * fL;
             if (k == 2) d = d - cC * psum;
             return lam * d;
         } else {
+#ifdef IB_STRICT_ARITH
             const double cA = lam * (rc - .5 * dr) / (rc);
             const double cB = lam * (rc + .5 * dr) / (rc);
             const double cC = lam * dr / rc;
+#else
+            const double cA = lam * (rc - .5 * dr) * ri;
+            const double cB = lam * (rc + .5 * dr) * ri;
+            const double cC = lam * dr * ri;
+#endif
             double d = cB * fR - cA * fL;
             if (k == 2) {
                 if (c.isotemp == -1) d = d - p_hll * cC;
@@ -245,7 +262,11 @@ __device__ __forceinline__ double cyl_dflux(int k, double fR, double fL, double 
             return d;
         }
     } else if constexpr (GEO == CYL_THETA_DIV) {
+#ifdef IB_STRICT_ARITH
         return lam * (fR - fL) / rpen;
+#else
+        return lam * (fR - fL) * (1.0 / rpen);
+#endif
     } else {
         return lam * (fR - fL);
     }

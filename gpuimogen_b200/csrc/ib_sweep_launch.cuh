@@ -487,11 +487,18 @@ int launch_sweep_cyl_t(double *q, int64_t slab, const int grid[3], DevScalar lam
         if (rc != IB_ERROR_NOIMPLEMENT) return rc;
         return launch_tile_dw<METHOD, SLOPE, double, 1, 1, CYL_RADIAL>(q, slab, grid, lambda, c, st, 248, cs.pencil);
     case CYL_THETA_DIV:
-        if (fast) rc = launch_pair<METHOD, SLOPE, double, 2, 0, 2, CYL_THETA_DIV>(q, slab, grid, lambda, c, st, 1, cs.pencil);
+        // 256-cell pencils get the length at compile time (fewer registers for indexing, no spills)
+        if (fast && grid[1] == 256)
+            rc = launch_pair<METHOD, SLOPE, double, 2, 256, 2, CYL_THETA_DIV>(q, slab, grid, lambda, c, st, 1, cs.pencil);
+        else if (fast)
+            rc = launch_pair<METHOD, SLOPE, double, 2, 0, 2, CYL_THETA_DIV>(q, slab, grid, lambda, c, st, 1, cs.pencil);
         if (rc != IB_ERROR_NOIMPLEMENT) return rc;
         return launch_tile_dw<METHOD, SLOPE, double, 2, 4, CYL_THETA_DIV>(q, slab, grid, lambda, c, st, 56, cs.pencil);
     case CYL_THETA_LAM:
-        if (fast) rc = launch_pair<METHOD, SLOPE, double, 2, 0, 2, CYL_THETA_LAM>(q, slab, grid, lambda, c, st, 1, cs.pencil);
+        if (fast && grid[1] == 256)
+            rc = launch_pair<METHOD, SLOPE, double, 2, 256, 2, CYL_THETA_LAM>(q, slab, grid, lambda, c, st, 1, cs.pencil);
+        else if (fast)
+            rc = launch_pair<METHOD, SLOPE, double, 2, 0, 2, CYL_THETA_LAM>(q, slab, grid, lambda, c, st, 1, cs.pencil);
         if (rc != IB_ERROR_NOIMPLEMENT) return rc;
         return launch_tile_dw<METHOD, SLOPE, double, 2, 4, CYL_THETA_LAM>(q, slab, grid, lambda, c, st, 56, cs.pencil);
     default: return IB_ERROR_INVALID_ARGS;

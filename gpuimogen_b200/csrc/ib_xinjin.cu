@@ -245,15 +245,27 @@ __global__ void __launch_bounds__(1024) xj_pencil_kernel(double *q, int64_t slab
                     if constexpr (GEO == CYL_NONE) {
                         pr[k] = b - lam * (Rb[IX(k, i)] - Rb[IX(k, il)] - Lb[IX(k, ir)] + Lb[IX(k, i)]);
                     } else if constexpr (GEO == CYL_THETA_DIV) {
+#ifdef IB_STRICT_ARITH
                         pr[k] = b - lam * (Rb[IX(k, i)] - Rb[IX(k, il)] - Lb[IX(k, ir)] + Lb[IX(k, i)]) / rpen;
+#else
+                        // the product build multiplies by the radius' reciprocal (one division)
+                        pr[k] = b - lam * (Rb[IX(k, i)] - Rb[IX(k, il)] - Lb[IX(k, ir)] + Lb[IX(k, i)]) * (1.0 / rpen);
+#endif
                     } else if constexpr (GEO == CYL_THETA_LAM) {
                         const double lr = lam / rpen;
                         pr[k] = b - lr * (Rb[IX(k, i)] - Rb[IX(k, il)] - Lb[IX(k, ir)] + Lb[IX(k, i)]);
                     } else {
                         const double rc = cyl.rin + i * cyl.dr;
+#ifdef IB_STRICT_ARITH
                         const double cA = (rc - .5 * cyl.dr) / (rc);
                         const double cB = (rc + .5 * cyl.dr) / (rc);
                         const double cC = 2.0 * cyl.dr / rc;
+#else
+                        const double ri = 1.0 / rc;  // the product build: one division per cell
+                        const double cA = (rc - .5 * cyl.dr) * ri;
+                        const double cB = (rc + .5 * cyl.dr) * ri;
+                        const double cC = 2.0 * cyl.dr * ri;
+#endif
                         pr[k] = b - lam * (cB * Rb[IX(k, i)] - cA * Rb[IX(k, il)] - cB * Lb[IX(k, ir)] + cA * Lb[IX(k, i)]);
                         if (k == 2) pr[k] += lam * cC * pcell[m];
                     }
@@ -423,7 +435,12 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
                     if constexpr (GEO == CYL_NONE) {
                         pr[k] = u0[k] - lam * (Rb[k * n + i] - Rb[k * n + il] - Lb[k * n + ir] + Lb[k * n + i]);
                     } else if constexpr (GEO == CYL_THETA_DIV) {
+#ifdef IB_STRICT_ARITH
                         pr[k] = u0[k] - lam * (Rb[k * n + i] - Rb[k * n + il] - Lb[k * n + ir] + Lb[k * n + i]) / rpen;
+#else
+                        pr[k] = u0[k] - lam * (Rb[k * n + i] - Rb[k * n + il] - Lb[k * n + ir] + Lb[k * n + i]) *
+                                            (1.0 / rpen);
+#endif
                     } else {
                         const double lr = lam / rpen;
                         pr[k] = u0[k] - lr * (Rb[k * n + i] - Rb[k * n + il] - Lb[k * n + ir] + Lb[k * n + i]);
