@@ -14,7 +14,7 @@ from helpers import bits_equal, first_diff, product_close
 
 pytestmark = pytest.mark.gpu
 
-SIZES = [9, 13, 40, 120, 255, 256, 300, 600, 1000]
+SIZES = [9, 13, 40, 120, 255, 256, 300, 600, 1000, 2049, 4096]
 
 
 def oracle_problem(po, q, h, gamma, cfl, t_end, itermax, method, slope, bc):
