@@ -213,7 +213,9 @@ def case_drag(args):
 
 def case_all(args):
     """Every kind of kernel of the library once: KH at n^3 (default 160^3, 164 MB of state) for
-    the sweeps of every method and precision, CFL, freezeAndPtot and the outflow fill; KH on
+    the sweeps of every method and precision, CFL, freezeAndPtot and the outflow fill; the
+    rotating annulus at the same size in cylindrical geometry (one complete HLLC iteration, the r
+    and theta sweeps of HLL and Xin-Jin); KH on
     512 x 512 x 8 (z sweeps of 2 MB planes: the wide-block kernels) and 2048 x 2048 x 1 (the
     chunked pipeline and its halo copy); the 2-D gas-dust state at --m^2 for the drag kernels
     (ETDRK2 included) and the learned drag; a 592-problem Riemann ensemble (4 iterations); the
@@ -231,6 +233,19 @@ def case_all(args):
         num = ib.numerics(slope="mc", precision=prec)
         for d in (1, 2, 3):
             ib.cudaFluidStep(fl, geo, [dt, 1, GAMMA, 1e-5, method, d], num)
+    # cylindrical geometry (x = r, y = theta) on the rotating annulus: one complete HLLC iteration
+    # (cylindrical CFL, cylinder source, radial, theta and z sweeps), then the r and theta sweeps of
+    # HLL and Xin-Jin
+    hc = [1.0 / shape[0], 2 * math.pi / shape[1], 1.0 / shape[2]]
+    qc = problems.rotating_annulus(shape, r_inner=1.0, dr=hc[0], gamma=GAMMA, seed=1)
+    gc = ib.Geometry(shape, h=hc, cylindrical=True, r_inner=1.0)
+    fcyl = ib.Fluid(shape, q=torch.from_numpy(qc).cuda(), gamma=GAMMA)
+    ib.run_iteration([fcyl], gc, ib.TimeManager(cfl=CFL), 2)
+    for method in (1, 3):
+        fcyl = ib.Fluid(shape, q=torch.from_numpy(qc).cuda(), gamma=GAMMA)
+        for d in (1, 2):
+            ib.cudaFluidStep(fcyl, gc, [dt, 1, GAMMA, 1e-5, method, d], ib.numerics(slope="mc"))
+    del fcyl
     shp = (512, 512, 8)
     qw = problems.kelvin_helmholtz(shp, seed=2)
     for prec in ("fp64", "fp32flux"):
@@ -254,7 +269,7 @@ def case_all(args):
     run.reset()
     ld.drag_step(run.gas, run.dust, model, 4e-5)
     ens = ensemble.RiemannEnsemble.random(592, seed=2)
-    ens.run(t_end=0.1, itermax=4, tuning={"threads": 512, "chunk": 504})
+    ens.run(t_end=0.1, itermax=4, tuning={"threads": 256, "chunk": 248})
     torch.cuda.synchronize()
     print("case all done")
 

@@ -53,6 +53,15 @@ int num_sms()
 
 static std::atomic<long long> g_tile_wait_limit{-1};
 
+int pair_min_cells()
+{
+    static const int v = [] {
+        const char *e = getenv("IMOGEN_B200_PAIRMIN");
+        return e ? atoi(e) : 64;
+    }();
+    return v;
+}
+
 uint32_t tile_wait_limit()
 {
     const long long v = g_tile_wait_limit.load(std::memory_order_relaxed);

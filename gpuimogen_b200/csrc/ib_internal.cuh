@@ -17,6 +17,10 @@ int check_launch();
 int num_sms();
 // Poll limit of the TMA-fed kernels' tile waits (IB_TMA_SPIN_LIMIT unless ib_setTileWaitLimit set one).
 uint32_t tile_wait_limit();
+// Shortest y/z pencil (cells) the pencil-box kernels take: a CTA of theirs has one thread per cell
+// and runs its pencils one after the other, so shorter pencils go to kernels that pack several
+// pencils into a block (IMOGEN_B200_PAIRMIN overrides).
+int pair_min_cells();
 
 // Reusable per-device scratch: grown on demand, never shrunk, freed at process exit.  The
 // reference allocates and frees a 6-slab temporary per call (cudaFluidStep.cu:508-513); the

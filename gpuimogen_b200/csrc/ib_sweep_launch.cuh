@@ -312,11 +312,13 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], DevScala
         // per 256-thread CTA, four CTAs per SM: 256^3 FP64 y 0.93 -> 0.76 ms, FP32 flux
         // 0.52 -> 0.44 ms; 512-cell y pencils 4.01 -> 3.60 ms at 512 x 512 x 256) rather than the
         // persistent pipeline, which remains for other lengths when the pair kernel declines
-        constexpr bool pair = true, pair512 = true;
+        // (pencils shorter than pair_min_cells() leave most of a pencil-pair CTA idle: pipeline)
+        const bool pair = n >= pair_min_cells();
+        constexpr bool pair512 = true;
         // z of x-y planes above 1 MB, FP64: 4-pencil boxes through the pencil-pair kernel (512 x 512
         // x 256: z 3.96 -> 3.58 ms); FP32 flux keeps its 8-column wide blocks (2.43 ms against 2.77
         // for the 4-pencil boxes)
-        constexpr bool wide4 = sizeof(FT) == 8;
+        const bool wide4 = sizeof(FT) == 8 && pair;
         static const int wide8 = [] {
             const char *e = getenv("IMOGEN_B200_WIDE8");  // 0 = 4-column blocks for wide z planes
             return (e && e[0] == '0') ? 0 : 1;
@@ -476,10 +478,12 @@ template <int METHOD, int SLOPE>
 int launch_sweep_cyl_t(double *q, int64_t slab, const int grid[3], DevScalar lambda, const FluidConsts<double> &c,
                        cudaStream_t st, const CylSweep &cs)
 {
-    static const bool fast = [] {
+    static const bool fast_env = [] {
         const char *e = getenv("IMOGEN_B200_CYLFAST");  // 0 = the tile kernel for every cylindrical sweep
         return !(e && e[0] == '0');
     }();
+    // theta pencils shorter than pair_min_cells() take the tile kernel (several pencils a CTA)
+    const bool fast = fast_env && (cs.kind == CYL_RADIAL || grid[1] >= pair_min_cells());
     int rc = IB_ERROR_NOIMPLEMENT;
     switch (cs.kind) {
     case CYL_RADIAL:

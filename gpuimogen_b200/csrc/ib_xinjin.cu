@@ -558,7 +558,8 @@ int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3
         const char *e = getenv("IMOGEN_B200_XJPAIR");
         return !(e && e[0] == '0');
     }();
-    if (xj_pair && dir > 1 && geo == CYL_NONE) {
+    const bool long_pencils = grid[dir - 1] >= pair_min_cells();
+    if (xj_pair && long_pencils && dir > 1 && geo == CYL_NONE) {
         const double mt = 1e-5 / (gamma - 1);
         int rc;
         switch (flim) {
@@ -570,7 +571,7 @@ int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3
         }
         if (rc != IB_ERROR_NOIMPLEMENT) return rc;
     }
-    if (xj_pair && dir == 2 && (geo == CYL_THETA_DIV || geo == CYL_THETA_LAM)) {
+    if (xj_pair && long_pencils && dir == 2 && (geo == CYL_THETA_DIV || geo == CYL_THETA_LAM)) {
         const double mt = 1e-5 / (gamma - 1);
         int rc;
         switch (flim) {

@@ -14,13 +14,13 @@ pytestmark = pytest.mark.gpu
 
 SHAPES = [
     (37, 11, 9),     # x: row kernel, 1 cell/thread; y,z: tile kernel (odd nx), single chunk
-    (600, 5, 4),     # x: row kernel, 2 cells/thread; y,z: TMA pipeline with 5- and 4-cell pencils
+    (600, 5, 4),     # x: row kernel, 2 cells/thread; y,z: TMA pipeline (pencils below 64 cells)
     (1100, 3, 4),    # x: chunked TMA pipeline (rows > 1024); y: 3-cell pencils
     (8, 300, 6),     # y: TMA pipeline, pencils of 257-512 cells (two box rows, 2 cells/thread)
-    (6, 7, 130),     # z: TMA pipeline, 130-cell pencils
+    (6, 7, 130),     # z: pencil-pair kernel, 130-cell pencils
     (5, 4, 3),       # tiny pencils; y,z: tile kernel
-    (8, 140, 3),     # Xin-Jin y: pencil pairs of 129-256 cells with nx a multiple of 4
-    (4, 3, 200),     # Xin-Jin z: the same
+    (8, 140, 3),     # y: pencil-pair kernels (HLL/HLLC, Xin-Jin) of 129-256 cells
+    (4, 3, 200),     # z: the same
 ]
 
 
