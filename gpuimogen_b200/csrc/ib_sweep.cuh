@@ -680,12 +680,13 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? 2 : 1)
 // the SSPRK sum u1 + u0 in a third), writes each pencil's result over its own column of the box
 // and leaves by one TMA store.  No persistent pipeline: the other CTAs on the SM hide a block's
 // load, as they hide the row kernel's.
-// Dynamic shared memory: the box (pipe_tile_bytes(n, 2)), 2 planes of 5 n elements of FT and
-// 5 n doubles for the SSPRK sum.
+// Dynamic shared memory: the box (pipe_tile_bytes(n, WC)), 2 planes of 5 NP elements of FT and
+// 5 NP doubles for the SSPRK sum (NP: the pencil length, or PADN).
 // ------------------------------------------------------------------------------------------
-__host__ __device__ __forceinline__ size_t pair_smem_bytes(int n, int ftsize, int wc)
+// n: pencil length (the box), np: stride of the planes (the pencil length, or PADN)
+__host__ __device__ __forceinline__ size_t pair_smem_bytes(int n, int ftsize, int wc, int np)
 {
-    return pipe_tile_bytes(n, wc) + (size_t)10 * n * ftsize + (size_t)40 * n;
+    return pipe_tile_bytes(n, wc) + (size_t)10 * np * ftsize + (size_t)40 * np;
 }
 
 // WC: pencils per box (2; 4 for z sweeps of x-y planes above 1 MB, whose 16-byte rows a plane
@@ -693,7 +694,11 @@ __host__ __device__ __forceinline__ size_t pair_smem_bytes(int n, int ftsize, in
 // GEO == CYL_THETA_DIV / CYL_THETA_LAM: the theta sweep of cylindrical geometry (y = theta), the
 // flux difference divided by the pencil's radius or lambda divided by it first (cyl_dflux); the
 // radius of the pencil at radial index x and z index z is theta_radius(cyl, x, z).  FP64, one sweep.
-template <int METHOD, int SLOPE, typename FT, int DIR, int NFIX = 0, int NS = 1, int WC = 2, int GEO = CYL_NONE>
+// PADN (pencils of a run-time length only): stride of the shared-memory planes fixed at PADN
+// cells, so that the phases address them at constant offsets (HLLC FP64, pencils of 129-255 cells:
+// fewer spills); 0 = the pencil length.
+template <int METHOD, int SLOPE, typename FT, int DIR, int NFIX = 0, int NS = 1, int WC = 2, int GEO = CYL_NONE,
+          int PADN = 0>
 __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : (WC == 4 ? 3 : 4))
     sweep_pair_kernel(const __grid_constant__ CUtensorMap tm, PipeArgs a, FluidConsts<FT> c, CylPencil cyl)
 {
@@ -703,10 +708,12 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : (WC
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full;
     const int n = NFIX ? NFIX : a.n;
+    // stride of the shared-memory planes
+    const int NP = NFIX ? NFIX : (PADN ? PADN : n);
     double *T = reinterpret_cast<double *>(smem_raw);  // the box: [slab][cell][column]
     FT *SA = reinterpret_cast<FT *>(smem_raw + pipe_tile_bytes(n, WC));
-    FT *SB = SA + 5 * n;
-    double *SS = reinterpret_cast<double *>(SB + 5 * n);
+    FT *SB = SA + 5 * NP;
+    double *SS = reinterpret_cast<double *>(SB + 5 * NP);
     constexpr int s0 = slot_of<METHOD, DIR>(0), s1 = slot_of<METHOD, DIR>(1), s2 = slot_of<METHOD, DIR>(2),
                   s3 = slot_of<METHOD, DIR>(3), s4 = slot_of<METHOD, DIR>(4);
     const int slots[5] = {s0, s1, s2, s3, s4};
@@ -763,10 +770,10 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : (WC
                 if (act) {
                     V5<FT> w = stage_prims<METHOD, DIR, FT>(u, c);
 #pragma unroll
-                    for (int k = 0; k < 5; k++) PX[k * n + i] = w.a[k];
+                    for (int k = 0; k < 5; k++) PX[k * NP + i] = w.a[k];
                     if (stage == 1) {
 #pragma unroll
-                        for (int k = 0; k < 5; k++) SS[k * n + i] = u1[k] + u0[k];
+                        for (int k = 0; k < 5; k++) SS[k * NP + i] = u1[k] + u0[k];
                     }
                 }
                 __syncthreads();
@@ -774,36 +781,36 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : (WC
                     V5<FT> w, dl, dr, L;
 #pragma unroll
                     for (int k = 0; k < 5; k++) {
-                        w.a[k] = PX[k * n + i];
-                        dl.a[k] = w.a[k] - PX[k * n + il];
-                        dr.a[k] = PX[k * n + ir] - w.a[k];
+                        w.a[k] = PX[k * NP + i];
+                        dl.a[k] = w.a[k] - PX[k * NP + il];
+                        dr.a[k] = PX[k * NP + ir] - w.a[k];
                     }
                     stage_faces<METHOD, SLOPE, FT>(c, w, dl, dr, L, keep);
 #pragma unroll
-                    for (int k = 0; k < 5; k++) PY[k * n + i] = L.a[k];
+                    for (int k = 0; k < 5; k++) PY[k * NP + i] = L.a[k];
                 }
                 __syncthreads();
                 if (act) {
                     V5<FT> Lr;
 #pragma unroll
-                    for (int k = 0; k < 5; k++) Lr.a[k] = PY[k * n + ir];
+                    for (int k = 0; k < 5; k++) Lr.a[k] = PY[k * NP + ir];
                     keep = stage_flux<METHOD, FT>(c, keep, Lr);
 #pragma unroll
-                    for (int k = 0; k < 5; k++) PX[k * n + i] = keep.a[k];
+                    for (int k = 0; k < 5; k++) PX[k * NP + i] = keep.a[k];
                 }
                 __syncthreads();
                 if (act) {
 #pragma unroll
                     for (int k = 0; k < 5; k++) {
                         if constexpr (GEO == CYL_NONE) {
-                            double df = (double)keep.a[k] - (double)PX[k * n + il];
+                            double df = (double)keep.a[k] - (double)PX[k * NP + il];
                             if (stage == 0) u1[k] = u0[k] - lambda * df;
-                            else u1[k] = .5 * (SS[k * n + i] - lambda * df);
+                            else u1[k] = .5 * (SS[k * NP + i] - lambda * df);
                         } else {
-                            const double d = cyl_dflux<METHOD, GEO>(k, (double)keep.a[k], (double)PX[k * n + il], lam,
+                            const double d = cyl_dflux<METHOD, GEO>(k, (double)keep.a[k], (double)PX[k * NP + il], lam,
                                                                     0.0, 0.0, rp, 0.0, 0.0, 0.0, c);
                             if (stage == 0) u1[k] = u0[k] - d;
-                            else u1[k] = .5 * (SS[k * n + i] - d);
+                            else u1[k] = .5 * (SS[k * NP + i] - d);
                         }
                     }
                 }

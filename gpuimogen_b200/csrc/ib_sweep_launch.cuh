@@ -124,10 +124,11 @@ int launch_pipe(double *q, int64_t slab, const int grid[3], DevScalar lambda, co
 // arrives as two rows of 256), x even; one CTA per block of two adjacent pencils.  Returns
 // IB_ERROR_NOIMPLEMENT (caller falls back) otherwise.  GEO: cylindrical theta pencils (y, one
 // sweep), with their radius rule in cyl.
-template <int METHOD, int SLOPE, typename FT, int DIR, int NFIX = 0, int WC = 2, int GEO = CYL_NONE>
+template <int METHOD, int SLOPE, typename FT, int DIR, int NFIX = 0, int WC = 2, int GEO = CYL_NONE, int PADN = 0>
 int launch_pair(double *q, int64_t slab, const int grid[3], DevScalar lambda, const FluidConsts<FT> &c, cudaStream_t st,
                 int nsweep, CylPencil cyl = CylPencil{0.0, 0.0, 0, 0})
 {
+    static_assert(PADN == 0 || NFIX == 0, "a fixed plane stride for pencils of a run-time length");
     static_assert(GEO == CYL_NONE || DIR == 2, "theta pencils run along y");
     if (GEO != CYL_NONE && nsweep != 1) return IB_ERROR_NOIMPLEMENT;
     static_assert(DIR != 1, "x rows take the row kernel");
@@ -154,11 +155,12 @@ int launch_pair(double *q, int64_t slab, const int grid[3], DevScalar lambda, co
     unsigned int *err = scratch().wait_flag();
     if (!err) return IB_ERROR_NOMEM;
     const int nt = (n + 31) / 32 * 32;
-    const size_t shm = pair_smem_bytes(n, (int)sizeof(FT), WC);
+    if (PADN && n > PADN) return IB_ERROR_NOIMPLEMENT;
+    const size_t shm = pair_smem_bytes(n, (int)sizeof(FT), WC, NFIX ? NFIX : (PADN ? PADN : n));
     const int ns = (nsweep == 2) ? 2 : 1;
-    auto kern = &sweep_pair_kernel<METHOD, SLOPE, FT, DIR, NFIX, 1, WC, GEO>;
+    auto kern = &sweep_pair_kernel<METHOD, SLOPE, FT, DIR, NFIX, 1, WC, GEO, PADN>;
     if constexpr (GEO == CYL_NONE) {
-        if (ns == 2) kern = &sweep_pair_kernel<METHOD, SLOPE, FT, DIR, NFIX, 2, WC>;
+        if (ns == 2) kern = &sweep_pair_kernel<METHOD, SLOPE, FT, DIR, NFIX, 2, WC, CYL_NONE, PADN>;
     }
     static int attr_bytes[2] = {0, 0};
     if ((int)shm > attr_bytes[ns - 1]) {
@@ -339,7 +341,16 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], DevScala
             else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1, 128>(q, slab, grid, lambda, c, st, nsweep);
         } else if (n <= 256 && !wide) {
             if (pair) {
-                if (dir == 2) rc = launch_pair<METHOD, SLOPE, FT, 2>(q, slab, grid, lambda, c, st, nsweep);
+                // HLLC FP64 pencils of 129-255 cells: planes of a fixed 256-cell stride (160^3 y/z
+                // 0.254 -> 0.225 ms, 192^3 0.436 -> 0.387; HLL and shorter pencils measured slower,
+                // the larger planes costing CTAs per SM)
+                constexpr bool padded = METHOD == IB_METHOD_HLLC && sizeof(FT) == 8;
+                if (padded && n > 128) {
+                    if (dir == 2) rc = launch_pair<METHOD, SLOPE, FT, 2, 0, 2, CYL_NONE, padded ? 256 : 0>(
+                                      q, slab, grid, lambda, c, st, nsweep);
+                    else rc = launch_pair<METHOD, SLOPE, FT, 3, 0, 2, CYL_NONE, padded ? 256 : 0>(q, slab, grid, lambda,
+                                                                                                c, st, nsweep);
+                } else if (dir == 2) rc = launch_pair<METHOD, SLOPE, FT, 2>(q, slab, grid, lambda, c, st, nsweep);
                 else rc = launch_pair<METHOD, SLOPE, FT, 3>(q, slab, grid, lambda, c, st, nsweep);
             }
             if (rc == IB_ERROR_NOIMPLEMENT) {

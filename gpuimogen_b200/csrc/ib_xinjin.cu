@@ -316,7 +316,9 @@ __host__ __device__ __forceinline__ size_t xj_box_bytes(int n, int wc) { return 
 // GEO == CYL_THETA_DIV / CYL_THETA_LAM: cylindrical theta pencils (y), the update's flux
 // difference divided by the pencil's radius or the stage's lambda divided by it, as in
 // xj_pencil_kernel.
-template <int FLIM, int DIR, int NFIX, int WC, int GEO = CYL_NONE>
+// PADN (pencils of a run-time length only): stride of the flux planes fixed at PADN cells, so
+// that the phases address them at constant offsets; 0 = the pencil length.
+template <int FLIM, int DIR, int NFIX, int WC, int GEO = CYL_NONE, int PADN = 0>
 __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
     xj_pair_kernel(const __grid_constant__ CUtensorMap tm, XjPairArgs a)
 {
@@ -326,9 +328,10 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
     __shared__ __align__(8) uint64_t full;
     __shared__ double red[32];
     const int n = NFIX ? NFIX : a.n;
+    const int NP = NFIX ? NFIX : (PADN ? PADN : n);  // stride of the flux planes
     double *T = reinterpret_cast<double *>(smem_raw);                        // [5][n][WC]
-    double *Lb = reinterpret_cast<double *>(smem_raw + xj_box_bytes(n, WC));  // [5][n]
-    double *Rb = Lb + 5 * n;                                                  // [5][n]
+    double *Lb = reinterpret_cast<double *>(smem_raw + xj_box_bytes(n, WC));  // [5][NP]
+    double *Rb = Lb + 5 * NP;                                                 // [5][NP]
     const int i = threadIdx.x;
     const bool act = i < n;
     const int il = (i == 0) ? n - 1 : i - 1, ir = (i == n - 1) ? 0 : i + 1;
@@ -401,8 +404,8 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
                     else if (k == 1) w = Vx * (qk + Pv);
                     else if (k == nslot) w = Vx * qk + Pv;
                     else w = Vx * qk;
-                    Lb[k * n + i] = (Cf * qk - w);
-                    Rb[k * n + i] = (Cf * qk + w);
+                    Lb[k * NP + i] = (Cf * qk - w);
+                    Rb[k * NP + i] = (Cf * qk + w);
                 }
             }
             __syncthreads();
@@ -411,8 +414,8 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
                 if (act) {
 #pragma unroll
                     for (int k = 0; k < 5; k++) {
-                        const double Lm = Lb[k * n + il], L0 = Lb[k * n + i], Lp = Lb[k * n + ir];
-                        const double Rm = Rb[k * n + il], R0 = Rb[k * n + i], Rp = Rb[k * n + ir];
+                        const double Lm = Lb[k * NP + il], L0 = Lb[k * NP + i], Lp = Lb[k * NP + ir];
+                        const double Rm = Rb[k * NP + il], R0 = Rb[k * NP + i], Rp = Rb[k * NP + ir];
                         const double dL0 = 0.5 * (L0 - Lm), dLp = 0.5 * (Lp - L0);
                         const double dR0 = 0.5 * (R0 - Rm), dRp = 0.5 * (Rp - R0);
                         double limL, limR;
@@ -424,7 +427,7 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
                 __syncthreads();
                 if (act) {
 #pragma unroll
-                    for (int k = 0; k < 5; k++) { Lb[k * n + i] = nl[k]; Rb[k * n + i] = nr[k]; }
+                    for (int k = 0; k < 5; k++) { Lb[k * NP + i] = nl[k]; Rb[k * NP + i] = nr[k]; }
                 }
                 __syncthreads();
             }
@@ -433,17 +436,17 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
 #pragma unroll
                 for (int k = 0; k < 5; k++) {
                     if constexpr (GEO == CYL_NONE) {
-                        pr[k] = u0[k] - lam * (Rb[k * n + i] - Rb[k * n + il] - Lb[k * n + ir] + Lb[k * n + i]);
+                        pr[k] = u0[k] - lam * (Rb[k * NP + i] - Rb[k * NP + il] - Lb[k * NP + ir] + Lb[k * NP + i]);
                     } else if constexpr (GEO == CYL_THETA_DIV) {
 #ifdef IB_STRICT_ARITH
-                        pr[k] = u0[k] - lam * (Rb[k * n + i] - Rb[k * n + il] - Lb[k * n + ir] + Lb[k * n + i]) / rpen;
+                        pr[k] = u0[k] - lam * (Rb[k * NP + i] - Rb[k * NP + il] - Lb[k * NP + ir] + Lb[k * NP + i]) / rpen;
 #else
-                        pr[k] = u0[k] - lam * (Rb[k * n + i] - Rb[k * n + il] - Lb[k * n + ir] + Lb[k * n + i]) *
+                        pr[k] = u0[k] - lam * (Rb[k * NP + i] - Rb[k * NP + il] - Lb[k * NP + ir] + Lb[k * NP + i]) *
                                             (1.0 / rpen);
 #endif
                     } else {
                         const double lr = lam / rpen;
-                        pr[k] = u0[k] - lr * (Rb[k * n + i] - Rb[k * n + il] - Lb[k * n + ir] + Lb[k * n + i]);
+                        pr[k] = u0[k] - lr * (Rb[k * NP + i] - Rb[k * NP + il] - Lb[k * NP + ir] + Lb[k * NP + i]);
                     }
                 }
                 double p0 = pr[0], p1 = pr[1];
@@ -477,13 +480,14 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
 // Returns IB_ERROR_NOIMPLEMENT (the caller falls back to xj_pencil_kernel) where TMA's rules or
 // the kernel's sizes do not hold: nx a multiple of WC, 16-byte aligned base and slab pitch, pencils
 // of up to 256 cells or of 512.
-template <int FLIM, int DIR, int NFIX, int WC, int GEO = CYL_NONE>
+template <int FLIM, int DIR, int NFIX, int WC, int GEO = CYL_NONE, int PADN = 0>
 static int launch_xj_pair(double *q, int64_t slab, const int grid[3], DevScalar lambda, double gamma, double rho_min,
                           double mintemp, cudaStream_t st, CylPencil cyl = CylPencil{0.0, 0.0, 0, 0})
 {
     const int nx = grid[0], ny = grid[1], nz = grid[2];
     const int n = grid[DIR - 1];
-    if ((NFIX && n != NFIX) || (!NFIX && n > 256) || n < 3 || (nx % WC)) return IB_ERROR_NOIMPLEMENT;
+    if ((NFIX && n != NFIX) || (!NFIX && n > 256) || n < 3 || (nx % WC) || (PADN && n > PADN))
+        return IB_ERROR_NOIMPLEMENT;
     if (((uintptr_t)q & 15) || (slab * 8) % 16) return IB_ERROR_NOIMPLEMENT;
     const uint64_t other = (DIR == 2) ? nz : ny;
     const uint64_t rs = (DIR == 2) ? (uint64_t)nx * 8 : (uint64_t)nx * ny * 8;  // along the pencil
@@ -502,16 +506,16 @@ static int launch_xj_pair(double *q, int64_t slab, const int grid[3], DevScalar 
     unsigned int *err = scratch().wait_flag();
     if (!err) return IB_ERROR_NOMEM;
     const int nt = (n + 31) / 32 * 32;
-    const size_t shm = xj_box_bytes(n, WC) + (size_t)80 * n;
+    const size_t shm = xj_box_bytes(n, WC) + (size_t)80 * (NFIX ? NFIX : (PADN ? PADN : n));
     static int attr_bytes = 0;
     if ((int)shm > attr_bytes) {
-        rc = check_cuda(cudaFuncSetAttribute(xj_pair_kernel<FLIM, DIR, NFIX, WC, GEO>,
+        rc = check_cuda(cudaFuncSetAttribute(xj_pair_kernel<FLIM, DIR, NFIX, WC, GEO, PADN>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
         if (rc) return rc;
         attr_bytes = (int)shm;
     }
     XjPairArgs a{n, npw, lambda, gamma, rho_min, mintemp, err, tile_wait_limit(), cyl};
-    xj_pair_kernel<FLIM, DIR, NFIX, WC, GEO><<<(unsigned)nblocks, nt, shm, st>>>(tm, a);
+    xj_pair_kernel<FLIM, DIR, NFIX, WC, GEO, PADN><<<(unsigned)nblocks, nt, shm, st>>>(tm, a);
     return check_launch();
 }
 
@@ -536,13 +540,18 @@ static int launch_xj_pair_dir(int dir, double *q, int64_t slab, const int grid[3
                               double rho_min, double mintemp, cudaStream_t st)
 {
     const int n = grid[dir - 1];
+    // pencils of 129-255 cells: flux planes of a fixed 256-cell stride (160^3 y/z 0.206 -> 0.194 ms,
+    // 192^3 0.351 -> 0.331; shorter pencils measured slower, the larger planes costing CTAs per SM)
     if (dir == 2) {
         if (n == 512) return launch_xj_pair<FLIM, 2, 512, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
         if (n == 256) return launch_xj_pair<FLIM, 2, 256, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
+        if (n > 128)
+            return launch_xj_pair<FLIM, 2, 0, 2, CYL_NONE, 256>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
         return launch_xj_pair<FLIM, 2, 0, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
     }
     if (n == 512) return launch_xj_pair<FLIM, 3, 512, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
     if (n == 256) return launch_xj_pair<FLIM, 3, 256, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
+    if (n > 128) return launch_xj_pair<FLIM, 3, 0, 2, CYL_NONE, 256>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
     return launch_xj_pair<FLIM, 3, 0, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
 }
 
