@@ -297,9 +297,12 @@ __host__ __device__ constexpr bool row_ssum() { return CPT == 1 && NFIX != 512; 
 // GEO == CYL_RADIAL: the radial sweep of cylindrical geometry (x = r), whose update weights the
 // faces by their radii and adds the geometric pressure term to p_r (cyl_dflux); one cell per
 // thread, FP64, one sweep.
-template <int METHOD, int SLOPE, typename FT, int CPT, int NFIX = 0, int NS = 1, int GEO = CYL_NONE>
+// PADN (rows of a run-time length only): stride of the shared-memory planes fixed at PADN cells,
+// so that the phases address them at constant offsets; 0 = the row length.
+template <int METHOD, int SLOPE, typename FT, int CPT, int NFIX = 0, int NS = 1, int GEO = CYL_NONE, int PADN = 0>
 __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_kernel(SweepArgs a, FluidConsts<FT> c)
 {
+    static_assert(PADN == 0 || (NFIX == 0 && CPT == 1), "a fixed plane stride for rows of a run-time length");
     static_assert(GEO == CYL_NONE || (GEO == CYL_RADIAL && row_ssum<CPT, NFIX>() && NS == 1 &&
                                       std::is_same<FT, double>::value),
                   "radial rows: one cell per thread with the SSPRK sum in shared memory, one FP64 sweep");
@@ -307,9 +310,10 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
     // the TMA kernels' smem_raw is 1024-byte aligned
     extern __shared__ __align__(16) unsigned char row_smem_raw[];
     const int n = NFIX ? NFIX : a.nx;  // NFIX: the row length fixed at compile time
+    const int NP = PADN ? PADN : n;    // stride of the planes
     FT *SA = reinterpret_cast<FT *>(row_smem_raw);
-    FT *SB = SA + 5 * n;
-    double *SS = reinterpret_cast<double *>(row_smem_raw + (size_t)10 * n * sizeof(FT));
+    FT *SB = SA + 5 * NP;
+    double *SS = reinterpret_cast<double *>(row_smem_raw + (size_t)10 * NP * sizeof(FT));
     const int64_t row = blockIdx.x;
     double *q = a.q + row * n;
     const int64_t S = a.slab;
@@ -352,11 +356,11 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
             if (act[m]) {
                 V5<FT> w = stage_prims<METHOD, 1, FT>(u[m], c);
 #pragma unroll
-                for (int k = 0; k < 5; k++) PX[k * n + i] = w.a[k];
+                for (int k = 0; k < 5; k++) PX[k * NP + i] = w.a[k];
                 if (GEO == CYL_RADIAL && METHOD == IB_METHOD_HLL) php = (double)w.a[2];
                 if (row_ssum<CPT, NFIX>() && stage == 1) {  // after the prims: HLL floors u1 in place
 #pragma unroll
-                    for (int k = 0; k < 5; k++) SS[k * n + i] = u1[m][k] + u0[m][k];
+                    for (int k = 0; k < 5; k++) SS[k * NP + i] = u1[m][k] + u0[m][k];
                 }
             }
         }
@@ -370,13 +374,13 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
                 V5<FT> w, dl, dr, L;
 #pragma unroll
                 for (int k = 0; k < 5; k++) {
-                    w.a[k] = PX[k * n + i];
-                    dl.a[k] = w.a[k] - PX[k * n + il];
-                    dr.a[k] = PX[k * n + ir] - w.a[k];
+                    w.a[k] = PX[k * NP + i];
+                    dl.a[k] = w.a[k] - PX[k * NP + il];
+                    dr.a[k] = PX[k * NP + ir] - w.a[k];
                 }
                 stage_faces<METHOD, SLOPE, FT>(c, w, dl, dr, L, keep[m]);
 #pragma unroll
-                for (int k = 0; k < 5; k++) PY[k * n + i] = L.a[k];
+                for (int k = 0; k < 5; k++) PY[k * NP + i] = L.a[k];
                 if (GEO == CYL_RADIAL && METHOD == IB_METHOD_HLLC) psum = (double)L.a[1] + (double)keep[m].a[1];
             }
         }
@@ -389,10 +393,10 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
                 int ir = (i == n - 1) ? 0 : i + 1;
                 V5<FT> Lr;
 #pragma unroll
-                for (int k = 0; k < 5; k++) Lr.a[k] = PY[k * n + ir];
+                for (int k = 0; k < 5; k++) Lr.a[k] = PY[k * NP + ir];
                 keep[m] = stage_flux<METHOD, FT>(c, keep[m], Lr);
 #pragma unroll
-                for (int k = 0; k < 5; k++) PX[k * n + i] = keep[m].a[k];
+                for (int k = 0; k < 5; k++) PX[k * NP + i] = keep[m].a[k];
             }
         }
         __syncthreads();
@@ -410,17 +414,17 @@ __global__ void __launch_bounds__(512, (CPT == 1) ? IB_ROW_MINB : 1) sweep_row_k
 #pragma unroll
                     for (int k = 0; k < 5; k++) {
                         const double rho1 = (stage == 0) ? (k == 0 ? 0.0 : u1[m][0]) : rho_in;
-                        const double d = cyl_dflux<METHOD, GEO>(k, (double)keep[m].a[k], (double)PX[k * n + il], lambda,
+                        const double d = cyl_dflux<METHOD, GEO>(k, (double)keep[m].a[k], (double)PX[k * NP + il], lambda,
                                                                 rc, a.cdr, 0.0, psum, php, rho1, c);
                         if (stage == 0) u1[m][k] = u0[m][k] - d;
-                        else u1[m][k] = .5 * (SS[k * n + i] - d);
+                        else u1[m][k] = .5 * (SS[k * NP + i] - d);
                     }
                 } else {
 #pragma unroll
                     for (int k = 0; k < 5; k++) {
-                        double df = (double)keep[m].a[k] - (double)PX[k * n + il];
+                        double df = (double)keep[m].a[k] - (double)PX[k * NP + il];
                         if (stage == 0) u1[m][k] = u0[m][k] - lambda * df;
-                        else if (row_ssum<CPT, NFIX>()) u1[m][k] = .5 * (SS[k * n + i] - lambda * df);
+                        else if (row_ssum<CPT, NFIX>()) u1[m][k] = .5 * (SS[k * NP + i] - lambda * df);
                         else u1[m][k] = .5 * (u1[m][k] + u0[m][k] - lambda * df);
                     }
                 }

@@ -185,6 +185,10 @@ int launch_row_radial(double *q, int64_t slab, const int grid[3], DevScalar lamb
     const int64_t rows = (int64_t)grid[1] * grid[2];
     const int nt = ((nx + 31) / 32) * 32;
     const size_t shm = (size_t)10 * nx * sizeof(double) + (size_t)40 * nx;  // two planes, the SSPRK sum
+    if (nx == 256) {  // the length at compile time (constant plane offsets, fewer spills); 30 KB
+        sweep_row_kernel<METHOD, SLOPE, double, 1, 256, 1, CYL_RADIAL><<<(unsigned)rows, nt, shm, st>>>(a, c);
+        return check_launch();
+    }
     auto kern = sweep_row_kernel<METHOD, SLOPE, double, 1, 0, 1, CYL_RADIAL>;
     static int attr_bytes = 0;
     if ((int)shm > attr_bytes) {
@@ -438,6 +442,10 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], DevScala
                     sweep_row_kernel<METHOD, SLOPE, FT, 1, 512, NS><<<(unsigned)rows, nt, shm, st>>>(a, c);
                 } else if (nx == 128) {
                     sweep_row_kernel<METHOD, SLOPE, FT, 1, 128, NS><<<(unsigned)rows, nt, shm, st>>>(a, c);
+                } else if (METHOD == IB_METHOD_HLLC && sizeof(FT) == 8 && nx > 128 && nx < 256) {
+                    // planes of a fixed 256-cell stride: constant offsets in the phases, fewer spills
+                    const size_t shm_p = (size_t)10 * 256 * sizeof(FT) + (size_t)40 * 256;
+                    sweep_row_kernel<METHOD, SLOPE, FT, 1, 0, NS, CYL_NONE, 256><<<(unsigned)rows, nt, shm_p, st>>>(a, c);
                 } else {
                     static const int rc1 = opt_in(sweep_row_kernel<METHOD, SLOPE, FT, 1, 0, NS>, max1);
                     if (rc1) return rc1;

@@ -30,8 +30,10 @@ def _n(shape):
 @pytest.mark.parametrize("geometric", [False, True])
 # radial rows up to 512 cells take the row kernel, theta pencils of at least 64 cells with x even
 # the pencil-pair kernels ((12, 72, 3)); shorter theta pencils, or x odd, the tile kernel (or the
-# Xin-Jin pencil kernel); (520, 6, 1) sends the radial rows to the tile kernel
-@pytest.mark.parametrize("shape", [(32, 24, 6), (32, 24, 1), (20, 9, 5), (21, 9, 5), (520, 6, 1), (12, 72, 3)])
+# Xin-Jin pencil kernel); (520, 6, 1) sends the radial rows to the tile kernel, (256, 4, 2) to the
+# 256-cell row kernel
+@pytest.mark.parametrize("shape", [(32, 24, 6), (32, 24, 1), (20, 9, 5), (21, 9, 5), (520, 6, 1), (12, 72, 3),
+                                   (256, 4, 2)])
 @pytest.mark.parametrize("method,c_iso", [(2, -1.0), (1, -1.0), (1, 0.8), (3, -1.0)])
 def test_cyl_sweeps_vs_oracle(cuda, ib, po, variant, geometric, shape, method, c_iso):
     n = _n(shape)

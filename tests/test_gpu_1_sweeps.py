@@ -21,6 +21,7 @@ SHAPES = [
     (5, 4, 3),       # tiny pencils; y,z: tile kernel
     (8, 140, 3),     # y: pencil-pair kernels (HLL/HLLC, Xin-Jin) of 129-256 cells
     (4, 3, 200),     # z: the same
+    (160, 3, 2),     # x: HLLC rows of 129-255 cells, planes of a fixed 256-cell stride
 ]
 
 
