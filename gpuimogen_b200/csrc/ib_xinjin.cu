@@ -324,6 +324,7 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
 {
     static_assert(GEO == CYL_NONE || ((GEO == CYL_THETA_DIV || GEO == CYL_THETA_LAM) && DIR == 2),
                   "theta pencils run along y");
+    static_assert(DIR != 1 || (WC == 1 && GEO == CYL_NONE), "x rows: one row per box, square geometry");
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full;
     __shared__ double red[32];
@@ -351,7 +352,8 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
         mbar_init(&full, 1);
         fence_mbar_init();
         mbar_arrive_expect_tx(&full, (uint32_t)(40 * WC * n));
-        tma_load_5d(T, &tm, (int)(b % a.npw) * WC, 0, 0, (int)(b / a.npw), 0, &full);
+        if constexpr (DIR == 1) tma_load_3d(T, &tm, 0, (int)b, 0, &full);
+        else tma_load_5d(T, &tm, (int)(b % a.npw) * WC, 0, 0, (int)(b / a.npw), 0, &full);
     }
     const bool ok = mbar_wait_cta(&full, 0, a.spin);  // uniform across the CTA
     if (!ok) {
@@ -471,7 +473,8 @@ __global__ void __launch_bounds__(NFIX == 512 ? 512 : 256, NFIX == 512 ? 2 : 4)
     fence_proxy_async_smem();
     __syncthreads();
     if (leader) {
-        tma_store_5d(&tm, T, (int)(b % a.npw) * WC, 0, 0, (int)(b / a.npw), 0);
+        if constexpr (DIR == 1) tma_store_3d(&tm, T, 0, (int)b, 0);
+        else tma_store_5d(&tm, T, (int)(b % a.npw) * WC, 0, 0, (int)(b / a.npw), 0);
         bulk_commit();
         bulk_wait_all();
     }
@@ -489,19 +492,35 @@ static int launch_xj_pair(double *q, int64_t slab, const int grid[3], DevScalar 
     if ((NFIX && n != NFIX) || (!NFIX && n > 256) || n < 3 || (nx % WC) || (PADN && n > PADN))
         return IB_ERROR_NOIMPLEMENT;
     if (((uintptr_t)q & 15) || (slab * 8) % 16) return IB_ERROR_NOIMPLEMENT;
-    const uint64_t other = (DIR == 2) ? nz : ny;
-    const uint64_t rs = (DIR == 2) ? (uint64_t)nx * 8 : (uint64_t)nx * ny * 8;  // along the pencil
-    const uint64_t os = (DIR == 2) ? (uint64_t)nx * ny * 8 : (uint64_t)nx * 8;  // across pencils
-    // TMA boxes are at most 256 rows: a 512-cell pencil comes as two rows of 256
-    const int bh = (n > 256) ? n / 2 : n, nh = (n > 256) ? 2 : 1;
-    uint64_t dims[5] = {(uint64_t)nx, (uint64_t)bh, (uint64_t)nh, other, 5};
-    uint64_t strides[4] = {rs, rs * bh, os, (uint64_t)slab * 8};
-    uint32_t box[5] = {WC, (uint32_t)bh, (uint32_t)nh, 1, 5};
-    const int npw = nx / WC;
-    const int64_t nblocks = (int64_t)npw * other;
-    if (nblocks >= (int64_t)1 << 31) return IB_ERROR_NOIMPLEMENT;
     CUtensorMap tm;
-    int rc = encode_tmap_f64(&tm, q, 5, dims, strides, box);
+    int npw;
+    int64_t nblocks;
+    int rc;
+    if constexpr (DIR == 1) {
+        // x rows: a box of one whole row and 5 slabs (rows of up to 256 cells, an even number, so
+        // that the row pitch is a multiple of 16 bytes)
+        if (n > 256 || (nx & 1)) return IB_ERROR_NOIMPLEMENT;
+        npw = 1;
+        nblocks = (int64_t)ny * nz;
+        if (nblocks >= (int64_t)1 << 31) return IB_ERROR_NOIMPLEMENT;
+        uint64_t dims[3] = {(uint64_t)nx, (uint64_t)nblocks, 5};
+        uint64_t strides[2] = {(uint64_t)nx * 8, (uint64_t)slab * 8};
+        uint32_t box[3] = {(uint32_t)nx, 1, 5};
+        rc = encode_tmap_f64(&tm, q, 3, dims, strides, box);
+    } else {
+        const uint64_t other = (DIR == 2) ? nz : ny;
+        const uint64_t rs = (DIR == 2) ? (uint64_t)nx * 8 : (uint64_t)nx * ny * 8;  // along the pencil
+        const uint64_t os = (DIR == 2) ? (uint64_t)nx * ny * 8 : (uint64_t)nx * 8;  // across pencils
+        // TMA boxes are at most 256 rows: a 512-cell pencil comes as two rows of 256
+        const int bh = (n > 256) ? n / 2 : n, nh = (n > 256) ? 2 : 1;
+        uint64_t dims[5] = {(uint64_t)nx, (uint64_t)bh, (uint64_t)nh, other, 5};
+        uint64_t strides[4] = {rs, rs * bh, os, (uint64_t)slab * 8};
+        uint32_t box[5] = {WC, (uint32_t)bh, (uint32_t)nh, 1, 5};
+        npw = nx / WC;
+        nblocks = (int64_t)npw * other;
+        if (nblocks >= (int64_t)1 << 31) return IB_ERROR_NOIMPLEMENT;
+        rc = encode_tmap_f64(&tm, q, 5, dims, strides, box);
+    }
     if (rc) return rc;
     unsigned int *err = scratch().wait_flag();
     if (!err) return IB_ERROR_NOMEM;
@@ -542,6 +561,12 @@ static int launch_xj_pair_dir(int dir, double *q, int64_t slab, const int grid[3
     const int n = grid[dir - 1];
     // pencils of 129-255 cells: flux planes of a fixed 256-cell stride (160^3 y/z 0.206 -> 0.194 ms,
     // 192^3 0.351 -> 0.331; shorter pencils measured slower, the larger planes costing CTAs per SM)
+    if (dir == 1) {  // x rows of up to 256 cells, one row per box
+        if (n == 256) return launch_xj_pair<FLIM, 1, 256, 1>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
+        if (n > 128)
+            return launch_xj_pair<FLIM, 1, 0, 1, CYL_NONE, 256>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
+        return launch_xj_pair<FLIM, 1, 0, 1>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
+    }
     if (dir == 2) {
         if (n == 512) return launch_xj_pair<FLIM, 2, 512, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
         if (n == 256) return launch_xj_pair<FLIM, 2, 256, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
@@ -562,13 +587,13 @@ int launch_xj_sweep(int flim, int dir, double *q, int64_t slab, const int grid[3
     const CylPencil cp = cyl ? cyl->pencil : CylPencil{0.0, 0.0, 0, 0};
     if ((geo == CYL_RADIAL && dir != 1) || ((geo == CYL_THETA_DIV || geo == CYL_THETA_LAM) && dir != 2))
         return IB_ERROR_INVALID_ARGS;
-    // y/z pencils of square grids: TMA pencil boxes (IMOGEN_B200_XJPAIR=0: the pencil kernel)
+    // square grids: TMA pencil boxes for y/z pencils and x rows (IMOGEN_B200_XJPAIR=0: the pencil kernel)
     static const bool xj_pair = [] {
         const char *e = getenv("IMOGEN_B200_XJPAIR");
         return !(e && e[0] == '0');
     }();
     const bool long_pencils = grid[dir - 1] >= pair_min_cells();
-    if (xj_pair && long_pencils && dir > 1 && geo == CYL_NONE) {
+    if (xj_pair && long_pencils && geo == CYL_NONE) {
         const double mt = 1e-5 / (gamma - 1);
         int rc;
         switch (flim) {

@@ -159,10 +159,13 @@ def test_xinjin_tiny_momenta_stay_finite(cuda, ib, po, direction):
         assert np.allclose(out[:, :N], ref[:, :N], rtol=1e-12, atol=1e-300), variant
 
 
-@pytest.mark.parametrize("shape,direction", [((4, 256, 5), 2), ((2, 5, 512), 3), ((6, 512, 2), 2), ((10, 4, 256), 3)])
+@pytest.mark.parametrize("shape,direction", [((4, 256, 5), 2), ((2, 5, 512), 3), ((6, 512, 2), 2), ((10, 4, 256), 3),
+                                             ((256, 3, 4), 1), ((200, 3, 2), 1), ((96, 5, 2), 1)])
 def test_xinjin_pencil_boxes_fixed_lengths(cuda, ib, po, shape, direction):
     """Xin-Jin y/z sweeps of 256- and 512-cell pencils go through the TMA pencil-box kernel's
-    fixed-length forms (a 512-cell pencil as two box rows of 256): bit for bit the oracle's."""
+    fixed-length forms (a 512-cell pencil as two box rows of 256), x rows of 64-256 cells through
+    its one-row boxes (256 cells: fixed length; 129-255: the fixed plane stride; up to 128: the
+    row length): bit for bit the oracle's."""
     n = shape[0] * shape[1] * shape[2]
     q = problems.random_jumpy(shape, gamma=1.4, seed=17)
     h = (0.05, 0.04, 0.03)
