@@ -345,11 +345,17 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], DevScala
             else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1, 128>(q, slab, grid, lambda, c, st, nsweep);
         } else if (n <= 256 && !wide) {
             if (pair) {
-                // HLLC FP64 pencils of 129-255 cells: planes of a fixed 256-cell stride (160^3 y/z
-                // 0.254 -> 0.225 ms, 192^3 0.436 -> 0.387; HLL and shorter pencils measured slower,
-                // the larger planes costing CTAs per SM)
+                // HLLC FP64 pencils of 65-127 and 129-255 cells: planes of a fixed 128- or 256-cell
+                // stride (96^3 y/z 0.061 -> 0.053 ms, 160^3 0.254 -> 0.225, 192^3 0.436 -> 0.387;
+                // HLL measured slower, and so did a 256-cell stride for pencils of 128 or fewer, the
+                // larger planes costing CTAs per SM)
                 constexpr bool padded = METHOD == IB_METHOD_HLLC && sizeof(FT) == 8;
-                if (padded && n > 128) {
+                if (padded && n > 64 && n < 128) {
+                    if (dir == 2) rc = launch_pair<METHOD, SLOPE, FT, 2, 0, 2, CYL_NONE, padded ? 128 : 0>(
+                                      q, slab, grid, lambda, c, st, nsweep);
+                    else rc = launch_pair<METHOD, SLOPE, FT, 3, 0, 2, CYL_NONE, padded ? 128 : 0>(q, slab, grid, lambda,
+                                                                                                c, st, nsweep);
+                } else if (padded && n > 128) {
                     if (dir == 2) rc = launch_pair<METHOD, SLOPE, FT, 2, 0, 2, CYL_NONE, padded ? 256 : 0>(
                                       q, slab, grid, lambda, c, st, nsweep);
                     else rc = launch_pair<METHOD, SLOPE, FT, 3, 0, 2, CYL_NONE, padded ? 256 : 0>(q, slab, grid, lambda,
@@ -442,8 +448,12 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], DevScala
                     sweep_row_kernel<METHOD, SLOPE, FT, 1, 512, NS><<<(unsigned)rows, nt, shm, st>>>(a, c);
                 } else if (nx == 128) {
                     sweep_row_kernel<METHOD, SLOPE, FT, 1, 128, NS><<<(unsigned)rows, nt, shm, st>>>(a, c);
+                } else if (METHOD == IB_METHOD_HLLC && sizeof(FT) == 8 && nx > 64 && nx < 128) {
+                    // planes of a fixed 128- or 256-cell stride: constant offsets in the phases,
+                    // fewer spills (96^3 x 0.049 -> 0.046 ms, 160^3 0.204 -> 0.190)
+                    const size_t shm_p = (size_t)10 * 128 * sizeof(FT) + (size_t)40 * 128;
+                    sweep_row_kernel<METHOD, SLOPE, FT, 1, 0, NS, CYL_NONE, 128><<<(unsigned)rows, nt, shm_p, st>>>(a, c);
                 } else if (METHOD == IB_METHOD_HLLC && sizeof(FT) == 8 && nx > 128 && nx < 256) {
-                    // planes of a fixed 256-cell stride: constant offsets in the phases, fewer spills
                     const size_t shm_p = (size_t)10 * 256 * sizeof(FT) + (size_t)40 * 256;
                     sweep_row_kernel<METHOD, SLOPE, FT, 1, 0, NS, CYL_NONE, 256><<<(unsigned)rows, nt, shm_p, st>>>(a, c);
                 } else {
