@@ -559,12 +559,15 @@ static int launch_xj_pair_dir(int dir, double *q, int64_t slab, const int grid[3
                               double rho_min, double mintemp, cudaStream_t st)
 {
     const int n = grid[dir - 1];
-    // pencils of 129-255 cells: flux planes of a fixed 256-cell stride (160^3 y/z 0.206 -> 0.194 ms,
-    // 192^3 0.351 -> 0.331; shorter pencils measured slower, the larger planes costing CTAs per SM)
+    // pencils of 65-127 and 129-255 cells: flux planes of a fixed 128- or 256-cell stride (96^3 y/z
+    // 0.048 -> 0.046 ms, 112^3 0.076 -> 0.071, 160^3 0.206 -> 0.194, 192^3 0.351 -> 0.331; a 256-cell
+    // stride for pencils of 128 or fewer measured slower, the larger planes costing CTAs per SM)
     if (dir == 1) {  // x rows of up to 256 cells, one row per box
         if (n == 256) return launch_xj_pair<FLIM, 1, 256, 1>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
         if (n > 128)
             return launch_xj_pair<FLIM, 1, 0, 1, CYL_NONE, 256>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
+        if (n > 64 && n < 128)
+            return launch_xj_pair<FLIM, 1, 0, 1, CYL_NONE, 128>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
         return launch_xj_pair<FLIM, 1, 0, 1>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
     }
     if (dir == 2) {
@@ -572,11 +575,15 @@ static int launch_xj_pair_dir(int dir, double *q, int64_t slab, const int grid[3
         if (n == 256) return launch_xj_pair<FLIM, 2, 256, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
         if (n > 128)
             return launch_xj_pair<FLIM, 2, 0, 2, CYL_NONE, 256>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
+        if (n > 64 && n < 128)
+            return launch_xj_pair<FLIM, 2, 0, 2, CYL_NONE, 128>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
         return launch_xj_pair<FLIM, 2, 0, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
     }
     if (n == 512) return launch_xj_pair<FLIM, 3, 512, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
     if (n == 256) return launch_xj_pair<FLIM, 3, 256, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
     if (n > 128) return launch_xj_pair<FLIM, 3, 0, 2, CYL_NONE, 256>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
+    if (n > 64 && n < 128)
+        return launch_xj_pair<FLIM, 3, 0, 2, CYL_NONE, 128>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
     return launch_xj_pair<FLIM, 3, 0, 2>(q, slab, grid, lambda, gamma, rho_min, mintemp, st);
 }
 
