@@ -814,7 +814,7 @@ def main():
     e2e_val = job_value(world, cells, e2e_steps, max_over_ranks(e2e_ms, world, dev))
     nbytes = 5 * slab * 8
 
-    # ---------------- north-star forms (rank 0, N = 1 only) ----------------
+    # ---------------- the FP32-flux, batched-ensemble and learned-drag forms (rank 0, N = 1 only) ----
     forms = None
     if rank == 0 and world == 1 and os.environ.get("IMOGEN_BENCH_SKIP_FORMS") != "1":
         forms = {"fp32_flux": form_fp32_flux(), "ensemble": form_ensemble(), "two_fluid": form_two_fluid()}
