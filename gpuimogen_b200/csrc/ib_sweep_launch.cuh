@@ -456,6 +456,14 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], DevScala
                     // fewer spills (HLLC 96^3 x 0.049 -> 0.046 ms, 160^3 0.204 -> 0.190; HLL 4-5 %)
                     const size_t shm_p = (size_t)10 * 128 * sizeof(FT) + (size_t)40 * 128;
                     sweep_row_kernel<METHOD, SLOPE, FT, 1, 0, NS, CYL_NONE, 128><<<(unsigned)rows, nt, shm_p, st>>>(a, c);
+                } else if (METHOD == IB_METHOD_HLLC && sizeof(FT) == 8 && nx > 256 && nx < 512) {
+                    // HLLC FP64 rows of 257-511 cells: planes of a fixed 512-cell stride (384 cells:
+                    // x 0.209 -> 0.195 ms at 384 x 96 x 96; registers already limit these CTAs to two
+                    // per SM, so the larger planes cost none)
+                    const size_t shm_p = (size_t)10 * 512 * sizeof(FT) + (size_t)40 * 512;
+                    static const int rcp = opt_in(sweep_row_kernel<METHOD, SLOPE, FT, 1, 0, NS, CYL_NONE, 512>, shm_p);
+                    if (rcp) return rcp;
+                    sweep_row_kernel<METHOD, SLOPE, FT, 1, 0, NS, CYL_NONE, 512><<<(unsigned)rows, nt, shm_p, st>>>(a, c);
                 } else if ((METHOD == IB_METHOD_HLLC || METHOD == IB_METHOD_HLL) && sizeof(FT) == 8 && nx > 128 &&
                            nx < 256) {
                     const size_t shm_p = (size_t)10 * 256 * sizeof(FT) + (size_t)40 * 256;

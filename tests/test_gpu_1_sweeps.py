@@ -23,6 +23,7 @@ SHAPES = [
     (4, 3, 200),     # z: the same
     (160, 3, 2),     # x: HLLC rows of 129-255 cells, planes of a fixed 256-cell stride
     (96, 100, 90),   # x, y, z: HLLC rows and pencils of 65-127 cells, planes of a 128-cell stride
+    (300, 4, 3),     # x: HLLC rows of 257-511 cells, planes of a 512-cell stride
 ]
 
 
