@@ -345,13 +345,15 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], DevScala
             else rc = launch_pipe<METHOD, SLOPE, FT, 3, 2, 1, 128>(q, slab, grid, lambda, c, st, nsweep);
         } else if (n <= 256 && !wide) {
             if (pair) {
-                // FP64 pencils of 65-127 cells (HLLC, HLL) and of 129-255 (HLLC): planes of a fixed
-                // 128- or 256-cell stride (HLLC 96^3 y/z 0.061 -> 0.053 ms, 160^3 0.254 -> 0.225,
-                // 192^3 0.436 -> 0.387; HLL 112^3 0.104 -> 0.102).  HLL's 129-255-cell pencils
-                // measured 4-5 % slower with it, and so did a 256-cell stride for pencils of 128 or
-                // fewer: the larger planes cost CTAs per SM.
-                constexpr bool padded128 = (METHOD == IB_METHOD_HLLC || METHOD == IB_METHOD_HLL) && sizeof(FT) == 8;
-                constexpr bool padded = METHOD == IB_METHOD_HLLC && sizeof(FT) == 8;
+                // Pencils of 65-127 cells (HLLC, FP32 flux too; HLL FP64) and of 129-255 (HLLC):
+                // planes of a fixed 128- or 256-cell stride (HLLC FP64 96^3 y/z 0.061 -> 0.053 ms,
+                // 160^3 0.254 -> 0.225, 192^3 0.436 -> 0.387; FP32 flux 192^3 0.225 -> 0.199; HLL
+                // 112^3 0.104 -> 0.102).  HLL's 129-255-cell pencils measured 4-5 % slower with it,
+                // and so did a 256-cell stride for pencils of 128 or fewer: the larger planes cost
+                // CTAs per SM.
+                constexpr bool padded128 =
+                    METHOD == IB_METHOD_HLLC || (METHOD == IB_METHOD_HLL && sizeof(FT) == 8);
+                constexpr bool padded = METHOD == IB_METHOD_HLLC;
                 if (padded128 && n > 64 && n < 128) {
                     if (dir == 2) rc = launch_pair<METHOD, SLOPE, FT, 2, 0, 2, CYL_NONE, padded128 ? 128 : 0>(
                                       q, slab, grid, lambda, c, st, nsweep);
@@ -450,21 +452,21 @@ int launch_sweep_t(int dir, double *q, int64_t slab, const int grid[3], DevScala
                     sweep_row_kernel<METHOD, SLOPE, FT, 1, 512, NS><<<(unsigned)rows, nt, shm, st>>>(a, c);
                 } else if (nx == 128) {
                     sweep_row_kernel<METHOD, SLOPE, FT, 1, 128, NS><<<(unsigned)rows, nt, shm, st>>>(a, c);
-                } else if ((METHOD == IB_METHOD_HLLC || METHOD == IB_METHOD_HLL) && sizeof(FT) == 8 && nx > 64 &&
+                } else if ((METHOD == IB_METHOD_HLLC || (METHOD == IB_METHOD_HLL && sizeof(FT) == 8)) && nx > 64 &&
                            nx < 128) {
                     // planes of a fixed 128- or 256-cell stride: constant offsets in the phases,
                     // fewer spills (HLLC 96^3 x 0.049 -> 0.046 ms, 160^3 0.204 -> 0.190; HLL 4-5 %)
                     const size_t shm_p = (size_t)10 * 128 * sizeof(FT) + (size_t)40 * 128;
                     sweep_row_kernel<METHOD, SLOPE, FT, 1, 0, NS, CYL_NONE, 128><<<(unsigned)rows, nt, shm_p, st>>>(a, c);
-                } else if (METHOD == IB_METHOD_HLLC && sizeof(FT) == 8 && nx > 256 && nx < 512) {
-                    // HLLC FP64 rows of 257-511 cells: planes of a fixed 512-cell stride (384 cells:
-                    // x 0.209 -> 0.195 ms at 384 x 96 x 96; registers already limit these CTAs to two
-                    // per SM, so the larger planes cost none)
+                } else if (METHOD == IB_METHOD_HLLC && nx > 256 && nx < 512) {
+                    // HLLC rows of 257-511 cells: planes of a fixed 512-cell stride (384 cells: x
+                    // 0.209 -> 0.195 ms at 384 x 96 x 96, FP32 flux 0.111 -> 0.106; registers already
+                    // limit these CTAs to two per SM, so the larger planes cost none)
                     const size_t shm_p = (size_t)10 * 512 * sizeof(FT) + (size_t)40 * 512;
                     static const int rcp = opt_in(sweep_row_kernel<METHOD, SLOPE, FT, 1, 0, NS, CYL_NONE, 512>, shm_p);
                     if (rcp) return rcp;
                     sweep_row_kernel<METHOD, SLOPE, FT, 1, 0, NS, CYL_NONE, 512><<<(unsigned)rows, nt, shm_p, st>>>(a, c);
-                } else if ((METHOD == IB_METHOD_HLLC || METHOD == IB_METHOD_HLL) && sizeof(FT) == 8 && nx > 128 &&
+                } else if ((METHOD == IB_METHOD_HLLC || (METHOD == IB_METHOD_HLL && sizeof(FT) == 8)) && nx > 128 &&
                            nx < 256) {
                     const size_t shm_p = (size_t)10 * 256 * sizeof(FT) + (size_t)40 * 256;
                     sweep_row_kernel<METHOD, SLOPE, FT, 1, 0, NS, CYL_NONE, 256><<<(unsigned)rows, nt, shm_p, st>>>(a, c);

@@ -12,8 +12,11 @@ pytestmark = pytest.mark.gpu
 
 # (392, 336, 6): z sweeps of a plane above 1 MB through the 8-column wide-block kernel;
 # (1040, 520, 1): x rows above 1024 and y pencils above 512 cells through the chunked pipeline
+# (160, 200, 2) and (96, 72, 4): rows and pencils of 65-127 and 129-255 cells, planes of a fixed
+# 128- or 256-cell stride; (392, 336, 6): rows of 257-511 cells, a 512-cell stride
 @pytest.mark.parametrize("shape,iters", [((48, 48, 48), 10), ((128, 96, 1), 20), ((512, 1, 1), 100),
-                                         ((392, 336, 6), 3), ((1040, 520, 1), 3)])
+                                         ((392, 336, 6), 3), ((1040, 520, 1), 3), ((160, 200, 2), 3),
+                                         ((96, 72, 4), 5)])
 def test_fp32_flux_close_to_fp64_oracle(cuda, ib, po, shape, iters):
     n = shape[0] * shape[1] * shape[2]
     q = problems.kelvin_helmholtz(shape, seed=5) if shape[1] > 1 else problems.sod(shape[0], 5 / 3.0)
